@@ -1,0 +1,261 @@
+/*
+ * qmcgpu.h -- C ABI of the B200 VMC walker hot path.
+ *
+ * This is the drop-in boundary for miniqmc's particle-by-particle (PbyP) VMC
+ * sweep: per-electron moves, electron-electron / electron-ion minimum-image
+ * distance rows, tricubic B-spline orbitals (SPO), one- and two-body B-spline
+ * Jastrows and the delayed-update Slater-determinant inverse.  Every entry
+ * point takes plain pointers and sizes, returns an int status (QMC_OK == 0)
+ * and never exits the process.
+ *
+ * The reference interfaces each group replaces (paths inside QMCPACK/miniqmc):
+ *   ParticleSet        src/Particle/ParticleSet.h:190-260, ParticleSet.cpp:280-378
+ *   SPOSet             src/QMCWaveFunctions/SPOSet.h:55-127
+ *   WaveFunction       src/QMCWaveFunctions/WaveFunction.h:62-96, WaveFunction.cpp:178-499
+ *   WaveFunctionComponent  src/QMCWaveFunctions/WaveFunctionComponent.h:127-252
+ *   BsplineFunctor     src/QMCWaveFunctions/Jastrow/BsplineFunctor.h:93-130
+ *   NiO input          src/Input/nio.hpp:17-169, src/Particle/ParticleSet_builder.cpp:23-53
+ *   PbyP sweep driver  src/Drivers/miniqmc.cpp:406-468
+ *
+ * Units: bohr.  Matrices are row-major.  Lattice tensors hold the lattice
+ * vectors as rows (a_i = lattice[3*i .. 3*i+2]), as CrystalLattice::R does.
+ *
+ * Threading: handles are externally synchronised (one host thread per walker
+ * batch at a time); distinct handles may be used concurrently.
+ */
+#ifndef QMCGPU_H
+#define QMCGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference aborts with APP_ABORT -> exit(1);
+ *      Configuration.h:35.  Here every failure is a return code) ---- */
+enum {
+  QMC_OK = 0,
+  QMC_ERR_ARG = 1,       /* null handle, size or index out of range        */
+  QMC_ERR_CUDA = 2,      /* CUDA runtime failure (launch, copy)             */
+  QMC_ERR_OOM = 3,       /* device allocation failed                        */
+  QMC_ERR_SINGULAR = 4,  /* zero pivot in the FP64 LU of a Slater matrix    */
+  QMC_ERR_NONFINITE = 5, /* NaN / Inf in a ratio or a log value             */
+  QMC_ERR_TIMEOUT = 6,   /* a bounded device wait ran out                   */
+  QMC_ERR_STATE = 7,     /* call out of protocol order (e.g. accept w/o move)*/
+  QMC_ERR_NODEVICE = 8,  /* no sm_100 device / library built for other arch */
+  QMC_ERR_ADMISSION = 9  /* job refused: does not fit the memory budget     */
+};
+
+/* arithmetic forms */
+enum {
+  QMC_PREC_FP64 = 0,  /* plain form: FP64 everywhere                        */
+  QMC_PREC_MIXED = 1  /* FP32 splines/tables/Jastrows/inverse, FP64 LU,
+                         log-det and the k x k Woodbury block              */
+};
+
+/* spline coefficient fills */
+enum {
+  QMC_FILL_USER = 0,      /* caller supplies the table                     */
+  QMC_FILL_REFERENCE = 1, /* einspline_spo::set: one mt19937(seed) uniform
+                             field times cos(2 pi n / norb)
+                             (einspline_spo.hpp:145-155,
+                              BsplineAllocator.hpp:161-182)                */
+  QMC_FILL_UNIFORM = 2    /* every coefficient independent, uniform
+                             [-0.5, 0.5) from SplitMix64(seed, index)      */
+};
+
+/* what the determinant uses as the orbital "laplacian" */
+enum {
+  QMC_LAP_HXX = 0,   /* the reference stores hess.xx (einspline_spo.hpp:220) */
+  QMC_LAP_TRACE = 1  /* hxx + hyy + hzz                                      */
+};
+
+/* wavefunction factors (check_wfc -f Det / J1 / J2 tests them one by one,
+ * check_wfc.cpp:152-156) */
+enum { QMC_WF_DET = 1, QMC_WF_J1 = 2, QMC_WF_J2 = 4, QMC_WF_ALL = 7 };
+
+/* random streams for the fused sweep */
+enum {
+  QMC_RNG_DEVICE = 0, /* per-walker device mt19937 streams (seeded at init)  */
+  QMC_RNG_HOST = 1    /* caller supplies ur[W][nsub][N], delta[W][nsub][N][3]*/
+};
+
+#define QMC_MAX_FUNCTOR_COEFS 32
+#define QMC_MAX_ION_GROUPS 4
+
+/* A radial cubic B-spline functor after BsplineFunctor::setupParameters:
+ * coefs = SplineCoefs (NumParams + 4 values), cutoff = cutoff_radius,
+ * delta_r_inv = DeltaRInv.  (BsplineFunctor.h:93-130) */
+typedef struct {
+  int n_coefs;
+  double cutoff;
+  double delta_r_inv;
+  double coefs[QMC_MAX_FUNCTOR_COEFS];
+} qmc_functor;
+
+/* Everything that defines one physical system (shared by all its walkers). */
+typedef struct {
+  double lattice[9];       /* simulation cell, rows = lattice vectors        */
+  int n_ions;
+  int n_ion_groups;        /* species count (<= QMC_MAX_ION_GROUPS)          */
+  const double* ion_pos;   /* [n_ions][3] Cartesian, grouped by species      */
+  const int* ion_group;    /* [n_ions] species index, non-decreasing         */
+  int n_elec;              /* electrons; the first n_up are spin up          */
+  int n_up;                /* must equal n_elec - n_up == n_orb              */
+  double spo_lattice[9];   /* cell on which the orbitals are periodic        */
+  int grid[3];             /* spline grid nx, ny, nz (table has +3 per axis) */
+  int n_orb;               /* orbitals per spin determinant                  */
+  int spo_fill;            /* QMC_FILL_*                                     */
+  uint64_t spo_seed;
+  const double* spo_user_coefs; /* QMC_FILL_USER: [nx+3][ny+3][nz+3][n_orb] */
+  int lap_mode;            /* QMC_LAP_*                                      */
+  int components;          /* QMC_WF_* mask of the factors in the wavefunction;
+                              0 means all (Slater determinants, J1, J2)      */
+  qmc_functor j1[QMC_MAX_ION_GROUPS]; /* one per ion species                 */
+  qmc_functor j2_uu;       /* same-spin pairs (uu and dd)                    */
+  qmc_functor j2_ud;       /* opposite-spin pairs                            */
+} qmc_system_desc;
+
+/* NiO builders -------------------------------------------------------- */
+enum {
+  QMC_NIO_REF32 = 0, /* the reference's 32-atom cell tiled by (na,nb,nc)
+                        (nio.hpp:23-79 + ParticleIOUtility.h:30-117)        */
+  QMC_NIO_PRIM4 = 1  /* the 4-atom NiO cell (half of each 32-atom lattice
+                        vector: O(0,0,1/2), O(1/2,1/2,0), Ni(0,0,0),
+                        Ni(1/2,1/2,1/2)) tiled by (na,nb,nc)               */
+};
+/* quirks of the reference's NiO input, reproduced when asked (REF32 only):
+ * bit 0: at tiling (1,1,1) the ion positions stay in lattice units and are
+ *        used as Cartesian coordinates (expandSuperCell returns before the
+ *        conversion; ParticleIOUtility.h:42-43, nio.hpp:35);
+ * bit 1: every ion is in species group 0 (ParticleSet::create(int) sets
+ *        GroupID = 0; nio.hpp:33, ParticleSet.cpp:96-101).                 */
+enum { QMC_NIO_QUIRK_UNIT_IONS = 1, QMC_NIO_QUIRK_ONE_GROUP = 2 };
+
+/* Number of ions for a NiO tiling (n_ions = 32*na*nb*nc or 4*na*nb*nc). */
+int qmc_nio_count(int cell, int na, int nb, int nc, int* n_ions);
+/* Fill lattice[9], ion_pos[n_ions*3], ion_group[n_ions], spo_lattice[9]
+ * (the untiled cell, as SPOSet_builder.cpp:38-39 uses) and n_groups. */
+int qmc_nio_build(int cell, int na, int nb, int nc, int quirks, double* lattice,
+                  double* ion_pos, int* ion_group, int* n_groups,
+                  double* spo_lattice);
+/* The reference's Jastrow tables (nio.hpp:81-168), cutoffs capped by the
+ * Wigner-Seitz radius of the given cell: j1[0] = O, j1[1] = Ni. */
+int qmc_nio_jastrows(const double* lattice, qmc_functor* j1_O, qmc_functor* j1_Ni,
+                     qmc_functor* j2_uu, qmc_functor* j2_ud);
+/* BsplineFunctor::setupParameters(n_params, rcut, cusp, params). */
+int qmc_functor_setup(int n_params, double rcut, double cusp, const double* params,
+                      qmc_functor* out);
+/* Wigner-Seitz radius of a periodic cell (CrystalLattice.cpp:118-125). */
+int qmc_lattice_ws_radius(const double* lattice, double* ws);
+
+/* Library / device ----------------------------------------------------- */
+const char* qmc_status_string(int status);
+/* Select the CUDA device for the calling thread and check it is sm_100. */
+int qmc_init(int device);
+/* Text of the last error recorded by this thread (never NULL). */
+const char* qmc_last_error(void);
+
+/* Systems (shared, read-only spline table) -------------------------------- */
+typedef struct qmc_system_s qmc_system;
+int qmc_system_create(const qmc_system_desc* desc, int precision, qmc_system** out);
+int qmc_system_destroy(qmc_system* sys);
+/* bytes of device memory held by the system (spline table + ions) */
+int qmc_system_bytes(const qmc_system* sys, size_t* bytes);
+
+/* SPOSet::evaluate (VGH) at arbitrary Cartesian points, for check_spo.
+ * v[n_pos][n_orb], g[n_pos][3][n_orb], h[n_pos][6][n_orb] (xx,xy,xz,yy,yz,zz);
+ * any output may be NULL.  (MultiBspline.hpp:165-280, einspline_spo.hpp:194) */
+int qmc_spo_evaluate_vgh(qmc_system* sys, int n_pos, const double* pos, double* v,
+                         double* g, double* h);
+/* SPOSet::evaluate (values only, MultiBspline.hpp:35-63). */
+int qmc_spo_evaluate_v(qmc_system* sys, int n_pos, const double* pos, double* v);
+
+/* Walker batches (device-resident walker state) ----------------------- */
+typedef struct qmc_walkers_s qmc_walkers;
+/* delay_rank k >= 1 (k == 1 is rank-1 Sherman-Morrison, DelayedUpdate.h:166). */
+int qmc_walkers_create(qmc_system* sys, int n_walkers, int delay_rank, qmc_walkers** out);
+int qmc_walkers_destroy(qmc_walkers* w);
+/* device bytes held by the batch */
+int qmc_walkers_bytes(const qmc_walkers* w, size_t* bytes);
+/* Stream used by every launch on this batch (a cudaStream_t; NULL = the
+ * batch's own stream). */
+int qmc_walkers_set_stream(qmc_walkers* w, void* stream);
+/* Mover(seed) + build_els: walker i's mt19937 is seeded with seeds[i] and its
+ * first 3N uniforms place the electrons (Mover.hpp:60-63,
+ * ParticleSet_builder.cpp:33-53); the stream then drives the sweep. */
+int qmc_walkers_init_random(qmc_walkers* w, const uint32_t* seeds);
+int qmc_walkers_set_positions(qmc_walkers* w, const double* R /* [W][N][3] */);
+int qmc_walkers_get_positions(qmc_walkers* w, double* R /* [W][N][3] */);
+
+/* ParticleSet verbs over all walkers of the batch (the flex_* forms of
+ * ParticleSet.cpp:296-346; W == 1 is the single-walker API). */
+int qmc_pset_update(qmc_walkers* w);
+int qmc_pset_set_active(qmc_walkers* w, int iat);
+int qmc_pset_make_move(qmc_walkers* w, int iat, const double* displ /* [W][3] */);
+/* accept[i] != 0: acceptMove(iat), else rejectMove(iat) */
+int qmc_pset_accept_reject(qmc_walkers* w, int iat, const int* accept);
+int qmc_pset_done(qmc_walkers* w);
+/* Distance rows of the active move (DistanceTableData Temp_r/Temp_dr):
+ * aa_r[W][N], aa_dr[W][N][3], ab_r[W][I], ab_dr[W][I][3]; NULL skips. */
+int qmc_pset_get_temp_rows(qmc_walkers* w, double* aa_r, double* aa_dr, double* ab_r,
+                           double* ab_dr);
+
+/* WaveFunction verbs (WaveFunction.cpp:178-279) */
+/* evaluateLog from scratch: SPO VGH of all electrons, FP64 LU inverse and
+ * log|det| per spin, J1/J2 recompute.  logpsi[W] may be NULL. */
+int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi);
+int qmc_wf_eval_grad(qmc_walkers* w, int iat, double* grad /* [W][3] */);
+/* ratioGrad: ratio[W] = det * J1 * J2 ratio; grad[W][3] = grad log psi at
+ * the proposed position. */
+int qmc_wf_ratio_grad(qmc_walkers* w, int iat, double* ratio, double* grad);
+/* ratio only (SPOSet values, no gradients). */
+int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio);
+/* accept[i] != 0: acceptMove(iat); else restore(iat) (a no-op). */
+int qmc_wf_accept_restore(qmc_walkers* w, int iat, const int* accept);
+int qmc_wf_complete_updates(qmc_walkers* w);
+/* evaluateGL: G[W][N][3], L[W][N] (either may be NULL), logpsi[W]. */
+int qmc_wf_evaluate_gl(qmc_walkers* w, double* G, double* L, double* logpsi);
+/* Per-component log values and phases after the last evaluateLog /
+ * accept / evaluateGL: comp[W][6] = {logdet_up, logdet_dn, phase_up,
+ * phase_dn, logJ1, logJ2}. */
+int qmc_wf_components(qmc_walkers* w, double* comp);
+/* Slater-matrix inverse of one walker and spin: (A^{-1})^T, n_orb x n_orb
+ * (DiracDeterminant::psiM), with any pending delayed update applied first. */
+int qmc_wf_get_inverse(qmc_walkers* w, int walker, int spin, double* psiM);
+
+/* The fused PbyP sweep (miniqmc.cpp:406-468): for each step, n_substeps x
+ * (N uniforms, 3N normals, N moves of evalGrad / makeMove / ratioGrad /
+ * threshold accept, completeUpdates), then donePbyP + evaluateGL.  One
+ * persistent launch per step covers every walker of the batch. */
+typedef struct {
+  int n_steps;
+  int n_substeps;
+  double accept;          /* accept if ur < accept (miniqmc.cpp:445)           */
+  int rng_mode;           /* QMC_RNG_*                                         */
+  const double* ur;       /* QMC_RNG_HOST: [n_steps][W][n_substeps][N]         */
+  const double* delta;    /* QMC_RNG_HOST: [n_steps][W][n_substeps][N][3]      */
+  int recompute_every;    /* FP64 LU refresh of the inverse every this many
+                             steps (0 = never)                                */
+  double* trace;          /* optional [n_steps][W][n_substeps][N][8]:
+                             ratio, grad_new[3], grad_now[3], accepted        */
+  int64_t* n_accepted;    /* optional [W] accepted-move counts (sum of steps) */
+  double* logpsi;         /* optional [W] log|psi| after the last step         */
+} qmc_sweep_opts;
+int qmc_sweep(qmc_walkers* w, const qmc_sweep_opts* opts);
+/* Asynchronous form for device-resident callers: no host copies, inputs
+ * already on the device (QMC_RNG_DEVICE only); results stay on the device
+ * until qmc_walkers_sync + qmc_sweep_results. */
+int qmc_sweep_async(qmc_walkers* w, int n_steps, int n_substeps, double accept,
+                    int recompute_every);
+int qmc_walkers_sync(qmc_walkers* w);
+int qmc_sweep_results(qmc_walkers* w, int64_t* n_accepted, double* logpsi);
+/* Number of CUDA kernel launches this batch issued since creation. */
+int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMCGPU_H */

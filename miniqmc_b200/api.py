@@ -1,0 +1,377 @@
+"""Python mirror of miniqmc's ParticleSet / SPOSet / WaveFunction interface.
+
+The classes below call a shared library that exports the C ABI of
+include/qmcgpu.h.  `Library()` loads the product library (libqmcgpu.so,
+built in-tree by miniqmc_b200/build.py); there is no CPU fallback -- if the
+library or a CUDA device is missing, the calls fail loudly.
+
+Reference interface each method mirrors (QMCPACK/miniqmc):
+  Walkers.make_move / accept_reject     ParticleSet::flex_makeMove, acceptMove,
+                                        rejectMove (ParticleSet.cpp:316-378)
+  Walkers.evaluate_log / eval_grad /    WaveFunction::evaluateLog, evalGrad,
+  ratio_grad / ratio / accept_restore / ratioGrad, ratio, acceptMove, restore,
+  complete_updates / evaluate_gl        completeUpdates, evaluateGL
+                                        (WaveFunction.cpp:178-279)
+  System.spo_vgh / spo_v                SPOSet::evaluate (SPOSet.h:55-66)
+  Walkers.sweep                         the PbyP loop of miniqmc.cpp:406-468
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import capi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_LIB = os.path.join(_HERE, 'libqmcgpu.so')
+
+
+class QMCError(RuntimeError):
+    def __init__(self, status, where, detail=''):
+        self.status = status
+        super().__init__('%s failed: %s %s' % (where, capi.STATUS.get(status, status), detail))
+
+
+def _pd(a):
+    return None if a is None else a.ctypes.data_as(capi.PD)
+
+
+def _pi(a):
+    return None if a is None else a.ctypes.data_as(capi.PI)
+
+
+class Library:
+    """A loaded qmc_* C-ABI library."""
+
+    def __init__(self, path=None, prefix='qmc_', extra=None):
+        path = path or DEFAULT_LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError('%s not built; run miniqmc_b200/build.py (or __graft_entry__.build())'
+                                    % path)
+        self.path = path
+        self.prefix = prefix
+        self.lib = C.CDLL(path)
+        if extra is None and prefix == 'qmc_':
+            extra = capi.PRODUCT_ONLY
+        self.fn = capi.bind(self.lib, prefix, extra)
+
+    def call(self, name, *args):
+        st = self.fn[name](*args)
+        if st != capi.QMC_OK:
+            detail = ''
+            if 'last_error' in self.fn:
+                detail = (self.fn['last_error']() or b'').decode()
+            raise QMCError(st, self.prefix + name, detail)
+        return st
+
+    def has(self, name):
+        return name in self.fn
+
+    # ---- builders --------------------------------------------------------
+    def nio(self, cell=capi.NIO_PRIM4, tiling=(1, 1, 1), quirks=0):
+        n = C.c_int()
+        self.call('nio_count', cell, tiling[0], tiling[1], tiling[2], C.byref(n))
+        lat = np.zeros(9)
+        spo_lat = np.zeros(9)
+        pos = np.zeros((n.value, 3))
+        grp = np.zeros(n.value, dtype=np.int32)
+        ng = C.c_int()
+        st = self.fn['nio_build'](cell, tiling[0], tiling[1], tiling[2], quirks, _pd(lat), _pd(pos), _pi(grp),
+                                  C.byref(ng), _pd(spo_lat))
+        if st < 0:
+            raise QMCError(-st, 'nio_build')
+        return dict(lattice=lat, ion_pos=pos, ion_group=grp, n_groups=ng.value, spo_lattice=spo_lat)
+
+    def functor(self, n_params, rcut, cusp, params):
+        f = capi.Functor()
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self.call('functor_setup', n_params, rcut, cusp, _pd(p), C.byref(f))
+        return f
+
+    def nio_jastrows(self, lattice):
+        fs = [capi.Functor() for _ in range(4)]
+        lat = np.ascontiguousarray(lattice, dtype=np.float64)
+        self.call('nio_jastrows', _pd(lat), *[C.byref(f) for f in fs])
+        return dict(j1=[fs[0], fs[1]], j2_uu=fs[2], j2_ud=fs[3])
+
+    def ws_radius(self, lattice):
+        ws = C.c_double()
+        lat = np.ascontiguousarray(lattice, dtype=np.float64)
+        self.call('lattice_ws_radius', _pd(lat), C.byref(ws))
+        return ws.value
+
+
+def synthetic_jastrows(lib, lattice, n_ion_groups=2, seed=13, n_params=8):
+    """Jastrows of the synthetic NiO configurations: n_params knot values
+    uniform in [-0.1, 0.1) from SplitMix64(seed), cutoff = half the
+    Wigner-Seitz radius, cusps 0 (J2) and -0.25 (J1) as the reference's
+    tables use."""
+    rc = 0.5 * lib.ws_radius(lattice)
+    rs = np.random.Generator(np.random.PCG64(seed))
+    def knots():
+        return rs.uniform(-0.1, 0.1, n_params)
+    j2_uu = lib.functor(n_params, rc, 0.0, knots())
+    j2_ud = lib.functor(n_params, rc, 0.0, knots())
+    j1 = [lib.functor(n_params, rc, -0.25, knots()) for _ in range(n_ion_groups)]
+    return dict(j1=j1, j2_uu=j2_uu, j2_ud=j2_ud)
+
+
+class SystemSpec:
+    """Host description of one system (qmc_system_desc plus the arrays it
+    points to, kept alive here)."""
+
+    def __init__(self, lib, cell=capi.NIO_PRIM4, tiling=(1, 1, 1), quirks=0, grid=(37, 37, 37),
+                 fill=capi.FILL_UNIFORM, spo_seed=11, jastrow='reference', components=capi.WF_ALL,
+                 lap_mode=capi.LAP_HXX, user_coefs=None, n_orb=None):
+        ions = lib.nio(cell, tiling, quirks)
+        self.ions = ions
+        n_ions = len(ions['ion_group'])
+        n_elec = 12 * n_ions  # count_electrons (nio.hpp:16-20)
+        self.n_elec = n_elec
+        self.n_up = n_elec // 2
+        self.n_orb = n_orb or self.n_up
+        self.n_ions = n_ions
+        self.grid = tuple(grid)
+        d = capi.SystemDesc()
+        d.lattice[:] = ions['lattice']
+        d.n_ions = n_ions
+        d.n_ion_groups = ions['n_groups']
+        self._pos = np.ascontiguousarray(ions['ion_pos'])
+        self._grp = np.ascontiguousarray(ions['ion_group'], dtype=np.int32)
+        d.ion_pos = _pd(self._pos)
+        d.ion_group = _pi(self._grp)
+        d.n_elec = n_elec
+        d.n_up = self.n_up
+        d.spo_lattice[:] = ions['spo_lattice']
+        d.grid[:] = grid
+        d.n_orb = self.n_orb
+        d.spo_fill = fill
+        d.spo_seed = spo_seed
+        self._coefs = None
+        if user_coefs is not None:
+            self._coefs = np.ascontiguousarray(user_coefs, dtype=np.float64)
+            d.spo_user_coefs = _pd(self._coefs)
+        d.lap_mode = lap_mode
+        d.components = components
+        if jastrow == 'reference':
+            js = lib.nio_jastrows(ions['lattice'])
+        else:
+            js = synthetic_jastrows(lib, ions['lattice'], ions['n_groups'])
+        for g in range(min(len(js['j1']), capi.MAX_ION_GROUPS)):
+            d.j1[g] = js['j1'][g]
+        d.j2_uu = js['j2_uu']
+        d.j2_ud = js['j2_ud']
+        self.desc = d
+        self.jastrows = js
+
+
+class System:
+    def __init__(self, lib, spec, precision=capi.PREC_FP64):
+        self.lib = lib
+        self.spec = spec
+        self.precision = precision
+        h = C.c_void_p()
+        lib.call('system_create', C.byref(spec.desc), precision, C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call('system_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def spo_vgh(self, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n, norb = len(pos), self.spec.n_orb
+        v = np.zeros((n, norb))
+        g = np.zeros((n, 3, norb))
+        h = np.zeros((n, 6, norb))
+        self.lib.call('spo_evaluate_vgh', self.h, n, _pd(pos), _pd(v), _pd(g), _pd(h))
+        return v, g, h
+
+    def spo_v(self, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        v = np.zeros((len(pos), self.spec.n_orb))
+        self.lib.call('spo_evaluate_v', self.h, len(pos), _pd(pos), _pd(v))
+        return v
+
+
+class Walkers:
+    """A batch of W walkers of one system (device-resident in the product)."""
+
+    def __init__(self, system, n_walkers, delay_rank=1):
+        self.sys = system
+        self.lib = system.lib
+        self.W = n_walkers
+        self.k = delay_rank
+        self.N = system.spec.n_elec
+        h = C.c_void_p()
+        self.lib.call('walkers_create', system.h, n_walkers, delay_rank, C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call('walkers_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_random(self, seeds):
+        s = np.ascontiguousarray(seeds, dtype=np.uint32)
+        self.lib.call('walkers_init_random', self.h, s.ctypes.data_as(C.POINTER(C.c_uint32)))
+
+    def positions(self):
+        R = np.zeros((self.W, self.N, 3))
+        self.lib.call('walkers_get_positions', self.h, _pd(R))
+        return R
+
+    def set_positions(self, R):
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        self.lib.call('walkers_set_positions', self.h, _pd(R))
+
+    # ParticleSet
+    def make_move(self, iat, displ):
+        d = np.ascontiguousarray(displ, dtype=np.float64).reshape(self.W, 3)
+        self.lib.call('pset_make_move', self.h, iat, _pd(d))
+
+    def accept_reject(self, iat, accept):
+        a = np.ascontiguousarray(accept, dtype=np.int32)
+        self.lib.call('pset_accept_reject', self.h, iat, _pi(a))
+
+    def temp_rows(self):
+        I = self.sys.spec.n_ions
+        aa_r = np.zeros((self.W, self.N))
+        aa_dr = np.zeros((self.W, self.N, 3))
+        ab_r = np.zeros((self.W, I))
+        ab_dr = np.zeros((self.W, I, 3))
+        self.lib.call('pset_get_temp_rows', self.h, _pd(aa_r), _pd(aa_dr), _pd(ab_r), _pd(ab_dr))
+        return aa_r, aa_dr, ab_r, ab_dr
+
+    # WaveFunction
+    def evaluate_log(self):
+        out = np.zeros(self.W)
+        self.lib.call('wf_evaluate_log', self.h, _pd(out))
+        return out
+
+    def eval_grad(self, iat):
+        g = np.zeros((self.W, 3))
+        self.lib.call('wf_eval_grad', self.h, iat, _pd(g))
+        return g
+
+    def ratio_grad(self, iat):
+        r = np.zeros(self.W)
+        g = np.zeros((self.W, 3))
+        self.lib.call('wf_ratio_grad', self.h, iat, _pd(r), _pd(g))
+        return r, g
+
+    def ratio(self, iat):
+        r = np.zeros(self.W)
+        self.lib.call('wf_ratio', self.h, iat, _pd(r))
+        return r
+
+    def accept_restore(self, iat, accept):
+        a = np.ascontiguousarray(accept, dtype=np.int32)
+        self.lib.call('wf_accept_restore', self.h, iat, _pi(a))
+
+    def complete_updates(self):
+        self.lib.call('wf_complete_updates', self.h)
+
+    def evaluate_gl(self):
+        G = np.zeros((self.W, self.N, 3))
+        L = np.zeros((self.W, self.N))
+        lp = np.zeros(self.W)
+        self.lib.call('wf_evaluate_gl', self.h, _pd(G), _pd(L), _pd(lp))
+        return G, L, lp
+
+    def components(self):
+        c = np.zeros((self.W, 6))
+        self.lib.call('wf_components', self.h, _pd(c))
+        return c
+
+    def inverse(self, walker, spin):
+        n = self.sys.spec.n_orb
+        m = np.zeros((n, n))
+        self.lib.call('wf_get_inverse', self.h, walker, spin, _pd(m))
+        return m
+
+    def sweep(self, n_steps=1, n_substeps=1, accept=0.5, ur=None, delta=None, recompute_every=0,
+              trace=False):
+        o = capi.SweepOpts()
+        o.n_steps = n_steps
+        o.n_substeps = n_substeps
+        o.accept = accept
+        keep = []
+        if ur is not None:
+            o.rng_mode = capi.RNG_HOST
+            ur = np.ascontiguousarray(ur, dtype=np.float64)
+            delta = np.ascontiguousarray(delta, dtype=np.float64)
+            keep += [ur, delta]
+            o.ur = _pd(ur)
+            o.delta = _pd(delta)
+        else:
+            o.rng_mode = capi.RNG_DEVICE
+        o.recompute_every = recompute_every
+        tr = None
+        if trace:
+            tr = np.zeros((n_steps, self.W, n_substeps, self.N, 8))
+            o.trace = _pd(tr)
+        acc = np.zeros(self.W, dtype=np.int64)
+        lp = np.zeros(self.W)
+        o.n_accepted = acc.ctypes.data_as(C.POINTER(C.c_int64))
+        o.logpsi = _pd(lp)
+        self.lib.call('sweep', self.h, C.byref(o))
+        return dict(accepted=acc, logpsi=lp, trace=tr)
+
+
+class DetEngine:
+    """DelayedUpdate + DiracMatrix on one n x n inverse (DelayedUpdate.h:28-231)."""
+
+    def __init__(self, lib, n, delay):
+        self.lib = lib
+        self.n = n
+        h = C.c_void_p()
+        lib.call('detengine_create', n, delay, C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call('detengine_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def invert_transpose(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        lg, ph = C.c_double(), C.c_double()
+        self.lib.call('detengine_invert_transpose', self.h, _pd(a), C.byref(lg), C.byref(ph))
+        return lg.value, ph.value
+
+    def get_inv_row(self, row):
+        r = np.zeros(self.n)
+        self.lib.call('detengine_get_inv_row', self.h, row, _pd(r))
+        return r
+
+    def accept_row(self, row, psiv):
+        p = np.ascontiguousarray(psiv, dtype=np.float64)
+        self.lib.call('detengine_accept_row', self.h, row, _pd(p))
+
+    def update_inv_mat(self):
+        self.lib.call('detengine_update_inv_mat', self.h)
+
+    def ainv(self):
+        m = np.zeros((self.n, self.n))
+        self.lib.call('detengine_get_ainv', self.h, _pd(m))
+        return m

@@ -1,0 +1,31 @@
+# Compiles the reference's own sources (from /root/reference/src, read-only)
+# with the golden-dump driver oracle/ref_harness.cpp into oracle/_ref/.
+# Test infrastructure only: not the reference's CMake build, no external
+# libraries; the hand-written oracle/ref_harness_config.h replaces the
+# CMake-generated config.h.
+REF ?= /root/reference/src
+HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
+OUT := $(HERE)_ref
+REF_CXX ?= $(shell test -x /usr/bin/g++ && echo /usr/bin/g++ || echo g++)
+# the reference's plain FP64 build flags (no -ffast-math)
+FLAGS := -O2 -std=c++11 -fopenmp -ffp-contract=off -w -Drestrict=__restrict__ -DHAVE_CONFIG_H -DADD_ -D__forceinline=inline -fomit-frame-pointer -fstrict-aliasing -include cstdint -I$(OUT)/include -I$(REF)
+SRCS := $(REF)/Particle/ParticleSet.cpp $(REF)/Particle/ParticleSet.BC.cpp \
+        $(REF)/Particle/DistanceTableAA.cpp $(REF)/Particle/DistanceTableAB.cpp \
+        $(REF)/Particle/ParticleSet_builder.cpp $(REF)/Utilities/SpeciesSet.cpp \
+        $(REF)/Utilities/NewTimer.cpp $(REF)/Utilities/OutputManager.cpp \
+        $(REF)/Utilities/InfoStream.cpp $(REF)/Utilities/XMLWriter.cpp \
+        $(REF)/Utilities/tinyxml/tinyxml2.cpp
+
+all: $(OUT)/ref_harness
+
+$(OUT)/include/config.h: $(HERE)ref_harness_config.h
+	mkdir -p $(OUT)/include
+	cp $< $@
+
+$(OUT)/ref_harness: $(HERE)ref_harness.cpp $(OUT)/include/config.h
+	$(REF_CXX) $(FLAGS) -o $@ $(HERE)ref_harness.cpp $(SRCS)
+
+clean:
+	rm -rf $(OUT)
+
+.PHONY: all clean
