@@ -1,0 +1,317 @@
+"""Benchmark: electron-moves/s of the VMC PbyP sweep on NiO-128.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): NiO tiled 4x4x2 from the 4-atom cell -- 128 atoms,
+1536 electrons, 768 orbitals per spin -- B-spline grid 148x148x74 with FP32
+coefficients (5.4 GB), 512 walkers, delay rank 32, mixed precision.  One
+"step" is one MC step of miniqmc's driver loop over the whole batch: 1536
+single-electron moves per walker (evalGrad, makeMove, ratioGrad, threshold
+accept, delayed Woodbury flushes, completeUpdates) then evaluateGL.  Inputs
+are synthetic (uniform spline coefficients from SplitMix64 seed 11,
+synthetic Jastrows, electrons from each walker's mt19937 stream).
+
+value: device-timed (CUDA events on the launching stream, max over ranks)
+whole-job moves/s with walker state resident in HBM.  e2e: the same metric
+through the public C ABI (qmc_sweep) with the random streams supplied from
+pinned host memory each step and the accept counts and log values read
+back, wall-clock timed.  Multi-GPU: walkers are independent, so each rank
+runs its own replica batch (weak scaling, no collective on the data path).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+MEASURED_PEAKS = os.path.join(REPO, 'MEASURED_PEAKS.json')
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--tiling', default='4,4,2')
+    ap.add_argument('--grid', default='148,148,74')
+    ap.add_argument('--walkers', type=int, default=512)
+    ap.add_argument('--delay', type=int, default=32)
+    ap.add_argument('--precision', default='mixed', choices=['mixed', 'fp64'])
+    ap.add_argument('--recompute-every', type=int, default=0)
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--cpu-walkers', type=int, default=0)
+    return ap.parse_args()
+
+
+def algorithmic_bytes_per_move(n, N, I, k, s, a):
+    """Algorithmic HBM bytes of one electron move (evalGrad + ratioGrad +
+    accept bookkeeping + amortised Woodbury flush), with n orbitals per spin,
+    N electrons, I ions, delay k, element size s and acceptance a:
+      64n (SPO stencil) + (k/2+1)n (Ainv row and U/V rows of getInvRow)
+      + 3n (dpsiM row) + 3N + 3I (positions for the AA and AB rows)
+      + a(14N + 6n) (J2 arrays read+write, U/V and dpsiM/d2psiM row writes)
+      + a(2n^2/k + 2n) (Ainv read+write per flush, amortised)."""
+    return s * (64 * n + (k / 2 + 1) * n + 3 * n + 3 * N + 3 * I + a * (14 * N + 6 * n) +
+                a * (2 * n * n / k + 2 * n))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.Q,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == 'active':
+                        reasons.add(nm)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(MEASURED_PEAKS)), 'measured'
+    except Exception:
+        return {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0}, 'fallback'
+
+
+def build_workload(lib, args, capi, api, device_rng_seeds):
+    tiling = tuple(int(x) for x in args.tiling.split(','))
+    grid = tuple(int(x) for x in args.grid.split(','))
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=grid, fill=capi.FILL_UNIFORM, spo_seed=11,
+                          jastrow='synthetic')
+    prec = capi.PREC_MIXED if args.precision == 'mixed' else capi.PREC_FP64
+    system = api.System(lib, spec, prec)
+    walkers = api.Walkers(system, args.walkers, args.delay)
+    walkers.init_random(device_rng_seeds)
+    return spec, system, walkers
+
+
+def cpu_baseline(args, n_threads, sample_walkers):
+    """The CPU FP64 oracle (a port of the reference algorithm) on the host
+    cores: `sample_walkers` walkers (one per thread) for one substep of the
+    same system on a coarser grid (same per-move work: 64 stencil points x
+    768 orbitals); returns electron-moves/s."""
+    from miniqmc_b200 import api, capi
+    from tests import oracle_lib
+    lib = oracle_lib.library()
+    tiling = tuple(int(x) for x in args.tiling.split(','))
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=(37, 37, 18), fill=capi.FILL_UNIFORM,
+                          spo_seed=11, jastrow='synthetic')
+    system = api.System(lib, spec, capi.PREC_FP64)
+    w = api.Walkers(system, sample_walkers, args.delay)
+    seeds = np.arange(sample_walkers, dtype=np.uint32) + 7
+    w.init_random(seeds)
+    w.evaluate_log()
+    t0 = time.perf_counter()
+    w.sweep(1, 1, 0.5)
+    dt = time.perf_counter() - t0
+    moves = sample_walkers * spec.n_elec
+    return moves / dt, ('%d walkers x 1 substep x %d electrons of NiO %s (FP64 oracle port, grid 37x37x18, k=%d)'
+                        % (sample_walkers, spec.n_elec, args.tiling, args.delay))
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ncpu = os.cpu_count() or 1
+    os.environ.setdefault('OMP_NUM_THREADS', str(ncpu))
+    sample = args.cpu_walkers or ncpu
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(args, ncpu, sample)
+    for _ in range(args.steps):
+        v, desc = cpu_baseline(args, ncpu, sample)
+        vals.append(v)
+    v = float(np.mean(vals))
+    tiling = args.tiling
+    print(json.dumps({
+        'impl': 'reference', 'metric': 'electron-moves/s', 'value': v, 'unit': 'electron-moves/s',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': 'NiO %s (4-atom cell), 1536 e-, k=%d' % (tiling, args.delay)},
+        'cpu_baseline': {'value': v, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'port', 'sample': desc},
+        'e2e': {'value': v, 'unit': 'electron-moves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+        'note': 'the reference needs an external BLAS/LAPACK and CMake; its algorithm is timed as the CPU oracle port'
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    from miniqmc_b200 import api, capi
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group('nccl', timeout=__import__('datetime').timedelta(seconds=600))
+    lib = api.Library()
+    lib.call('init', local)
+    seeds = (np.arange(args.walkers, dtype=np.uint32) * 7919 + 1009 * (rank + 1)).astype(np.uint32)
+    spec, system, walkers = build_workload(lib, args, capi, api, seeds)
+    stream = torch.cuda.Stream()
+    lib.call('walkers_set_stream', walkers.h, C.c_void_p(stream.cuda_stream))
+    walkers.evaluate_log()
+    W, N = args.walkers, spec.n_elec
+    count = C.c_int64()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (device RNG, fully resident)
+    for _ in range(args.warmup):
+        lib.call('sweep_async', walkers.h, 1, 1, 0.5, args.recompute_every)
+    lib.call('walkers_sync', walkers.h)
+    lib.call('walkers_launch_count', walkers.h, C.byref(count))
+    launches0 = count.value
+    acc0 = np.zeros(W, dtype=np.int64)
+    lib.call('sweep_results', walkers.h, acc0.ctypes.data_as(C.POINTER(C.c_int64)), None)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    with torch.cuda.stream(stream):
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for s in range(args.steps):
+            ev[s][0].record(stream)
+            lib.call('sweep_async', walkers.h, 1, 1, 0.5, args.recompute_every)
+            ev[s][1].record(stream)
+        t_all1.record(stream)
+    lib.call('walkers_sync', walkers.h)
+    barrier()
+    clk = clocks.stop()
+    ms_total = t_all0.elapsed_time(t_all1)
+    kernel_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    acc = np.zeros(W, dtype=np.int64)
+    lib.call('sweep_results', walkers.h, acc.ctypes.data_as(C.POINTER(C.c_int64)), None)
+    lib.call('walkers_launch_count', walkers.h, C.byref(count))
+    launches = count.value - launches0
+    t = torch.tensor([ms_total], device='cuda')
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total = float(t.item())
+    moves = W * N * args.steps * world
+    value = moves / (ms_total / 1e3)
+    a = float((acc - acc0).sum()) / (W * N * args.steps)
+
+    # e2e through the public API: host random streams in, results out
+    e2e = None
+    if not args.no_e2e:
+        pin = torch.empty((2, W, 1, N, 4), dtype=torch.float64, pin_memory=True)
+        rs = np.random.default_rng(5 + rank)
+        urb = pin[0, :, :, :, 0].numpy()
+        ur = np.ascontiguousarray(rs.uniform(size=(1, W, 1, N)))
+        de = np.ascontiguousarray(rs.normal(size=(1, W, 1, N, 3)))
+        pin_ur = torch.from_numpy(ur).pin_memory().numpy()
+        pin_de = torch.from_numpy(de).pin_memory().numpy()
+        walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de)  # warm
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de)
+        barrier()
+        dt = time.perf_counter() - t0
+        tt = torch.tensor([dt], device='cuda')
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = {'value': W * N * args.steps * world / float(tt.item()), 'unit': 'electron-moves/s',
+               'h2d_bytes_per_step': int(ur.nbytes + de.nbytes), 'd2h_bytes_per_step': int(W * 16)}
+
+    pk, pk_kind = peaks()
+    n, I, k = spec.n_orb, spec.n_ions, args.delay
+    s = 4 if args.precision == 'mixed' else 8
+    bpm = algorithmic_bytes_per_move(n, N, I, k, s, a)
+    avg_launch_ms = float(np.mean(kernel_ms))
+    achieved = bpm * W * N / (avg_launch_ms / 1e3) / 1e9
+    roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+                'frac': achieved / pk['hbm_gbs'], 'traffic': None,
+                'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm, 'kernel': 'sweep_kernel<float>'}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ncpu = os.cpu_count() or 1
+        try:
+            v, desc = cpu_baseline(args, ncpu, args.cpu_walkers or ncpu)
+            cpu = {'value': v, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'port', 'sample': desc}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {'value': None, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'port',
+                   'sample': 'failed: %s' % ex}
+    if rank == 0:
+        out = {
+            'metric': 'electron-moves/s', 'value': value, 'unit': 'electron-moves/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_total / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32' if args.precision == 'mixed' else 'f64', 'data': 'synthetic',
+            'config': {'workload': 'NiO %s of the 4-atom cell: %d atoms, %d e-, %d orbitals/spin, grid %s '
+                                   'FP32 table, %d walkers/GPU, delay %d, %s'
+                                   % (args.tiling, I, N, n, args.grid, W, k, args.precision),
+                       'walkers_per_gpu': W, 'l2': 'inputs larger than L2 (5.4 GB spline table, '
+                                                    '%.1f GB walker state)' % (walkers_bytes(lib, walkers) / 1e9),
+                       'acceptance': a, 'parallelism': 'replicas x%d' % world},
+            'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk,
+            'gpu_launches': launches,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def walkers_bytes(lib, walkers):
+    b = C.c_size_t()
+    lib.call('walkers_bytes', walkers.h, C.byref(b))
+    return b.value
+
+
+if __name__ == '__main__':
+    main()

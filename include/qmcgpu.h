@@ -148,6 +148,12 @@ int qmc_nio_jastrows(const double* lattice, qmc_functor* j1_O, qmc_functor* j1_N
 /* BsplineFunctor::setupParameters(n_params, rcut, cusp, params). */
 int qmc_functor_setup(int n_params, double rcut, double cusp, const double* params,
                       qmc_functor* out);
+/* Synthetic Jastrows of the NiO workloads (no reference counterpart): knot
+ * values uniform in [-0.1, 0.1) from SplitMix64(seed, 64 f + i) for functor
+ * f = 0 (uu), 1 (ud), 2 + g (ion species g); cutoff = half the
+ * Wigner-Seitz radius of `lattice`; cusp 0 for J2 and -0.25 for J1. */
+int qmc_synthetic_jastrows(const double* lattice, int n_groups, uint64_t seed, int n_params,
+                           qmc_functor* j1, qmc_functor* j2_uu, qmc_functor* j2_ud);
 /* Wigner-Seitz radius of a periodic cell (CrystalLattice.cpp:118-125). */
 int qmc_lattice_ws_radius(const double* lattice, double* ws);
 
@@ -254,6 +260,22 @@ int qmc_walkers_sync(qmc_walkers* w);
 int qmc_sweep_results(qmc_walkers* w, int64_t* n_accepted, double* logpsi);
 /* Number of CUDA kernel launches this batch issued since creation. */
 int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count);
+
+/* DelayedUpdate + DiracMatrix on one n x n inverse, FP64 on the device
+ * (DelayedUpdate.h:28-231, DiracMatrix.h:59-121): the object the reference's
+ * unit tests drive with fake orbital rows (test_dirac_matrix.cpp,
+ * test_dirac_det.cpp). */
+typedef struct qmc_detengine_s qmc_detengine;
+int qmc_detengine_create(int n, int delay, qmc_detengine** out);
+int qmc_detengine_destroy(qmc_detengine* e);
+/* DiracMatrix::invert_transpose(logdetT = a): psiM = (a^{-1})^T, log|det a|
+ * and its phase (0 or pi). */
+int qmc_detengine_invert_transpose(qmc_detengine* e, const double* a, double* logdet,
+                                   double* phase);
+int qmc_detengine_get_inv_row(qmc_detengine* e, int row, double* inv_row);
+int qmc_detengine_accept_row(qmc_detengine* e, int row, const double* psiv);
+int qmc_detengine_update_inv_mat(qmc_detengine* e);
+int qmc_detengine_get_ainv(qmc_detengine* e, double* ainv);
 
 #ifdef __cplusplus
 }

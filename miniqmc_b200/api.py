@@ -101,18 +101,31 @@ class Library:
         return ws.value
 
 
+_M64 = (1 << 64) - 1
+
+
+def splitmix_uniform(seed, index):
+    """SplitMix64 (Steele, Lea & Flood 2014) mapped to [0,1) with 53 bits."""
+    z = (seed + (index + 1) * 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    z ^= z >> 31
+    return (z >> 11) * (1.0 / 9007199254740992.0)
+
+
 def synthetic_jastrows(lib, lattice, n_ion_groups=2, seed=13, n_params=8):
-    """Jastrows of the synthetic NiO configurations: n_params knot values
-    uniform in [-0.1, 0.1) from SplitMix64(seed), cutoff = half the
-    Wigner-Seitz radius, cusps 0 (J2) and -0.25 (J1) as the reference's
-    tables use."""
+    """Jastrows of the synthetic NiO workloads (same values as the C entry
+    point qmc_synthetic_jastrows): knot i of functor f is uniform in
+    [-0.1, 0.1) from SplitMix64(seed, 64 f + i), f = 0 (uu), 1 (ud), 2 + g
+    (ion species g); cutoff = half the Wigner-Seitz radius; cusp 0 (J2) and
+    -0.25 (J1) as the reference's tables."""
     rc = 0.5 * lib.ws_radius(lattice)
-    rs = np.random.Generator(np.random.PCG64(seed))
-    def knots():
-        return rs.uniform(-0.1, 0.1, n_params)
-    j2_uu = lib.functor(n_params, rc, 0.0, knots())
-    j2_ud = lib.functor(n_params, rc, 0.0, knots())
-    j1 = [lib.functor(n_params, rc, -0.25, knots()) for _ in range(n_ion_groups)]
+
+    def knots(f):
+        return [0.2 * splitmix_uniform(seed, 64 * f + i) - 0.1 for i in range(n_params)]
+    j2_uu = lib.functor(n_params, rc, 0.0, knots(0))
+    j2_ud = lib.functor(n_params, rc, 0.0, knots(1))
+    j1 = [lib.functor(n_params, rc, -0.25, knots(2 + g)) for g in range(n_ion_groups)]
     return dict(j1=j1, j2_uu=j2_uu, j2_ud=j2_ud)
 
 

@@ -1,0 +1,1198 @@
+// api.cu -- the C ABI (include/qmcgpu.h): handles, device memory, launches.
+//
+// Host side of the drop-in boundary.  Every entry point returns a status and
+// records a message retrievable with qmc_last_error(); nothing here exits the
+// process.  All compute runs in the kernels of sweep.cu / others.cu; there
+// is no host fallback for any hot-path operation.
+#include "host_lattice.hpp"
+#include "kernels.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace qmc;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg)
+{
+  g_err = msg;
+  return code;
+}
+#define CK(call)                                                                                          \
+  do                                                                                                      \
+  {                                                                                                       \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? QMC_ERR_OOM : QMC_ERR_CUDA,                           \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                                    \
+  } while (0)
+
+struct qmc_system_s
+{
+  DevSystem h;          // host mirror with device pointers
+  DevSystem* d = nullptr;
+  bool fp32    = false;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+};
+
+struct qmc_walkers_s
+{
+  qmc_system* sys = nullptr;
+  DevWalkers dw{};
+  bool fp32   = false;
+  int threads = 128;
+  cudaStream_t stream = nullptr;
+  bool own_stream     = false;
+  std::vector<void*> allocs;
+  size_t bytes      = 0;
+  int64_t launches  = 0;
+  SweepTask* d_task = nullptr;
+  double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;
+  size_t cap_rng = 0, cap_trace = 0;
+  double* d_displ = nullptr;
+  int* d_flags    = nullptr;
+  double* d_rows  = nullptr;
+  size_t cap_rows = 0;
+};
+
+template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes, P** p, size_t count)
+{
+  *p = nullptr;
+  if (count == 0)
+    count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(P));
+  if (e != cudaSuccess)
+    return fail(QMC_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  e = cudaMemset(*p, 0, count * sizeof(P));
+  if (e != cudaSuccess)
+    return fail(QMC_ERR_CUDA, cudaGetErrorString(e));
+  list.push_back((void*)*p);
+  bytes += count * sizeof(P);
+  return QMC_OK;
+}
+
+static int device_status(qmc_walkers* w)
+{
+  unsigned st = 0;
+  CK(cudaMemcpyAsync(&st, w->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  if (st)
+  {
+    CK(cudaMemsetAsync(w->dw.status, 0, sizeof(unsigned), w->stream));
+    if (st & DEV_ERR_SINGULAR)
+      return fail(QMC_ERR_SINGULAR, "zero pivot in the FP64 inverse of a Slater matrix");
+    if (st & DEV_ERR_NONFINITE)
+      return fail(QMC_ERR_NONFINITE, "non-finite wavefunction ratio");
+    if (st & DEV_ERR_STATE)
+      return fail(QMC_ERR_STATE, "move protocol violated (no proposed move for this electron)");
+    return fail(QMC_ERR_CUDA, "device error bits set");
+  }
+  return QMC_OK;
+}
+
+extern "C" {
+
+const char* qmc_status_string(int s)
+{
+  switch (s)
+  {
+  case QMC_OK: return "QMC_OK";
+  case QMC_ERR_ARG: return "QMC_ERR_ARG";
+  case QMC_ERR_CUDA: return "QMC_ERR_CUDA";
+  case QMC_ERR_OOM: return "QMC_ERR_OOM";
+  case QMC_ERR_SINGULAR: return "QMC_ERR_SINGULAR";
+  case QMC_ERR_NONFINITE: return "QMC_ERR_NONFINITE";
+  case QMC_ERR_TIMEOUT: return "QMC_ERR_TIMEOUT";
+  case QMC_ERR_STATE: return "QMC_ERR_STATE";
+  case QMC_ERR_NODEVICE: return "QMC_ERR_NODEVICE";
+  case QMC_ERR_ADMISSION: return "QMC_ERR_ADMISSION";
+  default: return "QMC_ERR_UNKNOWN";
+  }
+}
+const char* qmc_last_error(void) { return g_err.c_str(); }
+
+int qmc_init(int device)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(QMC_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= n)
+    return fail(QMC_ERR_ARG, "device index out of range");
+  CK(cudaSetDevice(device));
+  cudaDeviceProp p;
+  CK(cudaGetDeviceProperties(&p, device));
+  if (p.major != 10)
+    return fail(QMC_ERR_NODEVICE, "library built for sm_100a; device is sm_" + std::to_string(p.major) +
+                                      std::to_string(p.minor));
+  return QMC_OK;
+}
+
+// -------------------------------------------------------------- builders --
+int qmc_nio_count(int cell, int na, int nb, int nc, int* n_ions)
+{
+  if (!n_ions || na < 1 || nb < 1 || nc < 1)
+    return fail(QMC_ERR_ARG, "bad tiling");
+  *n_ions = (cell == QMC_NIO_REF32 ? 32 : 4) * na * nb * nc;
+  return QMC_OK;
+}
+int qmc_nio_build(int cell, int na, int nb, int nc, int quirks, double* lattice, double* ion_pos, int* ion_group,
+                  int* n_groups, double* spo_lattice)
+{
+  if (!lattice || !ion_pos || !ion_group || !n_groups || !spo_lattice || na < 1 || nb < 1 || nc < 1)
+    return fail(QMC_ERR_ARG, "bad arguments to qmc_nio_build");
+  qmc_host::Ions s = cell == QMC_NIO_REF32 ? qmc_host::nio_ref32(na, nb, nc, quirks) : qmc_host::nio_prim4(na, nb, nc);
+  std::memcpy(lattice, s.lattice, sizeof(s.lattice));
+  std::memcpy(spo_lattice, s.spo_lattice, sizeof(s.spo_lattice));
+  std::copy(s.pos.begin(), s.pos.end(), ion_pos);
+  std::copy(s.group.begin(), s.group.end(), ion_group);
+  *n_groups = s.n_groups;
+  return QMC_OK;
+}
+int qmc_functor_setup(int n_params, double rcut, double cusp, const double* params, qmc_functor* out)
+{
+  int st = qmc_host::functor_setup(n_params, rcut, cusp, params, out);
+  return st ? fail(st, "bad functor parameters") : QMC_OK;
+}
+int qmc_lattice_ws_radius(const double* lattice, double* ws)
+{
+  if (!lattice || !ws)
+    return fail(QMC_ERR_ARG, "null pointer");
+  *ws = qmc_host::ws_radius(lattice);
+  return QMC_OK;
+}
+int qmc_nio_jastrows(const double* lattice, qmc_functor* j1_O, qmc_functor* j1_Ni, qmc_functor* j2_uu,
+                     qmc_functor* j2_ud)
+{
+  if (!lattice || !j1_O || !j1_Ni || !j2_uu || !j2_ud)
+    return fail(QMC_ERR_ARG, "null pointer");
+  const double ws       = qmc_host::ws_radius(lattice);
+  const double Yuu[10]  = {0.3062333936,  0.2068358231,  0.1324267459,  0.08673342451,  0.05641590391,
+                          0.03626533946, 0.02269217959, 0.01331043612, 0.006750919735, 0.002827476478};
+  const double Yud[10]  = {0.4397856796,  0.2589475889,  0.1516634434,  0.08962897215, 0.05676614496,
+                          0.03675758961, 0.02294244601, 0.01343860721, 0.00681803725, 0.002864695148};
+  const double YO[10]   = {-1.060468469,   -0.9741652012,  -0.8785027166, -0.6350075366,  -0.3276892194,
+                         -0.08646817952, -0.07340983171, -0.0377479213, -0.01507835571, -0.001101691898};
+  const double YNi[10]  = {-3.058259288,  -3.077898004,  -2.51188807,   -1.570208063,  -0.6204423266,
+                          0.06272826611, 0.06228214399, 0.06665099211, 0.03230352443, 0.009254036239};
+  const double rc2 = std::min(ws, 5.5727792532), rc1 = std::min(ws, 4.8261684030);
+  qmc_host::functor_setup(10, rc2, 0.0, Yuu, j2_uu);
+  qmc_host::functor_setup(10, rc2, 0.0, Yud, j2_ud);
+  qmc_host::functor_setup(10, rc1, -0.25, YO, j1_O);
+  qmc_host::functor_setup(10, rc1, -0.25, YNi, j1_Ni);
+  return QMC_OK;
+}
+
+// The synthetic Jastrows of the NiO workloads: n_params knot values per
+// functor, uniform in [-0.1, 0.1) from SplitMix64(seed, 64*f + i) with
+// f = 0 (uu), 1 (ud), 2.. (one per ion species); cutoff = half the
+// Wigner-Seitz radius; cusp 0 (J2) and -0.25 (J1) as the reference tables.
+int qmc_synthetic_jastrows(const double* lattice, int n_groups, uint64_t seed, int n_params, qmc_functor* j1,
+                           qmc_functor* j2_uu, qmc_functor* j2_ud)
+{
+  if (!lattice || !j1 || !j2_uu || !j2_ud || n_groups < 1 || n_groups > QMC_MAX_ION_GROUPS || n_params < 2 ||
+      n_params + 4 > QMC_MAX_FUNCTOR_COEFS)
+    return fail(QMC_ERR_ARG, "bad synthetic Jastrow arguments");
+  const double rc = 0.5 * qmc_host::ws_radius(lattice);
+  double k[QMC_MAX_FUNCTOR_COEFS];
+  auto knots = [&](int f) {
+    for (int i = 0; i < n_params; ++i)
+      k[i] = 0.2 * splitmix_uniform(seed, 64ull * f + i) - 0.1;
+  };
+  knots(0);
+  qmc_host::functor_setup(n_params, rc, 0.0, k, j2_uu);
+  knots(1);
+  qmc_host::functor_setup(n_params, rc, 0.0, k, j2_ud);
+  for (int g = 0; g < n_groups; ++g)
+  {
+    knots(2 + g);
+    qmc_host::functor_setup(n_params, rc, -0.25, k, &j1[g]);
+  }
+  return QMC_OK;
+}
+
+} // extern "C"
+
+// --------------------------------------------------------------- system --
+template <typename T>
+__global__ void fill_table_kernel(T* coefs, size_t n_points, int norb, int npad, int mode, uint64_t seed,
+                                  const double* field, const double* pref, const double* user)
+{
+  const size_t total = n_points * (size_t)npad;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+  {
+    const size_t g = e / npad;
+    const int j    = (int)(e % npad);
+    double v       = 0.0;
+    if (j < norb)
+    {
+      if (mode == QMC_FILL_UNIFORM)
+        v = splitmix_uniform(seed, g * norb + j) - 0.5;
+      else if (mode == QMC_FILL_REFERENCE)
+        v = field[g] * pref[j];
+      else
+        v = user[g * norb + j];
+    }
+    coefs[e] = (T)v;
+  }
+}
+
+extern "C" {
+
+int qmc_system_create(const qmc_system_desc* d, int precision, qmc_system** out)
+{
+  if (!d || !out)
+    return fail(QMC_ERR_ARG, "null pointer");
+  *out           = nullptr;
+  const int comp = d->components ? d->components : QMC_WF_ALL;
+  if (d->n_elec <= 0 || d->n_up < 0 || d->n_orb <= 0 || d->n_ions <= 0 || d->n_ion_groups < 1 ||
+      d->n_ion_groups > QMC_MAX_ION_GROUPS || d->grid[0] < 1 || d->grid[1] < 1 || d->grid[2] < 1 || !d->ion_pos ||
+      !d->ion_group)
+    return fail(QMC_ERR_ARG, "bad system description");
+  if ((comp & QMC_WF_DET) && (d->n_up != d->n_orb || d->n_elec - d->n_up != d->n_orb))
+    return fail(QMC_ERR_ARG, "the determinants need n_up == n_elec - n_up == n_orb");
+  if (d->spo_fill == QMC_FILL_USER && !d->spo_user_coefs)
+    return fail(QMC_ERR_ARG, "QMC_FILL_USER needs spo_user_coefs");
+  for (int i = 1; i < d->n_ions; ++i)
+    if (d->ion_group[i] < d->ion_group[i - 1])
+      return fail(QMC_ERR_ARG, "ions must be grouped by species");
+  auto* s  = new qmc_system_s;
+  s->fp32  = precision == QMC_PREC_MIXED;
+  DevSystem& h = s->h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.lattice, d->lattice, sizeof(h.lattice));
+  qmc_host::bconds(d->lattice, h.rb, h.gb, h.corners);
+  qmc_host::inverse3(d->spo_lattice, h.spoG);
+  for (int k = 0; k < 3; ++k)
+  {
+    h.grid[k]          = d->grid[k];
+    const double delta = (1.0 - 0.0) / (double)d->grid[k];
+    h.dinv[k]          = 1.0 / delta;
+  }
+  h.norb         = d->n_orb;
+  h.npad         = round_up(d->n_orb, 32);
+  h.zs           = h.npad;
+  h.ys           = (long long)(d->grid[2] + 3) * h.zs;
+  h.xs           = (long long)(d->grid[1] + 3) * h.ys;
+  h.table_fp32   = s->fp32 ? 1 : 0;
+  h.n_ions       = d->n_ions;
+  h.n_groups     = d->n_ion_groups;
+  h.n_elec       = d->n_elec;
+  h.n_up         = d->n_up;
+  h.lap_mode     = d->lap_mode;
+  h.comp         = comp;
+  for (int g = 0; g < QMC_MAX_ION_GROUPS; ++g)
+  {
+    int f = -1, l = -1;
+    for (int i = 0; i < d->n_ions; ++i)
+      if (d->ion_group[i] == g)
+      {
+        if (f < 0)
+          f = i;
+        l = i + 1;
+      }
+    h.gfirst[g] = f < 0 ? 0 : f;
+    h.glast[g]  = f < 0 ? 0 : l;
+  }
+  auto cp_functor = [](DevFunctor& o, const qmc_functor& f) {
+    o.n      = f.n_coefs;
+    o.cutoff = f.cutoff;
+    o.dinv   = f.delta_r_inv;
+    for (int c = 0; c < QMC_MAX_FUNCTOR_COEFS; ++c)
+      o.c[c] = c < f.n_coefs ? f.coefs[c] : 0.0;
+  };
+  for (int g = 0; g < QMC_MAX_ION_GROUPS; ++g)
+    cp_functor(h.j1[g], d->j1[g]);
+  cp_functor(h.j2uu, d->j2_uu);
+  cp_functor(h.j2ud, d->j2_ud);
+  // functor index (int)(r * dinv) + 3 must stay inside the coefficient table
+  // for r < cutoff: (numKnots-1) intervals + 3 < n_coefs holds by construction.
+  int st = QMC_OK;
+  const size_t npts = (size_t)(d->grid[0] + 3) * (d->grid[1] + 3) * (d->grid[2] + 3);
+  const size_t elem = s->fp32 ? 4 : 8;
+  void* coefs       = nullptr;
+  cudaError_t e     = cudaMalloc(&coefs, npts * h.npad * elem);
+  if (e != cudaSuccess)
+  {
+    delete s;
+    return fail(QMC_ERR_OOM, "spline table allocation failed: " + std::string(cudaGetErrorString(e)));
+  }
+  s->allocs.push_back(coefs);
+  s->bytes += npts * h.npad * elem;
+  h.coefs      = coefs;
+  h.coef_bytes = npts * h.npad * elem;
+  double *d_field = nullptr, *d_pref = nullptr, *d_user = nullptr;
+  if (d->spo_fill == QMC_FILL_REFERENCE)
+  {
+    std::mt19937 mt((uint32_t)d->spo_seed);
+    std::uniform_real_distribution<double> uni;
+    std::vector<double> field(npts), pref(d->n_orb);
+    for (auto& f : field)
+      f = uni(mt);
+    for (int ind = 0; ind < d->n_orb; ind++)
+      pref[ind] = std::cos(2 * M_PI * ind / d->n_orb);
+    cudaMalloc(&d_field, npts * sizeof(double));
+    cudaMalloc(&d_pref, d->n_orb * sizeof(double));
+    cudaMemcpy(d_field, field.data(), npts * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_pref, pref.data(), d->n_orb * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  else if (d->spo_fill == QMC_FILL_USER)
+  {
+    cudaMalloc(&d_user, npts * d->n_orb * sizeof(double));
+    cudaMemcpy(d_user, d->spo_user_coefs, npts * d->n_orb * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  if (s->fp32)
+    fill_table_kernel<float><<<4 * 148, 256>>>((float*)coefs, npts, d->n_orb, h.npad, d->spo_fill, d->spo_seed,
+                                              d_field, d_pref, d_user);
+  else
+    fill_table_kernel<double><<<4 * 148, 256>>>((double*)coefs, npts, d->n_orb, h.npad, d->spo_fill, d->spo_seed,
+                                               d_field, d_pref, d_user);
+  e = cudaDeviceSynchronize();
+  cudaFree(d_field);
+  cudaFree(d_pref);
+  cudaFree(d_user);
+  if (e != cudaSuccess)
+  {
+    for (void* p : s->allocs)
+      cudaFree(p);
+    delete s;
+    return fail(QMC_ERR_CUDA, std::string("spline fill: ") + cudaGetErrorString(e));
+  }
+  // ions: AoS double + SoA in the walker precision
+  double* ion_pos = nullptr;
+  if ((st = dalloc(s->allocs, s->bytes, &ion_pos, 3 * (size_t)d->n_ions)))
+    return st;
+  cudaMemcpy(ion_pos, d->ion_pos, 3 * d->n_ions * sizeof(double), cudaMemcpyHostToDevice);
+  h.ion_pos = ion_pos;
+  std::vector<double> soa(3 * (size_t)d->n_ions);
+  for (int i = 0; i < d->n_ions; ++i)
+    for (int c = 0; c < 3; ++c)
+      soa[(size_t)c * d->n_ions + i] = d->ion_pos[3 * i + c];
+  if (s->fp32)
+  {
+    std::vector<float> f(soa.begin(), soa.end());
+    float* p = nullptr;
+    if ((st = dalloc(s->allocs, s->bytes, &p, f.size())))
+      return st;
+    cudaMemcpy(p, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+    h.ion_soa = p;
+  }
+  else
+  {
+    double* p = nullptr;
+    if ((st = dalloc(s->allocs, s->bytes, &p, soa.size())))
+      return st;
+    cudaMemcpy(p, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice);
+    h.ion_soa = p;
+  }
+  if ((st = dalloc(s->allocs, s->bytes, &s->d, 1)))
+    return st;
+  CK(cudaMemcpy(s->d, &h, sizeof(DevSystem), cudaMemcpyHostToDevice));
+  *out = s;
+  return QMC_OK;
+}
+
+int qmc_system_destroy(qmc_system* s)
+{
+  if (!s)
+    return QMC_OK;
+  cudaDeviceSynchronize();
+  for (void* p : s->allocs)
+    cudaFree(p);
+  delete s;
+  return QMC_OK;
+}
+int qmc_system_bytes(const qmc_system* s, size_t* bytes)
+{
+  if (!s || !bytes)
+    return fail(QMC_ERR_ARG, "null pointer");
+  *bytes = s->bytes;
+  return QMC_OK;
+}
+
+static int spo_points(qmc_system* s, int n_pos, const double* pos, double* v, double* g, double* h, bool vonly)
+{
+  if (!s || n_pos < 0 || (n_pos > 0 && !pos))
+    return fail(QMC_ERR_ARG, "bad arguments");
+  if (n_pos == 0)
+    return QMC_OK;
+  const int norb = s->h.norb;
+  double *dp = nullptr, *dv = nullptr, *dg = nullptr, *dh = nullptr;
+  CK(cudaMalloc(&dp, 3 * n_pos * sizeof(double)));
+  CK(cudaMalloc(&dv, (size_t)n_pos * norb * sizeof(double)));
+  CK(cudaMalloc(&dg, (size_t)n_pos * 3 * norb * sizeof(double)));
+  CK(cudaMalloc(&dh, (size_t)n_pos * 6 * norb * sizeof(double)));
+  CK(cudaMemcpy(dp, pos, 3 * n_pos * sizeof(double), cudaMemcpyHostToDevice));
+  CK(launch_spo_points(s->fp32, s->d, n_pos, dp, dv, dg, dh, vonly, 0));
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess)
+  {
+    if (v)
+      cudaMemcpy(v, dv, (size_t)n_pos * norb * sizeof(double), cudaMemcpyDeviceToHost);
+    if (g && !vonly)
+      cudaMemcpy(g, dg, (size_t)n_pos * 3 * norb * sizeof(double), cudaMemcpyDeviceToHost);
+    if (h && !vonly)
+      cudaMemcpy(h, dh, (size_t)n_pos * 6 * norb * sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dp);
+  cudaFree(dv);
+  cudaFree(dg);
+  cudaFree(dh);
+  CK(e);
+  return QMC_OK;
+}
+int qmc_spo_evaluate_vgh(qmc_system* s, int n_pos, const double* pos, double* v, double* g, double* h)
+{
+  return spo_points(s, n_pos, pos, v, g, h, false);
+}
+int qmc_spo_evaluate_v(qmc_system* s, int n_pos, const double* pos, double* v)
+{
+  return spo_points(s, n_pos, pos, v, nullptr, nullptr, true);
+}
+
+// -------------------------------------------------------------- walkers --
+static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
+{
+  DevWalkers& d = w->dw;
+  const DevSystem& h = s->h;
+  const size_t es = s->fp32 ? 4 : 8;
+  d.W = W, d.N = h.n_elec, d.Npad = round_up(h.n_elec, 32), d.n = h.norb, d.npad = h.npad, d.I = h.n_ions, d.k = k;
+  const size_t N = d.N, Np = d.Npad, n = d.n, np = d.npad, KK = k;
+  std::vector<void*>& L = w->allocs;
+  size_t& B             = w->bytes;
+  auto T = [&](void** p, size_t count) -> int {
+    unsigned char* q = nullptr;
+    int st           = dalloc(L, B, &q, count * es);
+    *p               = q;
+    return st;
+  };
+  int st = 0;
+  st |= dalloc(L, B, &d.R, W * N * 3);
+  st |= T(&d.Rs, W * 3 * Np);
+  st |= T(&d.Ainv, W * 2 * n * np);
+  st |= T(&d.dpsiM, W * 2 * 3 * n * np);
+  st |= T(&d.d2psiM, W * 2 * n * np);
+  st |= T(&d.U, W * 2 * KK * np);
+  st |= T(&d.V, W * 2 * KK * np);
+  st |= dalloc(L, B, &d.Binv, W * 2 * KK * KK);
+  st |= dalloc(L, B, &d.delay_list, W * 2 * KK);
+  st |= dalloc(L, B, &d.delay_count, W * 2);
+  st |= dalloc(L, B, &d.det_log, W * 2);
+  st |= dalloc(L, B, &d.det_phase, W * 2);
+  st |= T(&d.j1_Vat, W * N);
+  st |= T(&d.j1_Lap, W * N);
+  st |= T(&d.j1_Grad, W * 3 * N);
+  st |= T(&d.j2_Uat, W * N);
+  st |= T(&d.j2_d2Uat, W * N);
+  st |= T(&d.j2_dUat, W * 3 * N);
+  st |= dalloc(L, B, &d.j_log, W * 2);
+  st |= dalloc(L, B, &d.mt, W * (size_t)(MT_N + 1));
+  st |= dalloc(L, B, &d.words, W * (8 * N + 8));
+  st |= dalloc(L, B, &d.ur, W * N);
+  st |= dalloc(L, B, &d.delta, W * 3 * N);
+  st |= T(&d.invRow, W * np);
+  st |= T(&d.psiV, W * np);
+  st |= T(&d.dpsiV, W * 3 * np);
+  st |= T(&d.d2psiV, W * np);
+  st |= T(&d.U2, W * KK * np);
+  st |= dalloc(L, B, &d.ms, W);
+  st |= dalloc(L, B, &d.G, W * N * 3);
+  st |= dalloc(L, B, &d.L, W * N);
+  st |= dalloc(L, B, &d.logpsi, W);
+  st |= dalloc(L, B, &d.accepted, W);
+  st |= dalloc(L, B, &d.out_grad, W * 3);
+  st |= dalloc(L, B, &d.out_ratio, W);
+  st |= dalloc(L, B, &d.accept_flags, W);
+  st |= dalloc(L, B, &d.status, 1);
+  st |= dalloc(L, B, &w->d_task, 1);
+  st |= dalloc(L, B, &w->d_displ, W * 3);
+  st |= dalloc(L, B, &w->d_flags, W);
+  d.lu = nullptr;
+  if (st)
+    return QMC_ERR_OOM;
+  std::vector<MoveState> ms(W);
+  for (auto& m : ms)
+  {
+    std::memset(&m, 0, sizeof(m));
+    m.active       = -1;
+    m.invrow_id[0] = m.invrow_id[1] = -1;
+    m.partial[0] = m.partial[1] = 1;
+    m.j_partial                 = 1;
+  }
+  CK(cudaMemcpy(d.ms, ms.data(), W * sizeof(MoveState), cudaMemcpyHostToDevice));
+  return QMC_OK;
+}
+
+static void free_walkers(qmc_walkers* w)
+{
+  if (w->stream)
+    cudaStreamSynchronize(w->stream);
+  for (void* p : w->allocs)
+    cudaFree(p);
+  w->allocs.clear();
+  cudaFree(w->d_ur);
+  cudaFree(w->d_delta);
+  cudaFree(w->d_trace);
+  cudaFree(w->d_rows);
+  if (w->own_stream && w->stream)
+    cudaStreamDestroy(w->stream);
+}
+
+int qmc_walkers_create(qmc_system* s, int n_walkers, int delay_rank, qmc_walkers** out)
+{
+  if (!s || !out || n_walkers < 1 || delay_rank < 1 || delay_rank > 64 || delay_rank > s->h.norb)
+    return fail(QMC_ERR_ARG, "bad walker batch arguments (1 <= delay_rank <= min(64, n_orb))");
+  *out = nullptr;
+  auto* w = new qmc_walkers_s;
+  w->sys  = s;
+  w->fp32 = s->fp32;
+  int st  = alloc_walkers(w, s, n_walkers, delay_rank);
+  if (st)
+  {
+    free_walkers(w);
+    delete w;
+    return st;
+  }
+  const int vw   = w->fp32 ? 4 : 2;
+  const int nvec = s->h.npad / vw;
+  w->threads     = std::min(256, std::max(std::max(64, 2 * delay_rank), round_up(nvec, 32)));
+  cudaError_t e  = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess)
+  {
+    free_walkers(w);
+    delete w;
+    return fail(QMC_ERR_CUDA, cudaGetErrorString(e));
+  }
+  w->own_stream = true;
+  *out          = w;
+  return QMC_OK;
+}
+int qmc_walkers_destroy(qmc_walkers* w)
+{
+  if (!w)
+    return QMC_OK;
+  free_walkers(w);
+  delete w;
+  return QMC_OK;
+}
+int qmc_walkers_bytes(const qmc_walkers* w, size_t* bytes)
+{
+  if (!w || !bytes)
+    return fail(QMC_ERR_ARG, "null pointer");
+  *bytes = w->bytes;
+  return QMC_OK;
+}
+int qmc_walkers_set_stream(qmc_walkers* w, void* stream)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null pointer");
+  cudaStreamSynchronize(w->stream);
+  if (w->own_stream)
+    cudaStreamDestroy(w->stream);
+  w->own_stream = false;
+  w->stream     = (cudaStream_t)stream;
+  if (!stream)
+  {
+    cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+    w->own_stream = true;
+  }
+  return QMC_OK;
+}
+int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count)
+{
+  if (!w || !count)
+    return fail(QMC_ERR_ARG, "null pointer");
+  *count = w->launches;
+  return QMC_OK;
+}
+int qmc_walkers_sync(qmc_walkers* w)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null pointer");
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+
+static int sync_rs(qmc_walkers* w)
+{
+  CK(launch_sync_rs(w->fp32, w->dw, w->stream));
+  w->launches++;
+  return QMC_OK;
+}
+
+int qmc_walkers_init_random(qmc_walkers* w, const uint32_t* seeds)
+{
+  if (!w || !seeds)
+    return fail(QMC_ERR_ARG, "null pointer");
+  const int W = w->dw.W, N = w->dw.N;
+  std::vector<double> R((size_t)W * N * 3);
+  std::vector<uint32_t> mt((size_t)W * (MT_N + 1));
+  for (int i = 0; i < W; ++i)
+  {
+    MTState st;
+    mt_seed_host(st, seeds[i]);
+    for (int e = 0; e < N; ++e)
+    {
+      double u[3];
+      for (int c = 0; c < 3; ++c)
+      {
+        const uint32_t w0 = mt_next_host(st);
+        const uint32_t w1 = mt_next_host(st);
+        u[c]              = canonical_double(w0, w1);
+      }
+      qmc_host::to_cart(w->sys->h.lattice, u, &R[((size_t)i * N + e) * 3]);
+    }
+    std::memcpy(&mt[(size_t)i * (MT_N + 1)], st.mt, sizeof(st.mt));
+    mt[(size_t)i * (MT_N + 1) + MT_N] = (uint32_t)st.mti;
+  }
+  CK(cudaMemcpyAsync(w->dw.R, R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  CK(cudaMemcpyAsync(w->dw.mt, mt.data(), mt.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
+  int st = sync_rs(w);
+  if (st)
+    return st;
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+int qmc_walkers_set_positions(qmc_walkers* w, const double* R)
+{
+  if (!w || !R)
+    return fail(QMC_ERR_ARG, "null pointer");
+  CK(cudaMemcpyAsync(w->dw.R, R, (size_t)w->dw.W * w->dw.N * 3 * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  int st = sync_rs(w);
+  if (st)
+    return st;
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+int qmc_walkers_get_positions(qmc_walkers* w, double* R)
+{
+  if (!w || !R)
+    return fail(QMC_ERR_ARG, "null pointer");
+  CK(cudaMemcpyAsync(R, w->dw.R, (size_t)w->dw.W * w->dw.N * 3 * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+
+// ------------------------------------------------------------ verbs -----
+static int verb(qmc_walkers* w, VerbArgs a)
+{
+  CK(launch_verb(w->fp32, w->sys->d, w->dw, a, w->threads, w->dw.k, w->stream));
+  w->launches++;
+  return QMC_OK;
+}
+static int check_iat(qmc_walkers* w, int iat)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  if (iat < 0 || iat >= w->dw.N)
+    return fail(QMC_ERR_ARG, "electron index out of range");
+  return QMC_OK;
+}
+
+int qmc_pset_update(qmc_walkers* w) { return w ? QMC_OK : fail(QMC_ERR_ARG, "null handle"); }
+int qmc_pset_done(qmc_walkers* w) { return w ? QMC_OK : fail(QMC_ERR_ARG, "null handle"); }
+int qmc_pset_set_active(qmc_walkers* w, int iat) { return check_iat(w, iat); }
+
+int qmc_pset_make_move(qmc_walkers* w, int iat, const double* displ)
+{
+  int st = check_iat(w, iat);
+  if (st)
+    return st;
+  if (!displ)
+    return fail(QMC_ERR_ARG, "null displacement");
+  CK(cudaMemcpyAsync(w->d_displ, displ, 3 * w->dw.W * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  VerbArgs a{};
+  a.op    = VERB_MAKE_MOVE;
+  a.iat   = iat;
+  a.displ = w->d_displ;
+  return verb(w, a);
+}
+static int flags_verb(qmc_walkers* w, int op, int iat, const int* accept)
+{
+  int st = check_iat(w, iat);
+  if (st)
+    return st;
+  if (!accept)
+    return fail(QMC_ERR_ARG, "null accept flags");
+  CK(cudaMemcpyAsync(w->d_flags, accept, w->dw.W * sizeof(int), cudaMemcpyHostToDevice, w->stream));
+  VerbArgs a{};
+  a.op    = op;
+  a.iat   = iat;
+  a.flags = w->d_flags;
+  if ((st = verb(w, a)))
+    return st;
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+int qmc_pset_accept_reject(qmc_walkers* w, int iat, const int* accept)
+{
+  return flags_verb(w, VERB_PSET_ACCEPT, iat, accept);
+}
+int qmc_wf_accept_restore(qmc_walkers* w, int iat, const int* accept)
+{
+  return flags_verb(w, VERB_WF_ACCEPT, iat, accept);
+}
+
+int qmc_pset_get_temp_rows(qmc_walkers* w, double* aa_r, double* aa_dr, double* ab_r, double* ab_dr)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  const size_t W = w->dw.W, N = w->dw.N, I = w->dw.I;
+  const size_t need = W * (4 * N + 4 * I);
+  if (w->cap_rows < need)
+  {
+    cudaFree(w->d_rows);
+    CK(cudaMalloc(&w->d_rows, need * sizeof(double)));
+    w->cap_rows = need;
+  }
+  VerbArgs a{};
+  a.op    = VERB_TEMP_ROWS;
+  a.iat   = 0;
+  a.aa_r  = w->d_rows;
+  a.aa_dr = a.aa_r + W * N;
+  a.ab_r  = a.aa_dr + W * N * 3;
+  a.ab_dr = a.ab_r + W * I;
+  int st  = verb(w, a);
+  if (st)
+    return st;
+  if (aa_r)
+    CK(cudaMemcpyAsync(aa_r, a.aa_r, W * N * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  if (aa_dr)
+    CK(cudaMemcpyAsync(aa_dr, a.aa_dr, W * N * 3 * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  if (ab_r)
+    CK(cudaMemcpyAsync(ab_r, a.ab_r, W * I * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  if (ab_dr)
+    CK(cudaMemcpyAsync(ab_dr, a.ab_dr, W * I * 3 * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+
+static int ensure_lu(qmc_walkers* w)
+{
+  if (w->dw.lu)
+    return QMC_OK;
+  return dalloc(w->allocs, w->bytes, &w->dw.lu, (size_t)w->dw.W * 2 * w->dw.n * w->dw.npad);
+}
+
+// FP64 refresh of both inverses from the current positions
+static int recompute_dets(qmc_walkers* w)
+{
+  int st = ensure_lu(w);
+  if (st)
+    return st;
+  CK(launch_spo_matrix(w->fp32, w->sys->d, w->dw, true, w->stream));
+  CK(launch_gj_inverse(w->fp32, w->sys->d, w->dw, 512, 2, w->stream));
+  w->launches += 2;
+  return QMC_OK;
+}
+
+int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  const int comp = w->sys->h.comp;
+  int st         = 0;
+  if (comp & QMC_WF_DET)
+    if ((st = recompute_dets(w)))
+      return st;
+  if (comp & (QMC_WF_J1 | QMC_WF_J2))
+  {
+    CK(launch_jastrow_recompute(w->fp32, w->sys->d, w->dw, 256, w->stream));
+    w->launches++;
+  }
+  CK(launch_gl(w->fp32, w->sys->d, w->dw, w->threads, w->stream));
+  w->launches++;
+  std::vector<MoveState> ms(w->dw.W);
+  for (auto& m : ms)
+  {
+    std::memset(&m, 0, sizeof(m));
+    m.active       = -1;
+    m.invrow_id[0] = m.invrow_id[1] = -1;
+    m.partial[0] = m.partial[1] = 1;
+    m.j_partial                 = 1;
+  }
+  CK(cudaMemcpyAsync(w->dw.ms, ms.data(), ms.size() * sizeof(MoveState), cudaMemcpyHostToDevice, w->stream));
+  if (logpsi)
+    CK(cudaMemcpyAsync(logpsi, w->dw.logpsi, w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+
+int qmc_wf_eval_grad(qmc_walkers* w, int iat, double* grad)
+{
+  int st = check_iat(w, iat);
+  if (st)
+    return st;
+  VerbArgs a{};
+  a.op  = VERB_EVAL_GRAD;
+  a.iat = iat;
+  if ((st = verb(w, a)))
+    return st;
+  if (grad)
+    CK(cudaMemcpyAsync(grad, w->dw.out_grad, 3 * w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+static int ratio_verb(qmc_walkers* w, int op, int iat, double* ratio, double* grad)
+{
+  int st = check_iat(w, iat);
+  if (st)
+    return st;
+  VerbArgs a{};
+  a.op  = op;
+  a.iat = iat;
+  if ((st = verb(w, a)))
+    return st;
+  if (ratio)
+    CK(cudaMemcpyAsync(ratio, w->dw.out_ratio, w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  if (grad)
+    CK(cudaMemcpyAsync(grad, w->dw.out_grad, 3 * w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+int qmc_wf_ratio_grad(qmc_walkers* w, int iat, double* ratio, double* grad)
+{
+  return ratio_verb(w, VERB_RATIO_GRAD, iat, ratio, grad);
+}
+int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio) { return ratio_verb(w, VERB_RATIO, iat, ratio, nullptr); }
+
+int qmc_wf_complete_updates(qmc_walkers* w)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  VerbArgs a{};
+  a.op   = VERB_COMPLETE;
+  int st = verb(w, a);
+  if (st)
+    return st;
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+
+int qmc_wf_evaluate_gl(qmc_walkers* w, double* G, double* L, double* logpsi)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  CK(launch_gl(w->fp32, w->sys->d, w->dw, w->threads, w->stream));
+  w->launches++;
+  const size_t W = w->dw.W, N = w->dw.N;
+  if (G)
+    CK(cudaMemcpyAsync(G, w->dw.G, W * N * 3 * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  if (L)
+    CK(cudaMemcpyAsync(L, w->dw.L, W * N * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  if (logpsi)
+    CK(cudaMemcpyAsync(logpsi, w->dw.logpsi, W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+
+int qmc_wf_components(qmc_walkers* w, double* comp)
+{
+  if (!w || !comp)
+    return fail(QMC_ERR_ARG, "null pointer");
+  const size_t W = w->dw.W;
+  std::vector<double> dl(2 * W), dp(2 * W), jl(2 * W);
+  CK(cudaMemcpyAsync(dl.data(), w->dw.det_log, 2 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(dp.data(), w->dw.det_phase, 2 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(jl.data(), w->dw.j_log, 2 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  for (size_t i = 0; i < W; ++i)
+  {
+    comp[6 * i + 0] = dl[2 * i];
+    comp[6 * i + 1] = dl[2 * i + 1];
+    comp[6 * i + 2] = dp[2 * i];
+    comp[6 * i + 3] = dp[2 * i + 1];
+    comp[6 * i + 4] = jl[2 * i];
+    comp[6 * i + 5] = jl[2 * i + 1];
+  }
+  return QMC_OK;
+}
+
+// Ainv with the pending delayed rows applied: Ainv - (Ainv U^T - E)(Binv V),
+// evaluated on a host copy (an inspection accessor, not on the move path).
+int qmc_wf_get_inverse(qmc_walkers* w, int walker, int spin, double* psiM)
+{
+  if (!w || !psiM || walker < 0 || walker >= w->dw.W || spin < 0 || spin > 1)
+    return fail(QMC_ERR_ARG, "bad arguments");
+  const size_t n = w->dw.n, np = w->dw.npad, k = w->dw.k, es = w->fp32 ? 4 : 8;
+  std::vector<unsigned char> a(n * np * es), u(k * np * es), v(k * np * es);
+  std::vector<double> B(k * k);
+  std::vector<int> dl(k);
+  int dc = 0;
+  const size_t mat = ((size_t)walker * 2 + spin);
+  CK(cudaMemcpy(a.data(), (unsigned char*)w->dw.Ainv + mat * n * np * es, a.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(u.data(), (unsigned char*)w->dw.U + mat * k * np * es, u.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(v.data(), (unsigned char*)w->dw.V + mat * k * np * es, v.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(B.data(), w->dw.Binv + mat * k * k, B.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(dl.data(), w->dw.delay_list + mat * k, k * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&dc, w->dw.delay_count + mat, sizeof(int), cudaMemcpyDeviceToHost));
+  auto at = [&](const std::vector<unsigned char>& buf, size_t i) -> double {
+    return es == 4 ? (double)((const float*)buf.data())[i] : ((const double*)buf.data())[i];
+  };
+  std::vector<double> A(n * n);
+  for (size_t i = 0; i < n; ++i)
+    for (size_t j = 0; j < n; ++j)
+      A[i * n + j] = at(a, i * np + j);
+  if (dc > 0)
+  {
+    std::vector<double> tm(n * dc), U2(dc * n, 0.0);
+    for (size_t i = 0; i < n; ++i)
+      for (int d = 0; d < dc; ++d)
+      {
+        double s = 0;
+        for (size_t j = 0; j < n; ++j)
+          s += at(u, d * np + j) * A[i * n + j];
+        tm[i * dc + d] = s - (dl[d] == (int)i ? 1.0 : 0.0);
+      }
+    for (int b = 0; b < dc; ++b)
+      for (int aa = 0; aa < dc; ++aa)
+        for (size_t j = 0; j < n; ++j)
+          U2[b * n + j] += B[b * k + aa] * at(v, aa * np + j);
+    for (size_t i = 0; i < n; ++i)
+      for (int d = 0; d < dc; ++d)
+        for (size_t j = 0; j < n; ++j)
+          A[i * n + j] -= tm[i * dc + d] * U2[d * n + j];
+  }
+  std::memcpy(psiM, A.data(), A.size() * sizeof(double));
+  return QMC_OK;
+}
+
+// ------------------------------------------------------------ sweep -----
+static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accept, int rng_mode, const double* ur,
+                       const double* delta, int recompute_every, double* trace, bool async)
+{
+  const size_t W = w->dw.W, N = w->dw.N;
+  if (rng_mode == QMC_RNG_HOST)
+  {
+    const size_t need = W * n_substeps * N;
+    if (w->cap_rng < need)
+    {
+      cudaFree(w->d_ur);
+      cudaFree(w->d_delta);
+      CK(cudaMalloc(&w->d_ur, need * sizeof(double)));
+      CK(cudaMalloc(&w->d_delta, 3 * need * sizeof(double)));
+      w->cap_rng = need;
+    }
+  }
+  if (trace)
+  {
+    const size_t need = W * n_substeps * N * 8;
+    if (w->cap_trace < need)
+    {
+      cudaFree(w->d_trace);
+      CK(cudaMalloc(&w->d_trace, need * sizeof(double)));
+      w->cap_trace = need;
+    }
+  }
+  SweepTask task{};
+  task.sys         = w->sys->d;
+  task.dw          = w->dw;
+  task.rng_mode    = rng_mode;
+  task.ur          = w->d_ur;
+  task.delta       = w->d_delta;
+  task.trace       = trace ? w->d_trace : nullptr;
+  task.first_block = 0;
+  CK(cudaMemcpyAsync(w->d_task, &task, sizeof(task), cudaMemcpyHostToDevice, w->stream));
+  for (int step = 0; step < n_steps; ++step)
+  {
+    if (rng_mode == QMC_RNG_HOST)
+    {
+      const size_t blk = W * n_substeps * N;
+      CK(cudaMemcpyAsync(w->d_ur, ur + step * blk, blk * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+      CK(cudaMemcpyAsync(w->d_delta, delta + step * blk * 3, 3 * blk * sizeof(double), cudaMemcpyHostToDevice,
+                         w->stream));
+    }
+    CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k, w->stream));
+    w->launches++;
+    if (trace)
+      CK(cudaMemcpyAsync(trace + (size_t)step * W * n_substeps * N * 8, w->d_trace,
+                         W * n_substeps * N * 8 * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+    if (recompute_every > 0 && (step + 1) % recompute_every == 0 && (w->sys->h.comp & QMC_WF_DET))
+    {
+      int st = recompute_dets(w);
+      if (st)
+        return st;
+      CK(launch_gl(w->fp32, w->sys->d, w->dw, w->threads, w->stream));
+      w->launches++;
+    }
+  }
+  if (!async)
+  {
+    CK(cudaStreamSynchronize(w->stream));
+    return device_status(w);
+  }
+  return QMC_OK;
+}
+
+int qmc_sweep(qmc_walkers* w, const qmc_sweep_opts* o)
+{
+  if (!w || !o || o->n_steps < 0 || o->n_substeps < 1)
+    return fail(QMC_ERR_ARG, "bad sweep options");
+  if (o->rng_mode == QMC_RNG_HOST && (!o->ur || !o->delta))
+    return fail(QMC_ERR_ARG, "QMC_RNG_HOST needs ur and delta");
+  CK(cudaMemsetAsync(w->dw.accepted, 0, w->dw.W * sizeof(long long), w->stream));
+  int st = sweep_steps(w, o->n_steps, o->n_substeps, o->accept, o->rng_mode, o->ur, o->delta, o->recompute_every,
+                       o->trace, false);
+  if (st)
+    return st;
+  if (o->n_accepted)
+    CK(cudaMemcpy(o->n_accepted, w->dw.accepted, w->dw.W * sizeof(long long), cudaMemcpyDeviceToHost));
+  if (o->logpsi)
+    CK(cudaMemcpy(o->logpsi, w->dw.logpsi, w->dw.W * sizeof(double), cudaMemcpyDeviceToHost));
+  return QMC_OK;
+}
+
+int qmc_sweep_async(qmc_walkers* w, int n_steps, int n_substeps, double accept, int recompute_every)
+{
+  if (!w || n_steps < 0 || n_substeps < 1)
+    return fail(QMC_ERR_ARG, "bad sweep options");
+  return sweep_steps(w, n_steps, n_substeps, accept, QMC_RNG_DEVICE, nullptr, nullptr, recompute_every, nullptr,
+                     true);
+}
+
+int qmc_sweep_results(qmc_walkers* w, int64_t* n_accepted, double* logpsi)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  if (n_accepted)
+    CK(cudaMemcpyAsync(n_accepted, w->dw.accepted, w->dw.W * sizeof(long long), cudaMemcpyDeviceToHost, w->stream));
+  if (logpsi)
+    CK(cudaMemcpyAsync(logpsi, w->dw.logpsi, w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+
+// ------------------------------------------------- DelayedUpdate engine --
+struct qmc_detengine_s
+{
+  qmc_walkers_s w;
+};
+
+int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
+{
+  if (!out || n < 1 || delay < 1 || delay > 64 || delay > n)
+    return fail(QMC_ERR_ARG, "bad engine size");
+  auto* e       = new qmc_detengine_s;
+  auto* w       = &e->w;
+  DevWalkers& d = w->dw;
+  std::memset(&d, 0, sizeof(d));
+  d.W = 1, d.N = n, d.Npad = round_up(n, 32), d.n = n, d.npad = round_up(n, 32), d.I = 0, d.k = delay;
+  w->fp32 = false;
+  const size_t np = d.npad, K = delay;
+  auto& L         = w->allocs;
+  auto& B         = w->bytes;
+  int st          = 0;
+  auto Dm         = [&](void** p, size_t c) {
+    double* q = nullptr;
+    int r     = dalloc(L, B, &q, c);
+    *p        = q;
+    return r;
+  };
+  st |= Dm(&d.Ainv, 2 * n * np);
+  st |= Dm(&d.dpsiM, 2 * 3 * n * np);
+  st |= Dm(&d.d2psiM, 2 * n * np);
+  st |= Dm(&d.U, 2 * K * np);
+  st |= Dm(&d.V, 2 * K * np);
+  st |= dalloc(L, B, &d.Binv, 2 * K * K);
+  st |= dalloc(L, B, &d.delay_list, 2 * K);
+  st |= dalloc(L, B, &d.delay_count, 2);
+  st |= dalloc(L, B, &d.det_log, 2);
+  st |= dalloc(L, B, &d.det_phase, 2);
+  st |= Dm(&d.invRow, np);
+  st |= Dm(&d.psiV, np);
+  st |= Dm(&d.dpsiV, 3 * np);
+  st |= Dm(&d.d2psiV, np);
+  st |= Dm(&d.U2, K * np);
+  st |= dalloc(L, B, &d.lu, 2 * n * np);
+  st |= dalloc(L, B, &d.status, 1);
+  st |= dalloc(L, B, &d.ms, 1);
+  if (st)
+  {
+    free_walkers(w);
+    delete e;
+    return QMC_ERR_OOM;
+  }
+  cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+  w->own_stream = true;
+  *out          = e;
+  return QMC_OK;
+}
+int qmc_detengine_destroy(qmc_detengine_s* e)
+{
+  if (!e)
+    return QMC_OK;
+  free_walkers(&e->w);
+  delete e;
+  return QMC_OK;
+}
+int qmc_detengine_invert_transpose(qmc_detengine_s* e, const double* a, double* logdet, double* phase)
+{
+  if (!e || !a)
+    return fail(QMC_ERR_ARG, "null pointer");
+  auto* w        = &e->w;
+  const size_t n = w->dw.n, np = w->dw.npad;
+  std::vector<double> m(n * np, 0.0);
+  for (size_t i = 0; i < n; ++i)
+    for (size_t j = 0; j < n; ++j)
+      m[i * np + j] = a[i * n + j];
+  CK(cudaMemcpyAsync(w->dw.lu, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  CK(launch_gj_inverse(false, nullptr, w->dw, 256, 1, w->stream));
+  double lg = 0, ph = 0;
+  CK(cudaMemcpyAsync(&lg, w->dw.det_log, sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(&ph, w->dw.det_phase, sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  if (logdet)
+    *logdet = lg;
+  if (phase)
+    *phase = ph;
+  return device_status(w);
+}
+int qmc_detengine_get_inv_row(qmc_detengine_s* e, int row, double* inv_row)
+{
+  if (!e || !inv_row || row < 0 || row >= e->w.dw.n)
+    return fail(QMC_ERR_ARG, "bad arguments");
+  auto* w = &e->w;
+  CK(launch_det_engine(false, DETENG_GET_INV_ROW, w->dw, row, w->dw.k, w->stream));
+  CK(cudaMemcpyAsync(inv_row, w->dw.invRow, w->dw.n * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+int qmc_detengine_accept_row(qmc_detengine_s* e, int row, const double* psiv)
+{
+  if (!e || !psiv || row < 0 || row >= e->w.dw.n)
+    return fail(QMC_ERR_ARG, "bad arguments");
+  auto* w = &e->w;
+  std::vector<double> p(w->dw.npad, 0.0);
+  std::memcpy(p.data(), psiv, w->dw.n * sizeof(double));
+  CK(cudaMemcpyAsync(w->dw.psiV, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  CK(launch_det_engine(false, DETENG_ACCEPT_ROW, w->dw, row, w->dw.k, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+int qmc_detengine_update_inv_mat(qmc_detengine_s* e)
+{
+  if (!e)
+    return fail(QMC_ERR_ARG, "null pointer");
+  auto* w = &e->w;
+  CK(launch_det_engine(false, DETENG_UPDATE, w->dw, 0, w->dw.k, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return QMC_OK;
+}
+int qmc_detengine_get_ainv(qmc_detengine_s* e, double* ainv)
+{
+  if (!e || !ainv)
+    return fail(QMC_ERR_ARG, "null pointer");
+  auto* w        = &e->w;
+  const size_t n = w->dw.n, np = w->dw.npad;
+  std::vector<double> m(n * np);
+  CK(cudaMemcpy(m.data(), w->dw.Ainv, m.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < n; ++i)
+    for (size_t j = 0; j < n; ++j)
+      ainv[i * n + j] = m[i * np + j];
+  return QMC_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,1146 @@
+// device.cuh -- __device__ building blocks of the VMC walker hot path (sm_100a).
+//
+// One CTA owns one walker.  The fused sweep kernel runs a whole MC step per
+// launch: per substep the walker's mt19937 stream is advanced (N uniforms,
+// 3N normals), then N single-electron moves (evalGrad, makeMove, ratioGrad,
+// threshold accept) and completeUpdates; at the end evaluateGL.  Every phase
+// is a __device__ function shared with the drop-in verb kernels, so the
+// per-call API and the fused sweep execute the same arithmetic.
+//
+// Reference algorithms (QMCPACK/miniqmc) restated here:
+//   minimum image             ParticleBConds.h:153-217
+//   B-spline SPO (VGH / V)    MultiBspline.hpp:34-280, MultiBsplineEvalHelper.hpp:43-113,
+//                             MultiBsplineData.hpp:52-80, einspline_spo.hpp:163-223
+//   radial functor            BsplineFunctor.h:222-339
+//   J1                        OneBodyJastrow.h:110-283
+//   J2                        TwoBodyJastrow.h:250-430
+//   determinant               DiracDeterminant.cpp:80-187
+//   delayed update            DelayedUpdate.h:95-231
+//   inverse + log|det|        DiracMatrix.h:25-38, 93-119 (Gauss-Jordan here)
+#pragma once
+#include "kernels.cuh"
+
+#include <cfloat>
+
+namespace qmc
+{
+constexpr int MAXK = 64; // largest delay rank a launch supports
+
+template <typename T> struct FunctorT
+{
+  int n;
+  T cutoff, dinv;
+  T c[QMC_MAX_FUNCTOR_COEFS];
+};
+
+template <typename T> struct SysSmem
+{
+  T rb[9], gb[9], cn[24];
+  FunctorT<T> j1[QMC_MAX_ION_GROUPS], j2uu, j2ud;
+  int gfirst[QMC_MAX_ION_GROUPS], glast[QMC_MAX_ION_GROUPS];
+  int n_groups, n_ions, n_elec, n_up, norb, npad, comp, lap_mode;
+};
+
+template <typename T> struct SplineSmem
+{
+  T a[3][4], da[3][4], d2a[3][4];
+  long long base;
+};
+
+struct MoveSmem
+{
+  double red[32 * 16];
+  double sums[16];
+  double pos_old[3], pos_new[3];
+  double p[MAXK + 1], wv[MAXK + 1], col[MAXK + 1];
+  double ratio_det, curAt, curLap, curGrad[3], curUat, y;
+  int accept, dc, ok;
+};
+
+// ----------------------------------------------------- typed views ------
+template <typename T> struct WV
+{
+  int N, Npad, n, npad, I, k, w;
+  double* R;
+  T* Rs;
+  T* Ainv;
+  T* dpsiM;
+  T* d2psiM;
+  T* U;
+  T* V;
+  double* Binv;
+  int* dlist;
+  int* dcount;
+  double* det_log;
+  double* det_phase;
+  T* Vat;
+  T* Lap;
+  T* Grad;
+  T* Uat;
+  T* d2Uat;
+  T* dUat;
+  double* jlog;
+  uint32_t* mt;
+  uint32_t* words;
+  double* ur;
+  double* delta;
+  T* invRow;
+  T* psiV;
+  T* dpsiV;
+  T* d2psiV;
+  T* U2;
+  double* lu;
+  MoveState* ms;
+  double* G;
+  double* L;
+  unsigned* status;
+
+  __device__ T* ainv(int s) const { return Ainv + (size_t)s * n * npad; }
+  __device__ T* dpsi(int s) const { return dpsiM + (size_t)s * n * 3 * npad; }
+  __device__ T* d2psi(int s) const { return d2psiM + (size_t)s * n * npad; }
+  __device__ T* u(int s) const { return U + (size_t)s * k * npad; }
+  __device__ T* v(int s) const { return V + (size_t)s * k * npad; }
+  __device__ double* binv(int s) const { return Binv + (size_t)s * k * k; }
+  __device__ int* dl(int s) const { return dlist + s * k; }
+};
+
+template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
+{
+  WV<T> v;
+  v.N = d.N, v.Npad = d.Npad, v.n = d.n, v.npad = d.npad, v.I = d.I, v.k = d.k, v.w = w;
+  const size_t nn = (size_t)d.n * d.npad, kn = (size_t)d.k * d.npad;
+  v.R         = d.R + (size_t)w * d.N * 3;
+  v.Rs        = (T*)d.Rs + (size_t)w * 3 * d.Npad;
+  v.Ainv      = (T*)d.Ainv + (size_t)w * 2 * nn;
+  v.dpsiM     = (T*)d.dpsiM + (size_t)w * 2 * 3 * nn;
+  v.d2psiM    = (T*)d.d2psiM + (size_t)w * 2 * nn;
+  v.U         = (T*)d.U + (size_t)w * 2 * kn;
+  v.V         = (T*)d.V + (size_t)w * 2 * kn;
+  v.Binv      = d.Binv + (size_t)w * 2 * d.k * d.k;
+  v.dlist     = d.delay_list + (size_t)w * 2 * d.k;
+  v.dcount    = d.delay_count + (size_t)w * 2;
+  v.det_log   = d.det_log + (size_t)w * 2;
+  v.det_phase = d.det_phase + (size_t)w * 2;
+  v.Vat       = (T*)d.j1_Vat + (size_t)w * d.N;
+  v.Lap       = (T*)d.j1_Lap + (size_t)w * d.N;
+  v.Grad      = (T*)d.j1_Grad + (size_t)w * 3 * d.N;
+  v.Uat       = (T*)d.j2_Uat + (size_t)w * d.N;
+  v.d2Uat     = (T*)d.j2_d2Uat + (size_t)w * d.N;
+  v.dUat      = (T*)d.j2_dUat + (size_t)w * 3 * d.N;
+  v.jlog      = d.j_log + (size_t)w * 2;
+  v.mt        = d.mt + (size_t)w * (MT_N + 1);
+  v.words     = d.words + (size_t)w * (8 * (size_t)d.N + 8);
+  v.ur        = d.ur + (size_t)w * d.N;
+  v.delta     = d.delta + (size_t)w * 3 * d.N;
+  v.invRow    = (T*)d.invRow + (size_t)w * d.npad;
+  v.psiV      = (T*)d.psiV + (size_t)w * d.npad;
+  v.dpsiV     = (T*)d.dpsiV + (size_t)w * 3 * d.npad;
+  v.d2psiV    = (T*)d.d2psiV + (size_t)w * d.npad;
+  v.U2        = (T*)d.U2 + (size_t)w * kn;
+  v.lu        = d.lu ? d.lu + (size_t)w * 2 * nn : nullptr;
+  v.ms        = d.ms + w;
+  v.G         = d.G + (size_t)w * d.N * 3;
+  v.L         = d.L + (size_t)w * d.N;
+  v.status    = d.status;
+  return v;
+}
+
+template <typename T> __device__ void load_sys(const DevSystem* __restrict__ s, SysSmem<T>& ss)
+{
+  const int tid = threadIdx.x;
+  if (tid < 9)
+  {
+    ss.rb[tid] = (T)s->rb[tid];
+    ss.gb[tid] = (T)s->gb[tid];
+  }
+  if (tid < 24)
+    ss.cn[tid] = (T)s->corners[tid];
+  for (int i = tid; i < QMC_MAX_ION_GROUPS * QMC_MAX_FUNCTOR_COEFS; i += blockDim.x)
+  {
+    const int g = i / QMC_MAX_FUNCTOR_COEFS, c = i % QMC_MAX_FUNCTOR_COEFS;
+    ss.j1[g].c[c] = (T)s->j1[g].c[c];
+  }
+  for (int c = tid; c < QMC_MAX_FUNCTOR_COEFS; c += blockDim.x)
+  {
+    ss.j2uu.c[c] = (T)s->j2uu.c[c];
+    ss.j2ud.c[c] = (T)s->j2ud.c[c];
+  }
+  if (tid == 0)
+  {
+    for (int g = 0; g < QMC_MAX_ION_GROUPS; ++g)
+    {
+      ss.j1[g].n      = s->j1[g].n;
+      ss.j1[g].cutoff = (T)s->j1[g].cutoff;
+      ss.j1[g].dinv   = (T)s->j1[g].dinv;
+      ss.gfirst[g]    = s->gfirst[g];
+      ss.glast[g]     = s->glast[g];
+    }
+    ss.j2uu.n = s->j2uu.n, ss.j2uu.cutoff = (T)s->j2uu.cutoff, ss.j2uu.dinv = (T)s->j2uu.dinv;
+    ss.j2ud.n = s->j2ud.n, ss.j2ud.cutoff = (T)s->j2ud.cutoff, ss.j2ud.dinv = (T)s->j2ud.dinv;
+    ss.n_groups = s->n_groups, ss.n_ions = s->n_ions, ss.n_elec = s->n_elec, ss.n_up = s->n_up;
+    ss.norb = s->norb, ss.npad = s->npad, ss.comp = s->comp, ss.lap_mode = s->lap_mode;
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------ minimum image --
+// DTD_BConds<T,3,PPPG+SOA_OFFSET>::computeDistances for one pair; the
+// caller has applied `flip` to the displacement and applies it again.
+template <typename T>
+__device__ __forceinline__ T min_image(T& dx, T& dy, T& dz, const T* __restrict__ rb, const T* __restrict__ gb,
+                                       const T* __restrict__ cn)
+{
+  const T ar0  = -floor(dx * gb[0] + dy * gb[3] + dz * gb[6]);
+  const T ar1  = -floor(dx * gb[1] + dy * gb[4] + dz * gb[7]);
+  const T ar2  = -floor(dx * gb[2] + dy * gb[5] + dz * gb[8]);
+  const T delx = dx + ar0 * rb[0] + ar1 * rb[3] + ar2 * rb[6];
+  const T dely = dy + ar0 * rb[1] + ar1 * rb[4] + ar2 * rb[7];
+  const T delz = dz + ar0 * rb[2] + ar1 * rb[5] + ar2 * rb[8];
+  T rmin       = delx * delx + dely * dely + delz * delz;
+  int ic       = 0;
+#pragma unroll
+  for (int c = 1; c < 8; ++c)
+  {
+    const T x  = delx + cn[3 * c];
+    const T y  = dely + cn[3 * c + 1];
+    const T z  = delz + cn[3 * c + 2];
+    const T r2 = x * x + y * y + z * z;
+    ic         = (r2 < rmin) ? c : ic;
+    rmin       = (r2 < rmin) ? r2 : rmin;
+  }
+  dx = delx + cn[3 * ic];
+  dy = dely + cn[3 * ic + 1];
+  dz = delz + cn[3 * ic + 2];
+  return sqrt(rmin);
+}
+
+// ------------------------------------------------------ radial functor --
+// BsplineFunctor::evaluateVGL for one pair inside the cutoff: u, du/dr / r, d2u/dr2
+template <typename T>
+__device__ __forceinline__ void functor_vgl(const FunctorT<T>& f, T r, T& u, T& du, T& d2u)
+{
+  const T rinv = T(1) / r;
+  r *= f.dinv;
+  const int i = (int)r;
+  const T t = r - T(i), tp1 = t * t, tp0 = tp1 * t, tp2 = t;
+  const T s0 = f.c[i], s1 = f.c[i + 1], s2 = f.c[i + 2], s3 = f.c[i + 3];
+  // constants of BsplineFunctor's A, dA, d2A tables
+  d2u = f.dinv * f.dinv *
+      (s0 * (T(-1.0) * tp2 + T(1.0)) + s1 * (T(3.0) * tp2 + T(-2.0)) + s2 * (T(-3.0) * tp2 + T(1.0)) +
+       s3 * (T(1.0) * tp2 + T(0.0)));
+  du = f.dinv * rinv *
+      (s0 * (T(-0.5) * tp1 + T(1.0) * tp2 + T(-0.5)) + s1 * (T(1.5) * tp1 + T(-2.0) * tp2 + T(0.0)) +
+       s2 * (T(-1.5) * tp1 + T(1.0) * tp2 + T(0.5)) + s3 * (T(0.5) * tp1 + T(0.0) * tp2 + T(0.0)));
+  u = (s0 * (T(-1.0 / 6.0) * tp0 + T(3.0 / 6.0) * tp1 + T(-3.0 / 6.0) * tp2 + T(1.0 / 6.0)) +
+       s1 * (T(3.0 / 6.0) * tp0 + T(-6.0 / 6.0) * tp1 + T(0.0 / 6.0) * tp2 + T(4.0 / 6.0)) +
+       s2 * (T(-3.0 / 6.0) * tp0 + T(3.0 / 6.0) * tp1 + T(3.0 / 6.0) * tp2 + T(1.0 / 6.0)) +
+       s3 * (T(1.0 / 6.0) * tp0 + T(0.0 / 6.0) * tp1 + T(0.0 / 6.0) * tp2 + T(0.0 / 6.0)));
+}
+// BsplineFunctor::evaluateV for one pair inside the cutoff
+template <typename T> __device__ __forceinline__ T functor_v(const FunctorT<T>& f, T r)
+{
+  r *= f.dinv;
+  const int i = (int)r;
+  const T t = r - T(i), tp1 = t * t, tp0 = tp1 * t, tp2 = t;
+  const T d1 = f.c[i] * (T(-1.0 / 6.0) * tp0 + T(3.0 / 6.0) * tp1 + T(-3.0 / 6.0) * tp2 + T(1.0 / 6.0));
+  const T d2 = f.c[i + 1] * (T(3.0 / 6.0) * tp0 + T(-6.0 / 6.0) * tp1 + T(0.0 / 6.0) * tp2 + T(4.0 / 6.0));
+  const T d3 = f.c[i + 2] * (T(-3.0 / 6.0) * tp0 + T(3.0 / 6.0) * tp1 + T(3.0 / 6.0) * tp2 + T(1.0 / 6.0));
+  const T d4 = f.c[i + 3] * (T(1.0 / 6.0) * tp0 + T(0.0 / 6.0) * tp1 + T(0.0 / 6.0) * tp2 + T(0.0 / 6.0));
+  return d1 + d2 + d3 + d4;
+}
+
+// --------------------------------------------------------- B-spline SPO --
+// computeLocationAndFractional + compute_prefactors for a Cartesian point
+// (one thread).  Fractional coordinates are formed in FP64 in both forms.
+template <typename T> __device__ void spline_locate(const DevSystem* __restrict__ s, const double* pos, SplineSmem<T>& sp)
+{
+  double u[3];
+  for (int d = 0; d < 3; ++d)
+  {
+    u[d] = pos[0] * s->spoG[d] + pos[1] * s->spoG[3 + d] + pos[2] * s->spoG[6 + d];
+    if (-DBL_EPSILON < u[d] && u[d] < 0)
+      u[d] = 0.0;
+    else
+      u[d] -= floor(u[d]);
+  }
+  long long base = 0;
+  const long long strides[3] = {s->xs, s->ys, s->zs};
+  for (int d = 0; d < 3; ++d)
+  {
+    const double x = u[d] * s->dinv[d];
+    int ind;
+    double t;
+    if (x < 0)
+    {
+      ind = 0;
+      t   = 0.0;
+    }
+    else
+    {
+      const double ip = floor(x);
+      t               = x - ip;
+      ind             = (int)ip;
+      if (ind > s->grid[d] - 1)
+      {
+        ind = s->grid[d] - 1;
+        t   = 1.0 - DBL_EPSILON;
+      }
+    }
+    base += (long long)ind * strides[d];
+    sp.a[d][0]   = (T)(((-1.0 / 6.0 * t + 3.0 / 6.0) * t + -3.0 / 6.0) * t + 1.0 / 6.0);
+    sp.a[d][1]   = (T)(((3.0 / 6.0 * t + -6.0 / 6.0) * t + 0.0 / 6.0) * t + 4.0 / 6.0);
+    sp.a[d][2]   = (T)(((-3.0 / 6.0 * t + 3.0 / 6.0) * t + 3.0 / 6.0) * t + 1.0 / 6.0);
+    sp.a[d][3]   = (T)(((1.0 / 6.0 * t + 0.0 / 6.0) * t + 0.0 / 6.0) * t + 0.0 / 6.0);
+    sp.da[d][0]  = (T)((-0.5 * t + 1.0) * t + -0.5);
+    sp.da[d][1]  = (T)((1.5 * t + -2.0) * t + 0.0);
+    sp.da[d][2]  = (T)((-1.5 * t + 1.0) * t + 0.5);
+    sp.da[d][3]  = (T)((0.5 * t + 0.0) * t + 0.0);
+    sp.d2a[d][0] = (T)(-1.0 * t + 1.0);
+    sp.d2a[d][1] = (T)(3.0 * t + -2.0);
+    sp.d2a[d][2] = (T)(-3.0 * t + 1.0);
+    sp.d2a[d][3] = (T)(1.0 * t + 0.0);
+  }
+  sp.base = base;
+}
+
+template <typename T> struct SplineOut
+{
+  static constexpr int VW = Vec16<T>::width;
+  T v[VW], gx[VW], gy[VW], gz[VW], hxx[VW], hxy[VW], hxz[VW], hyy[VW], hyz[VW], hzz[VW];
+};
+
+// evaluate_vgh for the VW orbitals starting at element e0 (16-byte vector)
+template <typename T, bool FULL>
+__device__ __forceinline__ void spline_eval(const T* __restrict__ coefs, long long xs, long long ys, long long zs,
+                                            const SplineSmem<T>& sp, const double* dinv, int e0, SplineOut<T>& o)
+{
+  using V              = typename Vec16<T>::type;
+  constexpr int VW     = Vec16<T>::width;
+#pragma unroll
+  for (int e = 0; e < VW; ++e)
+    o.v[e] = o.gx[e] = o.gy[e] = o.gz[e] = o.hxx[e] = o.hxy[e] = o.hxz[e] = o.hyy[e] = o.hyz[e] = o.hzz[e] = T(0);
+  const T* c0p = coefs + sp.base + e0;
+#pragma unroll 1
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+    {
+      const T* p = c0p + i * xs + j * ys;
+      V c[4];
+#pragma unroll
+      for (int z = 0; z < 4; ++z)
+        c[z] = __ldg(reinterpret_cast<const V*>(p + z * zs));
+      const T pre20 = sp.d2a[0][i] * sp.a[1][j];
+      const T pre10 = sp.da[0][i] * sp.a[1][j];
+      const T pre00 = sp.a[0][i] * sp.a[1][j];
+      const T pre11 = sp.da[0][i] * sp.da[1][j];
+      const T pre01 = sp.a[0][i] * sp.da[1][j];
+      const T pre02 = sp.a[0][i] * sp.d2a[1][j];
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+      {
+        const T v0 = reinterpret_cast<const T*>(&c[0])[e];
+        const T v1 = reinterpret_cast<const T*>(&c[1])[e];
+        const T v2 = reinterpret_cast<const T*>(&c[2])[e];
+        const T v3 = reinterpret_cast<const T*>(&c[3])[e];
+        const T sum0 = sp.a[2][0] * v0 + sp.a[2][1] * v1 + sp.a[2][2] * v2 + sp.a[2][3] * v3;
+        const T sum1 = sp.da[2][0] * v0 + sp.da[2][1] * v1 + sp.da[2][2] * v2 + sp.da[2][3] * v3;
+        const T sum2 = sp.d2a[2][0] * v0 + sp.d2a[2][1] * v1 + sp.d2a[2][2] * v2 + sp.d2a[2][3] * v3;
+        o.hxx[e] += pre20 * sum0;
+        o.hyy[e] += pre02 * sum0;
+        o.hzz[e] += pre00 * sum2;
+        if (FULL)
+        {
+          o.hxy[e] += pre11 * sum0;
+          o.hxz[e] += pre10 * sum1;
+          o.hyz[e] += pre01 * sum1;
+        }
+        o.gx[e] += pre10 * sum0;
+        o.gy[e] += pre01 * sum0;
+        o.gz[e] += pre00 * sum1;
+        o.v[e] += pre00 * sum0;
+      }
+    }
+  const T dx = (T)dinv[0], dy = (T)dinv[1], dz = (T)dinv[2];
+#pragma unroll
+  for (int e = 0; e < VW; ++e)
+  {
+    o.gx[e] *= dx;
+    o.gy[e] *= dy;
+    o.gz[e] *= dz;
+    o.hxx[e] *= dx * dx;
+    o.hyy[e] *= dy * dy;
+    o.hzz[e] *= dz * dz;
+    if (FULL)
+    {
+      o.hxy[e] *= dx * dy;
+      o.hxz[e] *= dx * dz;
+      o.hyz[e] *= dy * dz;
+    }
+  }
+}
+
+// evaluate_v (values only) for VW orbitals at e0
+template <typename T>
+__device__ __forceinline__ void spline_eval_v(const T* __restrict__ coefs, long long xs, long long ys, long long zs,
+                                              const SplineSmem<T>& sp, int e0, T* out)
+{
+  using V          = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+#pragma unroll
+  for (int e = 0; e < VW; ++e)
+    out[e] = T(0);
+  const T* c0p = coefs + sp.base + e0;
+#pragma unroll 1
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+    {
+      const T* p = c0p + i * xs + j * ys;
+      V c[4];
+#pragma unroll
+      for (int z = 0; z < 4; ++z)
+        c[z] = __ldg(reinterpret_cast<const V*>(p + z * zs));
+      const T pre00 = sp.a[0][i] * sp.a[1][j];
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+        out[e] += pre00 *
+            (sp.a[2][0] * reinterpret_cast<const T*>(&c[0])[e] + sp.a[2][1] * reinterpret_cast<const T*>(&c[1])[e] +
+             sp.a[2][2] * reinterpret_cast<const T*>(&c[2])[e] + sp.a[2][3] * reinterpret_cast<const T*>(&c[3])[e]);
+    }
+}
+
+// ------------------------------------------------------- determinant ----
+// DelayedUpdate::getInvRow: invRow = Ainv[r] - V^T (Binv^T (U Ainv[r])).
+// Stores the intermediate Binv^T p in row dc of Binv, as the reference does
+// (acceptRow reads it back).  Block-wide.
+template <typename T> __device__ void get_inv_row(const WV<T>& wv, MoveSmem& m, int s, int r, int dc)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const int nvec  = wv.npad / VW;
+  const T* arow   = wv.ainv(s) + (size_t)r * wv.npad;
+  if (dc == 0)
+  {
+    for (int q = tid; q < nvec; q += NT)
+      reinterpret_cast<Vt*>(wv.invRow)[q] = reinterpret_cast<const Vt*>(arow)[q];
+    return;
+  }
+  const T* U = wv.u(s);
+  const T* V = wv.v(s);
+  for (int d = wid; d < dc; d += nw)
+  {
+    const T* ud = U + (size_t)d * wv.npad;
+    double acc  = 0.0;
+    for (int j = lane; j < wv.npad; j += 32)
+      acc += (double)(ud[j] * arow[j]);
+    acc = warp_sum(acc);
+    if (lane == 0)
+      m.p[d] = acc;
+  }
+  __syncthreads();
+  double* B = wv.binv(s);
+  for (int a = tid; a < dc; a += NT)
+  {
+    double acc = 0.0;
+    for (int b = 0; b < dc; ++b)
+      acc += B[b * wv.k + a] * m.p[b];
+    m.wv[a] = acc;
+    if (dc < wv.k)
+      B[dc * wv.k + a] = acc;
+  }
+  __syncthreads();
+  for (int q = tid; q < nvec; q += NT)
+  {
+    Vt a = reinterpret_cast<const Vt*>(arow)[q];
+    T* ap = reinterpret_cast<T*>(&a);
+    double acc[VW];
+#pragma unroll
+    for (int e = 0; e < VW; ++e)
+      acc[e] = 0.0;
+    for (int d = 0; d < dc; ++d)
+    {
+      Vt vv = reinterpret_cast<const Vt*>(V + (size_t)d * wv.npad)[q];
+      const double wd = m.wv[d];
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+        acc[e] += (double)reinterpret_cast<T*>(&vv)[e] * wd;
+    }
+#pragma unroll
+    for (int e = 0; e < VW; ++e)
+      ap[e] = (T)((double)ap[e] - acc[e]);
+    reinterpret_cast<Vt*>(wv.invRow)[q] = a;
+  }
+}
+
+// Woodbury flush (DelayedUpdate::updateInvMat): with U2 = Binv V and
+// tm = Ainv U^T - E,  Ainv <- Ainv - tm U2.  Row blocks of Ainv are
+// independent, so each is read for tm and then updated in place.
+template <typename T> struct FlushTile
+{
+  static constexpr int BM = 32;
+  static constexpr int BK = sizeof(T) == 4 ? 64 : 32;
+};
+template <typename T> __host__ __device__ constexpr size_t flush_smem_bytes()
+{
+  return sizeof(T) * ((size_t)FlushTile<T>::BM * (FlushTile<T>::BK + 1) + (size_t)MAXK * (FlushTile<T>::BK + 1) +
+                      (size_t)FlushTile<T>::BM * (MAXK + 1));
+}
+
+template <typename T> __device__ void flush(const WV<T>& wv, MoveSmem& m, int s, T* smem)
+{
+  using Vt           = typename Vec16<T>::type;
+  constexpr int VW   = Vec16<T>::width;
+  constexpr int BM   = FlushTile<T>::BM, BK = FlushTile<T>::BK;
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const int dc = wv.dcount[s];
+  __syncthreads();
+  if (dc == 0)
+    return;
+  const int npad = wv.npad, n = wv.n, k = wv.k;
+  const double* B = wv.binv(s);
+  const T* U = wv.u(s);
+  const T* V = wv.v(s);
+  T* A       = wv.ainv(s);
+  const int* dl = wv.dl(s);
+  // U2[b][j] = sum_a Binv[b][a] V[a][j]
+  for (int bb = 0; bb < dc; bb += 16)
+    for (int j = tid; j < npad; j += NT)
+    {
+      double acc[16];
+#pragma unroll
+      for (int b = 0; b < 16; ++b)
+        acc[b] = 0.0;
+      for (int a = 0; a < dc; ++a)
+      {
+        const double va = (double)V[(size_t)a * npad + j];
+#pragma unroll
+        for (int b = 0; b < 16; ++b)
+          if (bb + b < dc)
+            acc[b] += B[(bb + b) * k + a] * va;
+      }
+#pragma unroll
+      for (int b = 0; b < 16; ++b)
+        if (bb + b < dc)
+          wv.U2[(size_t)(bb + b) * npad + j] = (T)acc[b];
+    }
+  __syncthreads();
+  T* As = smem;                        // [BM][BK+1]
+  T* Us = As + BM * (BK + 1);          // [MAXK][BK+1]
+  T* tm = Us + MAXK * (BK + 1);        // [BM][MAXK+1]
+  constexpr int MD = 16;               // d-values per thread in GEMM1 (nw >= 4)
+  const int nvec = npad / VW;
+  for (int i0 = 0; i0 < n; i0 += BM)
+  {
+    const int rows = min(BM, n - i0);
+    // GEMM1: tm[i][d] = sum_j Ainv[i0+i][j] U[d][j]; thread (i = lane, d = wid + m*nw)
+    T acc[MD];
+#pragma unroll
+    for (int mm = 0; mm < MD; ++mm)
+      acc[mm] = T(0);
+    for (int j0 = 0; j0 < npad; j0 += BK)
+    {
+      for (int idx = tid; idx < BM * BK; idx += NT)
+      {
+        const int i = idx / BK, kk = idx % BK;
+        As[i * (BK + 1) + kk] = (i < rows && j0 + kk < npad) ? A[(size_t)(i0 + i) * npad + j0 + kk] : T(0);
+      }
+      for (int idx = tid; idx < dc * BK; idx += NT)
+      {
+        const int d = idx / BK, kk = idx % BK;
+        Us[d * (BK + 1) + kk] = (j0 + kk < npad) ? U[(size_t)d * npad + j0 + kk] : T(0);
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int kk = 0; kk < BK; ++kk)
+      {
+        const T a = As[lane * (BK + 1) + kk];
+#pragma unroll
+        for (int mm = 0; mm < MD; ++mm)
+        {
+          const int d = wid + mm * nw;
+          if (d < dc)
+            acc[mm] += a * Us[d * (BK + 1) + kk];
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int mm = 0; mm < MD; ++mm)
+    {
+      const int d = wid + mm * nw;
+      if (d < dc)
+        tm[lane * (MAXK + 1) + d] = acc[mm] - ((dl[d] == i0 + lane) ? T(1) : T(0));
+    }
+    __syncthreads();
+    // GEMM3: Ainv[i0+i][j] -= sum_d tm[i][d] U2[d][j], 8 rows per pass
+    for (int q = tid; q < nvec; q += NT)
+      for (int rg = 0; rg < rows; rg += 8)
+      {
+        T c[8][VW];
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            c[rr][e] = T(0);
+        for (int d = 0; d < dc; ++d)
+        {
+          Vt u2 = reinterpret_cast<const Vt*>(wv.U2 + (size_t)d * npad)[q];
+#pragma unroll
+          for (int rr = 0; rr < 8; ++rr)
+          {
+            const T t = tm[(rg + rr) * (MAXK + 1) + d];
+#pragma unroll
+            for (int e = 0; e < VW; ++e)
+              c[rr][e] += t * reinterpret_cast<T*>(&u2)[e];
+          }
+        }
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr)
+          if (rg + rr < rows)
+          {
+            Vt* ap = reinterpret_cast<Vt*>(A + (size_t)(i0 + rg + rr) * npad) + q;
+            Vt a   = *ap;
+#pragma unroll
+            for (int e = 0; e < VW; ++e)
+              reinterpret_cast<T*>(&a)[e] -= c[rr][e];
+            *ap = a;
+          }
+      }
+    __syncthreads();
+  }
+  if (tid == 0)
+    wv.dcount[s] = 0;
+  __syncthreads();
+}
+
+// DiracDeterminant::acceptMove + DelayedUpdate::acceptRow.  psiV (and the
+// derivative rows when `partial`) come from the move scratch.  Block-wide.
+template <typename T>
+__device__ void det_accept(const WV<T>& wv, MoveSmem& m, int s, int r, double ratio, bool partial, bool track_log,
+                           T* smem)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const int npad = wv.npad, nvec = npad / VW, k = wv.k;
+  const int dc = wv.dcount[s];
+  T* arow      = wv.ainv(s) + (size_t)r * npad;
+  T* Vd        = wv.v(s) + (size_t)dc * npad;
+  T* Ud        = wv.u(s) + (size_t)dc * npad;
+  for (int q = tid; q < nvec; q += NT)
+  {
+    reinterpret_cast<Vt*>(Vd)[q] = reinterpret_cast<const Vt*>(arow)[q];
+    reinterpret_cast<Vt*>(Ud)[q] = reinterpret_cast<const Vt*>(wv.psiV)[q];
+    if (partial)
+    {
+      for (int c = 0; c < 3; ++c)
+        reinterpret_cast<Vt*>(wv.dpsi(s) + ((size_t)r * 3 + c) * npad)[q] =
+            reinterpret_cast<const Vt*>(wv.dpsiV + (size_t)c * npad)[q];
+      reinterpret_cast<Vt*>(wv.d2psi(s) + (size_t)r * npad)[q] = reinterpret_cast<const Vt*>(wv.d2psiV)[q];
+    }
+  }
+  if (tid == 0)
+  {
+    if (track_log)
+    {
+      wv.det_phase[s] += (ratio > 0) ? 0.0 : kPi;
+      wv.det_log[s] += log(fabs(ratio));
+    }
+    wv.dl(s)[dc] = r;
+  }
+  __syncthreads();
+  // p[d] = -V[d] . psiV  for d <= dc
+  const T* Vs = wv.v(s);
+  for (int d = wid; d <= dc; d += nw)
+  {
+    const T* vd = Vs + (size_t)d * npad;
+    double acc  = 0.0;
+    for (int j = lane; j < npad; j += 32)
+      acc += (double)(vd[j] * wv.psiV[j]);
+    acc = warp_sum(acc);
+    if (lane == 0)
+      m.p[d] = -acc;
+  }
+  __syncthreads();
+  double* B = wv.binv(s);
+  if (tid == 0)
+  {
+    double y = -m.p[dc];
+    for (int i = 0; i < dc; i++)
+      y += B[dc * k + i] * m.p[i];
+    y              = 1.0 / y;
+    B[dc * k + dc] = y;
+    m.y            = y;
+  }
+  __syncthreads();
+  const double y = m.y;
+  for (int b = tid; b < dc; b += NT)
+  {
+    double acc = 0.0;
+    for (int a = 0; a < dc; ++a)
+      acc += B[b * k + a] * m.p[a];
+    m.col[b] = y * acc;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < dc * dc; idx += NT)
+  {
+    const int b = idx / dc, a = idx % dc;
+    B[b * k + a] -= B[dc * k + a] * m.col[b];
+  }
+  for (int b = tid; b < dc; b += NT)
+    B[b * k + dc] = m.col[b];
+  __syncthreads();
+  for (int i = tid; i < dc; i += NT)
+    B[dc * k + i] *= -y;
+  if (tid == 0)
+    wv.dcount[s] = dc + 1;
+  __syncthreads();
+  if (dc + 1 == k)
+    flush(wv, m, s, smem);
+}
+
+// ---------------------------------------------------------- Jastrows ----
+template <typename T> __device__ __forceinline__ int ion_group(const SysSmem<T>& ss, int c)
+{
+  int g = 0;
+  for (int h = 0; h < ss.n_groups; ++h)
+    if (c >= ss.gfirst[h] && c < ss.glast[h])
+      g = h;
+  return g;
+}
+
+// partial J1 sums over the ions for a position: curAt, grad[3], lap
+// (OneBodyJastrow::computeU3 + accumulateGL; the AB row is always flipped)
+template <typename T>
+__device__ void j1_partials(const SysSmem<T>& ss, const T* __restrict__ ions /*[3][I]*/, const double* pos, double* part)
+{
+  const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];
+  for (int c = threadIdx.x; c < ss.n_ions; c += blockDim.x)
+  {
+    T dx = (ions[c] - px) * T(-1), dy = (ions[ss.n_ions + c] - py) * T(-1), dz = (ions[2 * ss.n_ions + c] - pz) * T(-1);
+    const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+    dx *= T(-1), dy *= T(-1), dz *= T(-1);
+    const FunctorT<T>& f = ss.j1[ion_group(ss, c)];
+    if (r < f.cutoff)
+    {
+      T u, du, d2u;
+      functor_vgl(f, r, u, du, d2u);
+      part[0] += (double)u;
+      part[1] += (double)(du * dx);
+      part[2] += (double)(du * dy);
+      part[3] += (double)(du * dz);
+      part[4] += (double)(d2u + T(2) * du);
+    }
+  }
+}
+template <typename T>
+__device__ void j1_value(const SysSmem<T>& ss, const T* __restrict__ ions, const double* pos, double* part)
+{
+  const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];
+  for (int c = threadIdx.x; c < ss.n_ions; c += blockDim.x)
+  {
+    T dx = (ions[c] - px) * T(-1), dy = (ions[ss.n_ions + c] - py) * T(-1), dz = (ions[2 * ss.n_ions + c] - pz) * T(-1);
+    const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+    const FunctorT<T>& f = ss.j1[ion_group(ss, c)];
+    if (r < f.cutoff)
+      part[0] += (double)functor_v(f, r);
+  }
+}
+
+// partial J2 sums over the electrons for electron iel moved to pos:
+// sum u, sum du*dr (TwoBodyJastrow::ratioGrad with the move row, flip = iel)
+template <typename T>
+__device__ void j2_partials(const SysSmem<T>& ss, const T* __restrict__ Rs, int Npad, int iel, const double* pos,
+                            double* part, bool grads)
+{
+  const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];
+  const int gi = iel < ss.n_up ? 0 : 1;
+  for (int j = threadIdx.x; j < ss.n_elec; j += blockDim.x)
+  {
+    if (j == iel)
+      continue;
+    const T flip = j < iel ? T(1) : T(-1);
+    T dx = (Rs[j] - px) * flip, dy = (Rs[Npad + j] - py) * flip, dz = (Rs[2 * Npad + j] - pz) * flip;
+    const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+    const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+    if (r < f.cutoff)
+    {
+      if (grads)
+      {
+        T u, du, d2u;
+        functor_vgl(f, r, u, du, d2u);
+        dx *= flip, dy *= flip, dz *= flip;
+        part[0] += (double)u;
+        part[1] += (double)(du * dx);
+        part[2] += (double)(du * dy);
+        part[3] += (double)(du * dz);
+      }
+      else
+        part[0] += (double)functor_v(f, r);
+    }
+  }
+}
+
+// TwoBodyJastrow::acceptMove: update every electron's Uat, dUat, d2Uat with
+// the old (setActive) and new (move) rows of electron iel.  Block-wide.
+template <typename T>
+__device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, int iel)
+{
+  const T ox = (T)m.pos_old[0], oy = (T)m.pos_old[1], oz = (T)m.pos_old[2];
+  const T nx = (T)m.pos_new[0], ny = (T)m.pos_new[1], nz = (T)m.pos_new[2];
+  const int gi = iel < ss.n_up ? 0 : 1;
+  const int Npad = wv.Npad, N = wv.N;
+  const T* Rs = wv.Rs;
+  double part[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = threadIdx.x; j < N; j += blockDim.x)
+  {
+    if (j == iel)
+      continue;
+    const T flip = j < iel ? T(1) : T(-1);
+    const T rx = Rs[j], ry = Rs[Npad + j], rz = Rs[2 * Npad + j];
+    const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+    T odx = (rx - ox) * flip, ody = (ry - oy) * flip, odz = (rz - oz) * flip;
+    const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
+    odx *= flip, ody *= flip, odz *= flip;
+    T ndx = (rx - nx) * flip, ndy = (ry - ny) * flip, ndz = (rz - nz) * flip;
+    const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
+    ndx *= flip, ndy *= flip, ndz *= flip;
+    T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
+    if (ro < f.cutoff)
+      functor_vgl(f, ro, uo, duo, d2uo);
+    if (rn < f.cutoff)
+      functor_vgl(f, rn, un, dun, d2un);
+    const T newl = d2un + T(2) * dun;
+    const T dl   = d2uo + T(2) * duo - newl;
+    wv.Uat[j] += un - uo;
+    wv.d2Uat[j] += dl;
+    part[0] -= (double)newl;
+    const T ng0 = dun * ndx, ng1 = dun * ndy, ng2 = dun * ndz;
+    wv.dUat[j] -= ng0 - duo * odx;
+    wv.dUat[N + j] -= ng1 - duo * ody;
+    wv.dUat[2 * N + j] -= ng2 - duo * odz;
+    part[1] += (double)ng0;
+    part[2] += (double)ng1;
+    part[3] += (double)ng2;
+  }
+  block_sum<4>(part, m.red, m.sums);
+  if (threadIdx.x == 0)
+  {
+    wv.jlog[1] += (double)wv.Uat[iel] - m.curUat;
+    wv.Uat[iel]        = (T)m.curUat;
+    wv.dUat[iel]       = (T)m.sums[1];
+    wv.dUat[N + iel]   = (T)m.sums[2];
+    wv.dUat[2 * N + iel] = (T)m.sums[3];
+    wv.d2Uat[iel]      = (T)m.sums[0];
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------- evaluateGL -----
+// WaveFunction::evaluateGL (WaveFunction.cpp:261-279): G, L per electron and
+// the log values; warp per electron for the determinant row dots.
+template <typename T> __device__ void evaluate_gl(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, double* logpsi)
+{
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const int N = wv.N, npad = wv.npad;
+  for (int i = wid; i < N; i += nw)
+  {
+    double rv[3] = {0.0, 0.0, 0.0}, lap = 0.0;
+    if (DET)
+    {
+      const int s = i < ss.n_up ? 0 : 1, r = i - (s ? ss.n_up : 0);
+      const T* a  = wv.ainv(s) + (size_t)r * npad;
+      const T* dp = wv.dpsi(s) + (size_t)r * 3 * npad;
+      const T* d2 = wv.d2psi(s) + (size_t)r * npad;
+      for (int j = lane; j < npad; j += 32)
+      {
+        const double aj = (double)a[j];
+        rv[0] += aj * (double)dp[j];
+        rv[1] += aj * (double)dp[npad + j];
+        rv[2] += aj * (double)dp[2 * npad + j];
+        lap += aj * (double)d2[j];
+      }
+      rv[0] = warp_sum(rv[0]);
+      rv[1] = warp_sum(rv[1]);
+      rv[2] = warp_sum(rv[2]);
+      lap   = warp_sum(lap);
+    }
+    if (lane == 0)
+    {
+      double g[3] = {rv[0], rv[1], rv[2]};
+      double l    = lap - (rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+      if (J1)
+      {
+        for (int c = 0; c < 3; ++c)
+          g[c] += (double)wv.Grad[c * N + i];
+        l -= (double)wv.Lap[i];
+      }
+      if (J2)
+      {
+        for (int c = 0; c < 3; ++c)
+          g[c] += (double)wv.dUat[c * N + i];
+        l += (double)wv.d2Uat[i];
+      }
+      for (int c = 0; c < 3; ++c)
+        wv.G[3 * i + c] = g[c];
+      wv.L[i] = l;
+    }
+  }
+  double part[2] = {0.0, 0.0};
+  for (int i = tid; i < N; i += NT)
+  {
+    if (J1)
+      part[0] += (double)wv.Vat[i];
+    if (J2)
+      part[1] += (double)wv.Uat[i];
+  }
+  block_sum<2>(part, m.red, m.sums);
+  if (tid == 0)
+  {
+    wv.jlog[0] = J1 ? -m.sums[0] : 0.0;
+    wv.jlog[1] = J2 ? -0.5 * m.sums[1] : 0.0;
+    const double lp = (DET ? wv.det_log[0] + wv.det_log[1] : 0.0) + wv.jlog[0] + wv.jlog[1];
+    if (logpsi)
+      *logpsi = lp;
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------- RNG ------
+// Advance the walker's mt19937 stream by the draws of one substep:
+// N uniforms then 3N BoxMuller2 normals (miniqmc.cpp:424-425,
+// RandomGenerator.h:49-62).  Block-wide.
+__device__ inline void mt_block_twist(uint32_t* mt)
+{
+  const int tid = threadIdx.x, NT = blockDim.x;
+  uint32_t nv[4];
+  // phase 1: i in [0,227): old neighbours only
+  {
+    int c = 0;
+    for (int i = tid; i < MT_N - MT_M; i += NT, ++c)
+      nv[c] = mt_twist_one(mt[i], mt[i + 1], mt[i + MT_M]);
+    __syncthreads();
+    c = 0;
+    for (int i = tid; i < MT_N - MT_M; i += NT, ++c)
+      mt[i] = nv[c];
+    __syncthreads();
+  }
+  // phases 2,3: i in [227,454), [454,623): far operand from an earlier phase
+  for (int lo = MT_N - MT_M; lo < MT_N - 1; lo += MT_N - MT_M)
+  {
+    const int hi = min(lo + (MT_N - MT_M), MT_N - 1);
+    int c        = 0;
+    for (int i = lo + tid; i < hi; i += NT, ++c)
+      nv[c] = mt_twist_one(mt[i], mt[i + 1], mt[i + MT_M - MT_N]);
+    __syncthreads();
+    c = 0;
+    for (int i = lo + tid; i < hi; i += NT, ++c)
+      mt[i] = nv[c];
+    __syncthreads();
+  }
+  if (tid == 0)
+    mt[MT_N - 1] = mt_twist_one(mt[MT_N - 1], mt[0], mt[MT_M - 1]);
+  __syncthreads();
+}
+
+template <typename T> __device__ void rng_substep(const WV<T>& wv, int N)
+{
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int npairs = (3 * N + 1) / 2;
+  const int M      = 2 * N + 4 * npairs;
+  uint32_t* mt     = wv.mt;
+  __shared__ int s_mti;
+  if (tid == 0)
+    s_mti = (int)mt[MT_N];
+  __syncthreads();
+  int produced = 0;
+  while (produced < M)
+  {
+    if (s_mti >= MT_N)
+    {
+      mt_block_twist(mt);
+      if (tid == 0)
+        s_mti = 0;
+      __syncthreads();
+    }
+    const int mti = s_mti;
+    const int cnt = min(MT_N - mti, M - produced);
+    for (int t = tid; t < cnt; t += NT)
+      wv.words[produced + t] = mt_temper(mt[mti + t]);
+    produced += cnt;
+    __syncthreads();
+    if (tid == 0)
+      s_mti = mti + cnt;
+    __syncthreads();
+  }
+  if (tid == 0)
+    mt[MT_N] = (uint32_t)s_mti;
+  for (int i = tid; i < N; i += NT)
+    wv.ur[i] = canonical_double(wv.words[2 * i], wv.words[2 * i + 1]);
+  const uint32_t* wn = wv.words + 2 * N;
+  for (int p = tid; p < npairs; p += NT)
+  {
+    const double u1 = canonical_double(wn[4 * p], wn[4 * p + 1]);
+    const double u2 = canonical_double(wn[4 * p + 2], wn[4 * p + 3]);
+    const double t1 = __dsub_rn(1.0, __dmul_rn(0.9999999999, u1));
+    const double rr = sqrt(__dmul_rn(-2.0, log(t1)));
+    const double an = __dmul_rn(6.283185306, u2);
+    wv.delta[2 * p] = __dmul_rn(rr, cos(an));
+    if (2 * p + 1 < 3 * N)
+      wv.delta[2 * p + 1] = __dmul_rn(rr, sin(an));
+  }
+  __syncthreads();
+}
+
+// --------------------------------------------------------- one move -----
+// evalGrad, makeMove, ratioGrad and the threshold accept of electron iel
+// (miniqmc.cpp:426-458).  Block-wide.
+template <typename T>
+__device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys, const WV<T>& wv, MoveSmem& m,
+                        SplineSmem<T>& sp, const T* __restrict__ ions, int iel, double accept_thr, double ur,
+                        const double* dlt, double* trace, T* smem)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const int s = iel < ss.n_up ? 0 : 1, r = iel - (s ? ss.n_up : 0);
+  const int npad = wv.npad, nvec = npad / VW;
+  if (tid == 0)
+  {
+    for (int c = 0; c < 3; ++c)
+    {
+      m.pos_old[c] = wv.R[3 * iel + c];
+      m.pos_new[c] = m.pos_old[c] + dlt[c];
+    }
+    m.accept = ur < accept_thr;
+    m.dc     = DET ? wv.dcount[s] : 0;
+    if (DET)
+      spline_locate(sys, m.pos_new, sp);
+  }
+  __syncthreads();
+  double part[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+    part[i] = 0.0;
+  if (DET)
+  {
+    get_inv_row(wv, m, s, r, m.dc);
+    const T* dprow = wv.dpsi(s) + (size_t)r * 3 * npad;
+    const T* coefs = (const T*)sys->coefs;
+    const long long xs = sys->xs, ys = sys->ys, zs = sys->zs;
+    const double dinv[3] = {sys->dinv[0], sys->dinv[1], sys->dinv[2]};
+    const bool trace_lap = ss.lap_mode == QMC_LAP_TRACE;
+    for (int q = tid; q < nvec; q += NT)
+    {
+      Vt iv = reinterpret_cast<const Vt*>(wv.invRow)[q];
+      const T* ivp = reinterpret_cast<const T*>(&iv);
+      for (int c = 0; c < 3; ++c)
+      {
+        Vt g = reinterpret_cast<const Vt*>(dprow + (size_t)c * npad)[q];
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+          part[4 + c] += (double)(ivp[e] * reinterpret_cast<T*>(&g)[e]);
+      }
+      SplineOut<T> o;
+      spline_eval<T, false>(coefs, xs, ys, zs, sp, dinv, q * VW, o);
+      Vt pv, gxv, gyv, gzv, lv;
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+      {
+        reinterpret_cast<T*>(&pv)[e]  = o.v[e];
+        reinterpret_cast<T*>(&gxv)[e] = o.gx[e];
+        reinterpret_cast<T*>(&gyv)[e] = o.gy[e];
+        reinterpret_cast<T*>(&gzv)[e] = o.gz[e];
+        reinterpret_cast<T*>(&lv)[e]  = trace_lap ? o.hxx[e] + o.hyy[e] + o.hzz[e] : o.hxx[e];
+        part[0] += (double)(ivp[e] * o.v[e]);
+        part[1] += (double)(ivp[e] * o.gx[e]);
+        part[2] += (double)(ivp[e] * o.gy[e]);
+        part[3] += (double)(ivp[e] * o.gz[e]);
+      }
+      reinterpret_cast<Vt*>(wv.psiV)[q]            = pv;
+      reinterpret_cast<Vt*>(wv.dpsiV)[q]           = gxv;
+      reinterpret_cast<Vt*>(wv.dpsiV + npad)[q]    = gyv;
+      reinterpret_cast<Vt*>(wv.dpsiV + 2 * npad)[q] = gzv;
+      reinterpret_cast<Vt*>(wv.d2psiV)[q]          = lv;
+    }
+  }
+  if (J1)
+    j1_partials(ss, ions, m.pos_new, part + 7);
+  if (J2)
+    j2_partials(ss, wv.Rs, wv.Npad, iel, m.pos_new, part + 12, true);
+  block_sum<16>(part, m.red, m.sums);
+  if (tid == 0)
+  {
+    const double* S = m.sums;
+    const double rdet = DET ? S[0] : 1.0;
+    double ratio      = rdet;
+    double gn[3], g0[3];
+    for (int c = 0; c < 3; ++c)
+    {
+      gn[c] = DET ? (1.0 / rdet) * S[1 + c] : 0.0;
+      g0[c] = DET ? S[4 + c] : 0.0;
+    }
+    m.ratio_det = rdet;
+    if (J1)
+    {
+      m.curAt  = S[7];
+      m.curLap = S[11];
+      for (int c = 0; c < 3; ++c)
+      {
+        m.curGrad[c] = S[8 + c];
+        gn[c] += S[8 + c];
+        g0[c] += (double)wv.Grad[c * wv.N + iel];
+      }
+      ratio *= exp((double)wv.Vat[iel] - m.curAt);
+    }
+    if (J2)
+    {
+      m.curUat = S[12];
+      for (int c = 0; c < 3; ++c)
+      {
+        gn[c] += S[13 + c];
+        g0[c] += (double)wv.dUat[c * wv.N + iel];
+      }
+      ratio *= exp((double)wv.Uat[iel] - m.curUat);
+    }
+    if (!isfinite(ratio))
+      atomicOr(wv.status, DEV_ERR_NONFINITE);
+    if (trace)
+    {
+      trace[0] = ratio;
+      trace[1] = gn[0], trace[2] = gn[1], trace[3] = gn[2];
+      trace[4] = g0[0], trace[5] = g0[1], trace[6] = g0[2];
+      trace[7] = m.accept ? 1.0 : 0.0;
+    }
+  }
+  __syncthreads();
+  if (m.accept)
+  {
+    if (DET)
+      det_accept(wv, m, s, r, m.ratio_det, true, true, smem);
+    if (J1 && tid == 0)
+    {
+      wv.jlog[0] += (double)wv.Vat[iel] - m.curAt;
+      wv.Vat[iel] = (T)m.curAt;
+      for (int c = 0; c < 3; ++c)
+        wv.Grad[c * wv.N + iel] = (T)m.curGrad[c];
+      wv.Lap[iel] = (T)m.curLap;
+    }
+    if (J2)
+      j2_accept(ss, wv, m, iel);
+    __syncthreads();
+    if (tid == 0)
+      for (int c = 0; c < 3; ++c)
+      {
+        wv.R[3 * iel + c]          = m.pos_new[c];
+        wv.Rs[c * wv.Npad + iel]   = (T)m.pos_new[c];
+      }
+    __syncthreads();
+  }
+}
+
+} // namespace qmc

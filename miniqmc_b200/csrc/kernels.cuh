@@ -1,0 +1,81 @@
+// kernels.cuh -- host-side launchers of the device code in kernels.cu.
+#pragma once
+
+#include "layout.cuh"
+
+namespace qmc
+{
+// One batch of walkers in a fused sweep launch.  Several tasks (walkers of
+// different systems) may share one launch; each CTA runs one walker.
+struct SweepTask
+{
+  const DevSystem* sys; // device pointer
+  DevWalkers dw;
+  int rng_mode;         // QMC_RNG_*
+  const double* ur;     // device [W][nsub][N] for QMC_RNG_HOST
+  const double* delta;  // device [W][nsub][N][3]
+  double* trace;        // device [W][nsub][N][8] or null
+  int first_block;      // first CTA of this task in the launch
+};
+
+struct LaunchCfg
+{
+  int threads;
+  size_t smem;
+};
+
+// fused sweep: one MC step (n_substeps x N moves + completeUpdates, then
+// evaluateGL) for every walker of every task
+cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st);
+
+// evaluateLog pieces
+cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu,
+                              cudaStream_t st);
+cudaError_t launch_gj_inverse(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads, int n_spins,
+                              cudaStream_t st);
+cudaError_t launch_jastrow_recompute(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads,
+                                     cudaStream_t st);
+cudaError_t launch_gl(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads, cudaStream_t st);
+cudaError_t launch_sync_rs(bool fp32, const DevWalkers& dw, cudaStream_t st);
+
+// drop-in verbs (all walkers of a batch, same electron)
+enum VerbOp
+{
+  VERB_MAKE_MOVE = 0,
+  VERB_EVAL_GRAD,
+  VERB_RATIO_GRAD,
+  VERB_RATIO,
+  VERB_WF_ACCEPT,
+  VERB_PSET_ACCEPT,
+  VERB_COMPLETE,
+  VERB_TEMP_ROWS,
+  VERB_SET_ACTIVE
+};
+struct VerbArgs
+{
+  int op, iat;
+  const double* displ;   // [W][3] device
+  const int* flags;      // [W] device
+  double* aa_r;          // temp-row outputs (device), may be null
+  double* aa_dr;
+  double* ab_r;
+  double* ab_dr;
+};
+cudaError_t launch_verb(bool fp32, const DevSystem* sys, const DevWalkers& dw, const VerbArgs& a, int threads,
+                        int max_k, cudaStream_t st);
+
+// standalone SPO evaluation at arbitrary points (check_spo)
+cudaError_t launch_spo_points(bool fp32, const DevSystem* sys, int n_pos, const double* pos, double* v,
+                              double* g, double* h, bool values_only, cudaStream_t st);
+
+// DelayedUpdate engine on one matrix (W = 1 batch view)
+cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, int max_k, cudaStream_t st);
+enum DetEngineOp
+{
+  DETENG_GET_INV_ROW = 0,
+  DETENG_ACCEPT_ROW  = 1,
+  DETENG_UPDATE      = 2
+};
+
+} // namespace qmc

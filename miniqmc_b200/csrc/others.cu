@@ -1,0 +1,780 @@
+// others.cu -- drop-in verb kernels, the evaluateLog pipeline (SPO matrix,
+// FP64 Gauss-Jordan inverse, Jastrow recompute, evaluateGL), SPO evaluation
+// at arbitrary points and the DelayedUpdate engine kernel.
+#include "device.cuh"
+
+namespace qmc
+{
+// ------------------------------------------------------------- verbs ----
+// One CTA per walker.  The per-move scalars live in MoveState between calls.
+template <typename T>
+__global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__ sys, DevWalkers dw, VerbArgs a)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  __shared__ SysSmem<T> ss;
+  __shared__ MoveSmem m;
+  __shared__ SplineSmem<T> sp;
+  __shared__ int s_invrow, s_partial, s_jpartial, s_active, s_flag;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  T* smem     = reinterpret_cast<T*>(dyn);
+  const int w = blockIdx.x, tid = threadIdx.x, NT = blockDim.x;
+  load_sys(sys, ss);
+  const WV<T> wv = make_wv<T>(dw, w);
+  MoveState* ms  = wv.ms;
+  const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const int iat = a.iat;
+  const int s = iat < ss.n_up ? 0 : 1, r = iat - (s ? ss.n_up : 0);
+  const int npad = wv.npad, nvec = npad / VW, N = wv.N;
+  const T* ions = (const T*)sys->ion_soa;
+  if (tid == 0)
+  {
+    s_invrow   = ms->invrow_id[s];
+    s_partial  = ms->partial[s];
+    s_jpartial = ms->j_partial;
+    s_active   = ms->active;
+    s_flag     = a.flags ? a.flags[w] : 1;
+    for (int c = 0; c < 3; ++c)
+    {
+      m.pos_new[c] = ms->pos[c];
+      m.pos_old[c] = wv.R[3 * iat + c];
+    }
+  }
+  __syncthreads();
+  switch (a.op)
+  {
+  case VERB_SET_ACTIVE:
+    break;
+  case VERB_MAKE_MOVE:
+    if (tid == 0)
+    {
+      ms->active = iat;
+      for (int c = 0; c < 3; ++c)
+        ms->pos[c] = wv.R[3 * iat + c] + a.displ[3 * w + c];
+    }
+    break;
+  case VERB_EVAL_GRAD:
+  {
+    double part[3] = {0.0, 0.0, 0.0};
+    if (DET)
+    {
+      get_inv_row(wv, m, s, r, wv.dcount[s]);
+      const T* dprow = wv.dpsi(s) + (size_t)r * 3 * npad;
+      for (int q = tid; q < nvec; q += NT)
+      {
+        Vt iv = reinterpret_cast<const Vt*>(wv.invRow)[q];
+        for (int c = 0; c < 3; ++c)
+        {
+          Vt g = reinterpret_cast<const Vt*>(dprow + (size_t)c * npad)[q];
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            part[c] += (double)(reinterpret_cast<T*>(&iv)[e] * reinterpret_cast<T*>(&g)[e]);
+        }
+      }
+    }
+    block_sum<3>(part, m.red, m.sums);
+    if (tid == 0)
+    {
+      if (DET)
+        ms->invrow_id[s] = r;
+      for (int c = 0; c < 3; ++c)
+      {
+        double g = m.sums[c];
+        if (J1)
+          g += (double)wv.Grad[c * N + iat];
+        if (J2)
+          g += (double)wv.dUat[c * N + iat];
+        dw.out_grad[3 * w + c] = g;
+      }
+    }
+    break;
+  }
+  case VERB_RATIO_GRAD:
+  case VERB_RATIO:
+  {
+    const bool grads = a.op == VERB_RATIO_GRAD;
+    if (s_active != iat)
+    {
+      if (tid == 0)
+        atomicOr(wv.status, DEV_ERR_STATE);
+      break;
+    }
+    double part[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      part[i] = 0.0;
+    if (DET)
+    {
+      if (tid == 0)
+        spline_locate(sys, m.pos_new, sp);
+      if (s_invrow != r)
+        get_inv_row(wv, m, s, r, wv.dcount[s]);
+      __syncthreads();
+      const T* coefs = (const T*)sys->coefs;
+      const double dinv[3] = {sys->dinv[0], sys->dinv[1], sys->dinv[2]};
+      for (int q = tid; q < nvec; q += NT)
+      {
+        Vt iv        = reinterpret_cast<const Vt*>(wv.invRow)[q];
+        const T* ivp = reinterpret_cast<const T*>(&iv);
+        if (grads)
+        {
+          SplineOut<T> o;
+          spline_eval<T, false>(coefs, sys->xs, sys->ys, sys->zs, sp, dinv, q * VW, o);
+          for (int e = 0; e < VW; ++e)
+          {
+            const int j = q * VW + e;
+            wv.psiV[j]            = o.v[e];
+            wv.dpsiV[j]           = o.gx[e];
+            wv.dpsiV[npad + j]    = o.gy[e];
+            wv.dpsiV[2 * npad + j] = o.gz[e];
+            wv.d2psiV[j] = ss.lap_mode == QMC_LAP_TRACE ? o.hxx[e] + o.hyy[e] + o.hzz[e] : o.hxx[e];
+            part[0] += (double)(ivp[e] * o.v[e]);
+            part[1] += (double)(ivp[e] * o.gx[e]);
+            part[2] += (double)(ivp[e] * o.gy[e]);
+            part[3] += (double)(ivp[e] * o.gz[e]);
+          }
+        }
+        else
+        {
+          T v[VW];
+          spline_eval_v(coefs, sys->xs, sys->ys, sys->zs, sp, q * VW, v);
+          for (int e = 0; e < VW; ++e)
+          {
+            wv.psiV[q * VW + e] = v[e];
+            part[0] += (double)(ivp[e] * v[e]);
+          }
+        }
+      }
+    }
+    if (J1)
+    {
+      if (grads)
+        j1_partials(ss, ions, m.pos_new, part + 7);
+      else
+        j1_value(ss, ions, m.pos_new, part + 7);
+    }
+    if (J2)
+      j2_partials(ss, wv.Rs, wv.Npad, iat, m.pos_new, part + 12, grads);
+    block_sum<16>(part, m.red, m.sums);
+    if (tid == 0)
+    {
+      const double* S = m.sums;
+      const double rdet = DET ? S[0] : 1.0;
+      double ratio      = rdet, gn[3] = {0.0, 0.0, 0.0};
+      if (DET)
+      {
+        ms->cur_ratio[s] = rdet;
+        ms->invrow_id[s] = r;
+        ms->partial[s]   = grads ? 1 : 0;
+        if (grads)
+          for (int c = 0; c < 3; ++c)
+            gn[c] = (1.0 / rdet) * S[1 + c];
+      }
+      ms->j_partial = grads ? 1 : 0;
+      if (J1)
+      {
+        ms->j1_curAt = S[7];
+        if (grads)
+        {
+          ms->j1_curLap = S[11];
+          for (int c = 0; c < 3; ++c)
+          {
+            ms->j1_curGrad[c] = S[8 + c];
+            gn[c] += S[8 + c];
+          }
+        }
+        ratio *= exp((double)wv.Vat[iat] - S[7]);
+      }
+      if (J2)
+      {
+        ms->j2_curUat = S[12];
+        if (grads)
+          for (int c = 0; c < 3; ++c)
+            gn[c] += S[13 + c];
+        ratio *= exp((double)wv.Uat[iat] - S[12]);
+      }
+      if (!isfinite(ratio))
+        atomicOr(wv.status, DEV_ERR_NONFINITE);
+      dw.out_ratio[w] = ratio;
+      for (int c = 0; c < 3; ++c)
+        dw.out_grad[3 * w + c] = gn[c];
+    }
+    break;
+  }
+  case VERB_WF_ACCEPT:
+  {
+    if (!s_flag)
+      break;
+    if (s_active != iat)
+    {
+      if (tid == 0)
+        atomicOr(wv.status, DEV_ERR_STATE);
+      break;
+    }
+    if (DET)
+    {
+      det_accept(wv, m, s, r, ms->cur_ratio[s], s_partial != 0, true, smem);
+      if (tid == 0)
+      {
+        ms->invrow_id[s] = -1;
+        ms->cur_ratio[s] = 1.0;
+      }
+    }
+    if (J1)
+    {
+      if (!s_jpartial)
+      {
+        double part[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        j1_partials(ss, ions, m.pos_new, part);
+        block_sum<5>(part, m.red, m.sums);
+        if (tid == 0)
+        {
+          ms->j1_curLap = m.sums[4];
+          for (int c = 0; c < 3; ++c)
+            ms->j1_curGrad[c] = m.sums[1 + c];
+        }
+      }
+      if (tid == 0)
+      {
+        wv.jlog[0] += (double)wv.Vat[iat] - ms->j1_curAt;
+        wv.Vat[iat] = (T)ms->j1_curAt;
+        for (int c = 0; c < 3; ++c)
+          wv.Grad[c * N + iat] = (T)ms->j1_curGrad[c];
+        wv.Lap[iat] = (T)ms->j1_curLap;
+      }
+    }
+    if (J2)
+    {
+      if (tid == 0)
+        m.curUat = ms->j2_curUat;
+      __syncthreads();
+      j2_accept(ss, wv, m, iat);
+    }
+    break;
+  }
+  case VERB_PSET_ACCEPT:
+    if (tid == 0)
+    {
+      if (s_flag)
+      {
+        if (s_active != iat)
+          atomicOr(wv.status, DEV_ERR_STATE);
+        else
+          for (int c = 0; c < 3; ++c)
+          {
+            wv.R[3 * iat + c]        = ms->pos[c];
+            wv.Rs[c * wv.Npad + iat] = (T)ms->pos[c];
+          }
+      }
+      ms->active = -1;
+    }
+    break;
+  case VERB_COMPLETE:
+    if (DET)
+    {
+      flush(wv, m, 0, smem);
+      flush(wv, m, 1, smem);
+      if (tid == 0)
+        ms->invrow_id[0] = ms->invrow_id[1] = -1;
+    }
+    break;
+  case VERB_TEMP_ROWS:
+  {
+    const int act = s_active;
+    const T px = (T)m.pos_new[0], py = (T)m.pos_new[1], pz = (T)m.pos_new[2];
+    if (a.aa_r || a.aa_dr)
+      for (int j = tid; j < N; j += NT)
+      {
+        const T flip = j < act ? T(1) : T(-1);
+        T dx = (wv.Rs[j] - px) * flip, dy = (wv.Rs[wv.Npad + j] - py) * flip, dz = (wv.Rs[2 * wv.Npad + j] - pz) * flip;
+        const T rr = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+        if (a.aa_r)
+          a.aa_r[(size_t)w * N + j] = (double)rr;
+        if (a.aa_dr)
+        {
+          a.aa_dr[((size_t)w * N + j) * 3]     = (double)(dx * flip);
+          a.aa_dr[((size_t)w * N + j) * 3 + 1] = (double)(dy * flip);
+          a.aa_dr[((size_t)w * N + j) * 3 + 2] = (double)(dz * flip);
+        }
+      }
+    const int I = ss.n_ions;
+    if (a.ab_r || a.ab_dr)
+      for (int c = tid; c < I; c += NT)
+      {
+        T dx = (ions[c] - px) * T(-1), dy = (ions[I + c] - py) * T(-1), dz = (ions[2 * I + c] - pz) * T(-1);
+        const T rr = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+        if (a.ab_r)
+          a.ab_r[(size_t)w * I + c] = (double)rr;
+        if (a.ab_dr)
+        {
+          a.ab_dr[((size_t)w * I + c) * 3]     = (double)(-dx);
+          a.ab_dr[((size_t)w * I + c) * 3 + 1] = (double)(-dy);
+          a.ab_dr[((size_t)w * I + c) * 3 + 2] = (double)(-dz);
+        }
+      }
+    break;
+  }
+  }
+}
+
+// --------------------------------------------------- evaluateLog parts --
+// SPOSet::evaluate_notranspose for every electron of every walker: the
+// FP64 Slater matrices (for the inverse) and the derivative rows.
+template <typename T>
+__global__ void __launch_bounds__(256) spo_matrix_kernel(const DevSystem* __restrict__ sys, DevWalkers dw, int want_lu)
+{
+  constexpr int VW = Vec16<T>::width;
+  __shared__ SplineSmem<T> sp;
+  __shared__ double pos[3];
+  const int i = blockIdx.x, w = blockIdx.y;
+  const WV<T> wv = make_wv<T>(dw, w);
+  if (threadIdx.x == 0)
+  {
+    for (int c = 0; c < 3; ++c)
+      pos[c] = wv.R[3 * i + c];
+    spline_locate(sys, pos, sp);
+  }
+  __syncthreads();
+  const int s = i < sys->n_up ? 0 : 1, r = i - (s ? sys->n_up : 0);
+  const int npad = wv.npad, nvec = npad / VW;
+  const double dinv[3] = {sys->dinv[0], sys->dinv[1], sys->dinv[2]};
+  const bool trace_lap = sys->lap_mode == QMC_LAP_TRACE;
+  T* dp  = wv.dpsi(s) + (size_t)r * 3 * npad;
+  T* d2p = wv.d2psi(s) + (size_t)r * npad;
+  double* lrow = want_lu ? wv.lu + ((size_t)s * wv.n + r) * npad : nullptr;
+  for (int q = threadIdx.x; q < nvec; q += blockDim.x)
+  {
+    SplineOut<T> o;
+    spline_eval<T, false>((const T*)sys->coefs, sys->xs, sys->ys, sys->zs, sp, dinv, q * VW, o);
+    for (int e = 0; e < VW; ++e)
+    {
+      const int j = q * VW + e;
+      if (lrow)
+        lrow[j] = (double)o.v[e];
+      dp[j]            = o.gx[e];
+      dp[npad + j]     = o.gy[e];
+      dp[2 * npad + j] = o.gz[e];
+      d2p[j]           = trace_lap ? o.hxx[e] + o.hyy[e] + o.hzz[e] : o.hxx[e];
+    }
+  }
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting in FP64 of the Slater
+// matrix A[i][j] = phi_j(r_i) of one walker and spin; writes
+// psiM = (A^{-1})^T in the walker precision, log|det A| and its phase
+// (DiracMatrix::invert_transpose + computeLogDet, DiracMatrix.h:25-38,
+// 93-119: the pivots are LU's U diagonal, the pivot rows LU's ipiv).
+template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(DevWalkers dw)
+{
+  extern __shared__ __align__(16) unsigned char dyn[];
+  const int n = dw.n, npad = dw.npad;
+  double* col = reinterpret_cast<double*>(dyn);      // [n]
+  int* perm   = reinterpret_cast<int*>(col + n);     // [n]
+  __shared__ double s_val[32];
+  __shared__ int s_idx[32];
+  __shared__ double s_logdet;
+  __shared__ int s_sign, s_p, s_sing;
+  const int s = blockIdx.x, w = blockIdx.y, tid = threadIdx.x, NT = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const WV<T> wv = make_wv<T>(dw, w);
+  double* M      = wv.lu + (size_t)s * n * npad;
+  if (tid == 0)
+  {
+    s_logdet = 0.0;
+    s_sign   = 1;
+    s_sing   = 0;
+  }
+  __syncthreads();
+  for (int k = 0; k < n; ++k)
+  {
+    // pivot: first row of maximal |M[i][k]|, i >= k
+    double bv = -1.0;
+    int bi    = n;
+    for (int i = k + tid; i < n; i += NT)
+    {
+      const double v = fabs(M[(size_t)i * npad + k]);
+      if (v > bv)
+        bv = v, bi = i;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi    = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi))
+        bv = ov, bi = oi;
+    }
+    if (lane == 0)
+      s_val[wid] = bv, s_idx[wid] = bi;
+    __syncthreads();
+    if (tid == 0)
+    {
+      double v = s_val[0];
+      int p    = s_idx[0];
+      for (int q = 1; q < nw; ++q)
+        if (s_val[q] > v || (s_val[q] == v && s_idx[q] < p))
+          v = s_val[q], p = s_idx[q];
+      s_p     = p;
+      perm[k] = p;
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k)
+      for (int j = tid; j < n; j += NT)
+      {
+        const double t            = M[(size_t)k * npad + j];
+        M[(size_t)k * npad + j] = M[(size_t)p * npad + j];
+        M[(size_t)p * npad + j] = t;
+      }
+    __syncthreads();
+    const double piv = M[(size_t)k * npad + k];
+    if (tid == 0)
+    {
+      if (p != k)
+        s_sign = -s_sign;
+      if (piv == 0.0)
+        s_sing = 1;
+      else
+      {
+        s_logdet += log(fabs(piv));
+        if (piv < 0)
+          s_sign = -s_sign;
+      }
+    }
+    if (piv == 0.0)
+    {
+      __syncthreads();
+      continue;
+    }
+    const double rp = 1.0 / piv;
+    for (int i = tid; i < n; i += NT)
+      col[i] = M[(size_t)i * npad + k];
+    __syncthreads();
+    for (int j = tid; j < n; j += NT)
+      M[(size_t)k * npad + j] = (j == k) ? rp : M[(size_t)k * npad + j] * rp;
+    __syncthreads();
+    // eliminate every other row; warp per row, lanes over columns
+    for (int i = wid; i < n; i += nw)
+    {
+      if (i == k)
+        continue;
+      const double f = col[i];
+      double* mi       = M + (size_t)i * npad;
+      const double* mk = M + (size_t)k * npad;
+      for (int j = lane; j < n; j += 32)
+        mi[j] = (j == k) ? -f * rp : mi[j] - f * mk[j];
+    }
+    __syncthreads();
+  }
+  // (P A)^{-1} -> A^{-1}: swap columns back in reverse pivot order
+  for (int k = n - 1; k >= 0; --k)
+  {
+    const int p = perm[k];
+    if (p != k)
+      for (int i = tid; i < n; i += NT)
+      {
+        const double t            = M[(size_t)i * npad + k];
+        M[(size_t)i * npad + k] = M[(size_t)i * npad + p];
+        M[(size_t)i * npad + p] = t;
+      }
+    __syncthreads();
+  }
+  // psiM[i][j] = Ainv(j, i)
+  T* out = wv.ainv(s);
+  for (int i = wid; i < n; i += nw)
+    for (int j = lane; j < n; j += 32)
+      out[(size_t)i * npad + j] = (T)M[(size_t)j * npad + i];
+  if (tid == 0)
+  {
+    wv.det_log[s]   = s_logdet;
+    wv.det_phase[s] = s_sign > 0 ? 0.0 : kPi;
+    wv.dcount[s]    = 0;
+    if (s_sing)
+      atomicOr(wv.status, DEV_ERR_SINGULAR);
+  }
+}
+
+// J1 / J2 from scratch (OneBodyJastrow::recompute, TwoBodyJastrow::recompute):
+// warp per electron over its full rows.
+template <typename T>
+__global__ void __launch_bounds__(256) jastrow_recompute_kernel(const DevSystem* __restrict__ sys, DevWalkers dw)
+{
+  __shared__ SysSmem<T> ss;
+  load_sys(sys, ss);
+  const int w = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const WV<T> wv = make_wv<T>(dw, w);
+  const int N = wv.N, I = ss.n_ions, Npad = wv.Npad;
+  const T* ions = (const T*)sys->ion_soa;
+  const T* Rs   = wv.Rs;
+  for (int i = wid; i < N; i += nw)
+  {
+    const T px = Rs[i], py = Rs[Npad + i], pz = Rs[2 * Npad + i];
+    if (ss.comp & QMC_WF_J1)
+    {
+      double v = 0, g0 = 0, g1 = 0, g2 = 0, l = 0;
+      for (int c = lane; c < I; c += 32)
+      {
+        T dx = (ions[c] - px) * T(-1), dy = (ions[I + c] - py) * T(-1), dz = (ions[2 * I + c] - pz) * T(-1);
+        const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+        const FunctorT<T>& f = ss.j1[ion_group(ss, c)];
+        if (r < f.cutoff)
+        {
+          T u, du, d2u;
+          functor_vgl(f, r, u, du, d2u);
+          v += u;
+          g0 += (double)(du * -dx);
+          g1 += (double)(du * -dy);
+          g2 += (double)(du * -dz);
+          l += (double)(d2u + T(2) * du);
+        }
+      }
+      v = warp_sum(v), g0 = warp_sum(g0), g1 = warp_sum(g1), g2 = warp_sum(g2), l = warp_sum(l);
+      if (lane == 0)
+      {
+        wv.Vat[i]         = (T)v;
+        wv.Grad[i]        = (T)g0;
+        wv.Grad[N + i]    = (T)g1;
+        wv.Grad[2 * N + i] = (T)g2;
+        wv.Lap[i]         = (T)l;
+      }
+    }
+    if (ss.comp & QMC_WF_J2)
+    {
+      const int gi = i < ss.n_up ? 0 : 1;
+      double v = 0, g0 = 0, g1 = 0, g2 = 0, l = 0;
+      for (int j = lane; j < N; j += 32)
+      {
+        if (j == i)
+          continue;
+        const T flip = j < i ? T(1) : T(-1);
+        T dx = (Rs[j] - px) * flip, dy = (Rs[Npad + j] - py) * flip, dz = (Rs[2 * Npad + j] - pz) * flip;
+        const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+        const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+        if (r < f.cutoff)
+        {
+          T u, du, d2u;
+          functor_vgl(f, r, u, du, d2u);
+          v += u;
+          g0 += (double)(du * dx * flip);
+          g1 += (double)(du * dy * flip);
+          g2 += (double)(du * dz * flip);
+          l += (double)(d2u + T(2) * du);
+        }
+      }
+      v = warp_sum(v), g0 = warp_sum(g0), g1 = warp_sum(g1), g2 = warp_sum(g2), l = warp_sum(l);
+      if (lane == 0)
+      {
+        wv.Uat[i]          = (T)v;
+        wv.dUat[i]         = (T)g0;
+        wv.dUat[N + i]     = (T)g1;
+        wv.dUat[2 * N + i] = (T)g2;
+        wv.d2Uat[i]        = (T)(-l);
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) gl_kernel(const DevSystem* __restrict__ sys, DevWalkers dw)
+{
+  __shared__ SysSmem<T> ss;
+  __shared__ MoveSmem m;
+  load_sys(sys, ss);
+  const WV<T> wv = make_wv<T>(dw, blockIdx.x);
+  evaluate_gl(ss, wv, m, dw.logpsi + blockIdx.x);
+}
+
+template <typename T> __global__ void sync_rs_kernel(DevWalkers dw)
+{
+  const int w = blockIdx.x;
+  T* Rs       = (T*)dw.Rs + (size_t)w * 3 * dw.Npad;
+  for (int i = threadIdx.x; i < dw.Npad; i += blockDim.x)
+    for (int c = 0; c < 3; ++c)
+      Rs[c * dw.Npad + i] = i < dw.N ? (T)dw.R[((size_t)w * dw.N + i) * 3 + c] : T(0);
+}
+
+// SPOSet::evaluate (VGH, or values only) at arbitrary Cartesian points
+template <typename T>
+__global__ void __launch_bounds__(256) spo_points_kernel(const DevSystem* __restrict__ sys, const double* pos, double* v,
+                                                         double* g, double* h, int values_only)
+{
+  constexpr int VW = Vec16<T>::width;
+  __shared__ SplineSmem<T> sp;
+  __shared__ double p[3];
+  const int ip = blockIdx.x;
+  if (threadIdx.x == 0)
+  {
+    for (int c = 0; c < 3; ++c)
+      p[c] = pos[3 * ip + c];
+    spline_locate(sys, p, sp);
+  }
+  __syncthreads();
+  const int norb = sys->norb, nvec = sys->npad / VW;
+  const double dinv[3] = {sys->dinv[0], sys->dinv[1], sys->dinv[2]};
+  for (int q = threadIdx.x; q < nvec; q += blockDim.x)
+  {
+    if (values_only)
+    {
+      T out[VW];
+      spline_eval_v((const T*)sys->coefs, sys->xs, sys->ys, sys->zs, sp, q * VW, out);
+      for (int e = 0; e < VW; ++e)
+        if (q * VW + e < norb && v)
+          v[(size_t)ip * norb + q * VW + e] = (double)out[e];
+      continue;
+    }
+    SplineOut<T> o;
+    spline_eval<T, true>((const T*)sys->coefs, sys->xs, sys->ys, sys->zs, sp, dinv, q * VW, o);
+    for (int e = 0; e < VW; ++e)
+    {
+      const int j = q * VW + e;
+      if (j >= norb)
+        continue;
+      if (v)
+        v[(size_t)ip * norb + j] = (double)o.v[e];
+      if (g)
+      {
+        g[((size_t)ip * 3 + 0) * norb + j] = (double)o.gx[e];
+        g[((size_t)ip * 3 + 1) * norb + j] = (double)o.gy[e];
+        g[((size_t)ip * 3 + 2) * norb + j] = (double)o.gz[e];
+      }
+      if (h)
+      {
+        const T hv[6] = {o.hxx[e], o.hxy[e], o.hxz[e], o.hyy[e], o.hyz[e], o.hzz[e]};
+        for (int c = 0; c < 6; ++c)
+          h[((size_t)ip * 6 + c) * norb + j] = (double)hv[c];
+      }
+    }
+  }
+}
+
+// DelayedUpdate engine on spin 0 of walker 0 of a batch view
+template <typename T> __global__ void __launch_bounds__(256) det_engine_kernel(DevWalkers dw, int op, int row)
+{
+  __shared__ MoveSmem m;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  T* smem        = reinterpret_cast<T*>(dyn);
+  const WV<T> wv = make_wv<T>(dw, 0);
+  if (op == DETENG_GET_INV_ROW)
+    get_inv_row(wv, m, 0, row, wv.dcount[0]);
+  else if (op == DETENG_ACCEPT_ROW)
+  {
+    get_inv_row(wv, m, 0, row, wv.dcount[0]); // fills row dc of Binv, as DiracDeterminant does via ratio
+    __syncthreads();
+    det_accept(wv, m, 0, row, 1.0, false, false, smem);
+  }
+  else
+    flush(wv, m, 0, smem);
+}
+
+// ----------------------------------------------------------- launchers --
+template <typename K> static void allow_smem(K kernel, size_t bytes)
+{
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_verb(bool fp32, const DevSystem* sys, const DevWalkers& dw, const VerbArgs& a, int threads,
+                        int max_k, cudaStream_t st)
+{
+  if (max_k > MAXK)
+    return cudaErrorInvalidValue;
+  if (fp32)
+  {
+    allow_smem(verb_kernel<float>, flush_smem_bytes<float>());
+    verb_kernel<float><<<dw.W, threads, flush_smem_bytes<float>(), st>>>(sys, dw, a);
+  }
+  else
+  {
+    allow_smem(verb_kernel<double>, flush_smem_bytes<double>());
+    verb_kernel<double><<<dw.W, threads, flush_smem_bytes<double>(), st>>>(sys, dw, a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu, cudaStream_t st)
+{
+  dim3 grid(dw.N, dw.W);
+  const int vw      = fp32 ? 4 : 2;
+  const int threads = min(256, round_up(dw.npad / vw, 32));
+  if (fp32)
+    spo_matrix_kernel<float><<<grid, threads, 0, st>>>(sys, dw, want_lu ? 1 : 0);
+  else
+    spo_matrix_kernel<double><<<grid, threads, 0, st>>>(sys, dw, want_lu ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gj_inverse(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads, int n_spins,
+                              cudaStream_t st)
+{
+  (void)sys;
+  dim3 grid(n_spins, dw.W);
+  const size_t smem = (size_t)dw.n * (sizeof(double) + sizeof(int));
+  if (fp32)
+  {
+    allow_smem(gj_inverse_kernel<float>, smem);
+    gj_inverse_kernel<float><<<grid, threads, smem, st>>>(dw);
+  }
+  else
+  {
+    allow_smem(gj_inverse_kernel<double>, smem);
+    gj_inverse_kernel<double><<<grid, threads, smem, st>>>(dw);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_jastrow_recompute(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads,
+                                     cudaStream_t st)
+{
+  if (fp32)
+    jastrow_recompute_kernel<float><<<dw.W, threads, 0, st>>>(sys, dw);
+  else
+    jastrow_recompute_kernel<double><<<dw.W, threads, 0, st>>>(sys, dw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gl(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads, cudaStream_t st)
+{
+  if (fp32)
+    gl_kernel<float><<<dw.W, threads, 0, st>>>(sys, dw);
+  else
+    gl_kernel<double><<<dw.W, threads, 0, st>>>(sys, dw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sync_rs(bool fp32, const DevWalkers& dw, cudaStream_t st)
+{
+  if (fp32)
+    sync_rs_kernel<float><<<dw.W, 256, 0, st>>>(dw);
+  else
+    sync_rs_kernel<double><<<dw.W, 256, 0, st>>>(dw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spo_points(bool fp32, const DevSystem* sys, int n_pos, const double* pos, double* v, double* g,
+                              double* h, bool values_only, cudaStream_t st)
+{
+  if (n_pos <= 0)
+    return cudaSuccess;
+  if (fp32)
+    spo_points_kernel<float><<<n_pos, 128, 0, st>>>(sys, pos, v, g, h, values_only ? 1 : 0);
+  else
+    spo_points_kernel<double><<<n_pos, 128, 0, st>>>(sys, pos, v, g, h, values_only ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, int max_k, cudaStream_t st)
+{
+  if (max_k > MAXK)
+    return cudaErrorInvalidValue;
+  if (fp32)
+  {
+    allow_smem(det_engine_kernel<float>, flush_smem_bytes<float>());
+    det_engine_kernel<float><<<1, 256, flush_smem_bytes<float>(), st>>>(dw, op, row);
+  }
+  else
+  {
+    allow_smem(det_engine_kernel<double>, flush_smem_bytes<double>());
+    det_engine_kernel<double><<<1, 256, flush_smem_bytes<double>(), st>>>(dw, op, row);
+  }
+  return cudaGetLastError();
+}
+
+} // namespace qmc
