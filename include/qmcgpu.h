@@ -261,6 +261,17 @@ int qmc_sweep_results(qmc_walkers* w, int64_t* n_accepted, double* logpsi);
 /* Number of CUDA kernel launches this batch issued since creation. */
 int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count);
 
+/* Device phase timers of the fused sweep (the reference's NewTimer phases,
+ * miniqmc.cpp:138-147): when enabled, each walker's CTA accumulates SM
+ * cycles per phase.  qmc_walkers_phase_times returns, per phase, the mean
+ * over walkers in milliseconds at the device's nominal SM clock:
+ * [0] random streams, [1] getInvRow, [2] SPO VGH + determinant dots,
+ * [3] J1/J2 sums, [4] reductions and ratio, [5] acceptRow bookkeeping,
+ * [6] Woodbury flush, [7] J2 accept, [8] position update,
+ * [9] completeUpdates, [10] evaluateGL.  n_phases receives 11. */
+int qmc_walkers_enable_timers(qmc_walkers* w, int enable);
+int qmc_walkers_phase_times(qmc_walkers* w, double* ms, int* n_phases);
+
 /* DelayedUpdate + DiracMatrix on one n x n inverse, FP64 on the device
  * (DelayedUpdate.h:28-231, DiracMatrix.h:59-121): the object the reference's
  * unit tests drive with fake orbital rows (test_dirac_matrix.cpp,

@@ -102,7 +102,11 @@ PRODUCT_ONLY = {
     'walkers_sync': (I, [P]),
     'sweep_results': (I, [P, C.POINTER(C.c_int64), PD]),
     'walkers_launch_count': (I, [P, C.POINTER(C.c_int64)]),
+    'walkers_enable_timers': (I, [P, I]),
+    'walkers_phase_times': (I, [P, PD, PI]),
 }
+PHASES = ['random', 'getInvRow', 'spo+det dots', 'jastrow sums', 'reduce+ratio', 'acceptRow', 'woodbury flush',
+          'J2 accept', 'position', 'completeUpdates', 'evaluateGL']
 
 
 def bind(lib, prefix, extra=None):

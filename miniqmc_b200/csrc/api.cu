@@ -57,6 +57,7 @@ struct qmc_walkers_s
   int* d_flags    = nullptr;
   double* d_rows  = nullptr;
   size_t cap_rows = 0;
+  long long* d_timers = nullptr;
 };
 
 template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes, P** p, size_t count)
@@ -537,6 +538,7 @@ static void free_walkers(qmc_walkers* w)
   cudaFree(w->d_delta);
   cudaFree(w->d_trace);
   cudaFree(w->d_rows);
+  cudaFree(w->d_timers);
   if (w->own_stream && w->stream)
     cudaStreamDestroy(w->stream);
 }
@@ -608,6 +610,44 @@ int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count)
   *count = w->launches;
   return QMC_OK;
 }
+int qmc_walkers_enable_timers(qmc_walkers* w, int enable)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  cudaStreamSynchronize(w->stream);
+  cudaFree(w->d_timers);
+  w->d_timers = nullptr;
+  if (enable)
+  {
+    CK(cudaMalloc(&w->d_timers, (size_t)w->dw.W * NPHASE * sizeof(long long)));
+    CK(cudaMemset(w->d_timers, 0, (size_t)w->dw.W * NPHASE * sizeof(long long)));
+  }
+  return QMC_OK;
+}
+int qmc_walkers_phase_times(qmc_walkers* w, double* ms, int* n_phases)
+{
+  if (!w || !ms)
+    return fail(QMC_ERR_ARG, "null pointer");
+  if (n_phases)
+    *n_phases = NPHASE;
+  if (!w->d_timers)
+    return fail(QMC_ERR_STATE, "timers not enabled");
+  std::vector<long long> t((size_t)w->dw.W * NPHASE);
+  CK(cudaStreamSynchronize(w->stream));
+  CK(cudaMemcpy(t.data(), w->d_timers, t.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+  int dev = 0, khz = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev);
+  for (int p = 0; p < NPHASE; ++p)
+  {
+    double s = 0;
+    for (int i = 0; i < w->dw.W; ++i)
+      s += (double)t[(size_t)i * NPHASE + p];
+    ms[p] = s / w->dw.W / (double)khz;
+  }
+  return QMC_OK;
+}
+
 int qmc_walkers_sync(qmc_walkers* w)
 {
   if (!w)
@@ -995,6 +1035,7 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
   task.delta       = w->d_delta;
   task.trace       = trace ? w->d_trace : nullptr;
   task.first_block = 0;
+  task.timers      = w->d_timers;
   CK(cudaMemcpyAsync(w->d_task, &task, sizeof(task), cudaMemcpyHostToDevice, w->stream));
   for (int step = 0; step < n_steps; ++step)
   {

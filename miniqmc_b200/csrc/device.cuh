@@ -55,7 +55,22 @@ struct MoveSmem
   double p[MAXK + 1], wv[MAXK + 1], col[MAXK + 1];
   double ratio_det, curAt, curLap, curGrad[3], curUat, y;
   int accept, dc, ok;
+  // per-phase device timers (thread 0, clock64 at phase boundaries)
+  int timing;
+  long long tstamp;
+  long long tacc[NPHASE];
 };
+
+// attribute the cycles since the last mark to `phase` (thread 0 only)
+__device__ __forceinline__ void phase_mark(MoveSmem& m, int phase)
+{
+  if (m.timing && threadIdx.x == 0)
+  {
+    const long long t = clock64();
+    m.tacc[phase] += t - m.tstamp;
+    m.tstamp = t;
+  }
+}
 
 // ----------------------------------------------------- typed views ------
 template <typename T> struct WV
@@ -498,6 +513,7 @@ template <typename T> __device__ void flush(const WV<T>& wv, MoveSmem& m, int s,
   __syncthreads();
   if (dc == 0)
     return;
+  phase_mark(m, PH_DET_ACCEPT);
   const int npad = wv.npad, n = wv.n, k = wv.k;
   const double* B = wv.binv(s);
   const T* U = wv.u(s);
@@ -613,6 +629,7 @@ template <typename T> __device__ void flush(const WV<T>& wv, MoveSmem& m, int s,
   if (tid == 0)
     wv.dcount[s] = 0;
   __syncthreads();
+  phase_mark(m, PH_FLUSH);
 }
 
 // DiracDeterminant::acceptMove + DelayedUpdate::acceptRow.  psiV (and the
@@ -1026,9 +1043,11 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
 #pragma unroll
   for (int i = 0; i < 16; ++i)
     part[i] = 0.0;
+  phase_mark(m, PH_REDUCE);
   if (DET)
   {
     get_inv_row(wv, m, s, r, m.dc);
+    phase_mark(m, PH_INVROW);
     const T* dprow = wv.dpsi(s) + (size_t)r * 3 * npad;
     const T* coefs = (const T*)sys->coefs;
     const long long xs = sys->xs, ys = sys->ys, zs = sys->zs;
@@ -1067,11 +1086,13 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
       reinterpret_cast<Vt*>(wv.dpsiV + 2 * npad)[q] = gzv;
       reinterpret_cast<Vt*>(wv.d2psiV)[q]          = lv;
     }
+    phase_mark(m, PH_SPO);
   }
   if (J1)
     j1_partials(ss, ions, m.pos_new, part + 7);
   if (J2)
     j2_partials(ss, wv.Rs, wv.Npad, iel, m.pos_new, part + 12, true);
+  phase_mark(m, PH_JASTROW);
   block_sum<16>(part, m.red, m.sums);
   if (tid == 0)
   {
@@ -1118,10 +1139,12 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
     }
   }
   __syncthreads();
+  phase_mark(m, PH_REDUCE);
   if (m.accept)
   {
     if (DET)
       det_accept(wv, m, s, r, m.ratio_det, true, true, smem);
+    phase_mark(m, PH_DET_ACCEPT);
     if (J1 && tid == 0)
     {
       wv.jlog[0] += (double)wv.Vat[iel] - m.curAt;
@@ -1133,6 +1156,7 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
     if (J2)
       j2_accept(ss, wv, m, iel);
     __syncthreads();
+    phase_mark(m, PH_J2_ACCEPT);
     if (tid == 0)
       for (int c = 0; c < 3; ++c)
       {
@@ -1140,6 +1164,7 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
         wv.Rs[c * wv.Npad + iel]   = (T)m.pos_new[c];
       }
     __syncthreads();
+    phase_mark(m, PH_POSITION);
   }
 }
 

@@ -5,10 +5,29 @@
 
 namespace qmc
 {
+// device phase timers of the fused sweep (names follow the reference's
+// timers where one exists: miniqmc.cpp:138-147, WaveFunction.cpp:33-41)
+enum Phase
+{
+  PH_RANDOM = 0,    // random streams of a substep
+  PH_INVROW,        // DelayedUpdate::getInvRow ("Current Gradient")
+  PH_SPO,           // SPO VGH + determinant dots ("New Gradient")
+  PH_JASTROW,       // J1/J2 ratio and gradient sums
+  PH_REDUCE,        // block reduction + ratio assembly
+  PH_DET_ACCEPT,    // acceptRow bookkeeping ("Update")
+  PH_FLUSH,         // Woodbury flush (updateInvMat)
+  PH_J2_ACCEPT,     // J2 acceptMove
+  PH_POSITION,      // ParticleSet::acceptMove
+  PH_COMPLETE,      // completeUpdates ("Complete Updates")
+  PH_GL,            // evaluateGL ("Kinetic Energy")
+  NPHASE
+};
+
 // One batch of walkers in a fused sweep launch.  Several tasks (walkers of
 // different systems) may share one launch; each CTA runs one walker.
 struct SweepTask
 {
+  long long* timers;    // device [W][NPHASE] cycle counters, or null
   const DevSystem* sys; // device pointer
   DevWalkers dw;
   int rng_mode;         // QMC_RNG_*

@@ -34,6 +34,14 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   const int N    = wv.N;
   const T* ions  = (const T*)sys->ion_soa;
   long long acc  = 0;
+  if (threadIdx.x == 0)
+  {
+    m.timing = task.timers != nullptr;
+    m.tstamp = clock64();
+    for (int p = 0; p < NPHASE; ++p)
+      m.tacc[p] = 0;
+  }
+  __syncthreads();
   for (int l = 0; l < n_substeps; ++l)
   {
     const double* urp;
@@ -43,6 +51,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
       rng_substep(wv, N);
       urp = wv.ur;
       dp  = wv.delta;
+      phase_mark(m, PH_RANDOM);
     }
     else
     {
@@ -56,15 +65,23 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
       acc += m.accept ? 1 : 0;
       __syncthreads(); // m.accept is rewritten by the next move
     }
+    phase_mark(m, PH_REDUCE);
     if (ss.comp & QMC_WF_DET)
     {
       flush(wv, m, 0, smem);
       flush(wv, m, 1, smem);
     }
+    phase_mark(m, PH_COMPLETE);
   }
   evaluate_gl(ss, wv, m, task.dw.logpsi + w);
+  phase_mark(m, PH_GL);
   if (threadIdx.x == 0)
+  {
     task.dw.accepted[w] += acc;
+    if (task.timers)
+      for (int p = 0; p < NPHASE; ++p)
+        task.timers[(size_t)w * NPHASE + p] += m.tacc[p];
+  }
 }
 
 template <typename T> static void set_smem_attr()
