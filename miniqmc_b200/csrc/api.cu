@@ -499,6 +499,7 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   st |= T(&d.dpsiV, W * 3 * np);
   st |= T(&d.d2psiV, W * np);
   st |= T(&d.U2, W * KK * np);
+  st |= T(&d.tm, W * n * KK);
   st |= dalloc(L, B, &d.ms, W);
   st |= dalloc(L, B, &d.G, W * N * 3);
   st |= dalloc(L, B, &d.L, W * N);
@@ -1147,6 +1148,7 @@ int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
   st |= Dm(&d.dpsiV, 3 * np);
   st |= Dm(&d.d2psiV, np);
   st |= Dm(&d.U2, K * np);
+  st |= Dm(&d.tm, n * K);
   st |= dalloc(L, B, &d.lu, 2 * n * np);
   st |= dalloc(L, B, &d.status, 1);
   st |= dalloc(L, B, &d.ms, 1);

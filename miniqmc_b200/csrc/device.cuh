@@ -104,6 +104,7 @@ template <typename T> struct WV
   T* dpsiV;
   T* d2psiV;
   T* U2;
+  T* tm;
   double* lu;
   MoveState* ms;
   double* G;
@@ -152,6 +153,7 @@ template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
   v.dpsiV     = (T*)d.dpsiV + (size_t)w * 3 * d.npad;
   v.d2psiV    = (T*)d.d2psiV + (size_t)w * d.npad;
   v.U2        = (T*)d.U2 + (size_t)w * kn;
+  v.tm        = (T*)d.tm + (size_t)w * d.n * d.k;
   v.lu        = d.lu ? d.lu + (size_t)w * 2 * nn : nullptr;
   v.ms        = d.ms + w;
   v.G         = d.G + (size_t)w * d.N * 3;
@@ -446,13 +448,20 @@ template <typename T> __device__ void get_inv_row(const WV<T>& wv, MoveSmem& m, 
   const T* V = wv.v(s);
   for (int d = wid; d < dc; d += nw)
   {
-    const T* ud = U + (size_t)d * wv.npad;
-    double acc  = 0.0;
-    for (int j = lane; j < wv.npad; j += 32)
-      acc += (double)(ud[j] * arow[j]);
-    acc = warp_sum(acc);
+    const Vt* ud = reinterpret_cast<const Vt*>(U + (size_t)d * wv.npad);
+    const Vt* av = reinterpret_cast<const Vt*>(arow);
+    T acc        = T(0);
+#pragma unroll 4
+    for (int jv = lane; jv < nvec; jv += 32)
+    {
+      const Vt x = ud[jv], y = av[jv];
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+        acc += reinterpret_cast<const T*>(&x)[e] * reinterpret_cast<const T*>(&y)[e];
+    }
+    const double sum = warp_sum((double)acc);
     if (lane == 0)
-      m.p[d] = acc;
+      m.p[d] = sum;
   }
   __syncthreads();
   double* B = wv.binv(s);
@@ -474,6 +483,7 @@ template <typename T> __device__ void get_inv_row(const WV<T>& wv, MoveSmem& m, 
 #pragma unroll
     for (int e = 0; e < VW; ++e)
       acc[e] = 0.0;
+#pragma unroll 4
     for (int d = 0; d < dc; ++d)
     {
       Vt vv = reinterpret_cast<const Vt*>(V + (size_t)d * wv.npad)[q];
@@ -489,148 +499,7 @@ template <typename T> __device__ void get_inv_row(const WV<T>& wv, MoveSmem& m, 
   }
 }
 
-// Woodbury flush (DelayedUpdate::updateInvMat): with U2 = Binv V and
-// tm = Ainv U^T - E,  Ainv <- Ainv - tm U2.  Row blocks of Ainv are
-// independent, so each is read for tm and then updated in place.
-template <typename T> struct FlushTile
-{
-  static constexpr int BM = 32;
-  static constexpr int BK = sizeof(T) == 4 ? 64 : 32;
-};
-template <typename T> __host__ __device__ constexpr size_t flush_smem_bytes()
-{
-  return sizeof(T) * ((size_t)FlushTile<T>::BM * (FlushTile<T>::BK + 1) + (size_t)MAXK * (FlushTile<T>::BK + 1) +
-                      (size_t)FlushTile<T>::BM * (MAXK + 1));
-}
-
-template <typename T> __device__ void flush(const WV<T>& wv, MoveSmem& m, int s, T* smem)
-{
-  using Vt           = typename Vec16<T>::type;
-  constexpr int VW   = Vec16<T>::width;
-  constexpr int BM   = FlushTile<T>::BM, BK = FlushTile<T>::BK;
-  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
-  const int dc = wv.dcount[s];
-  __syncthreads();
-  if (dc == 0)
-    return;
-  phase_mark(m, PH_DET_ACCEPT);
-  const int npad = wv.npad, n = wv.n, k = wv.k;
-  const double* B = wv.binv(s);
-  const T* U = wv.u(s);
-  const T* V = wv.v(s);
-  T* A       = wv.ainv(s);
-  const int* dl = wv.dl(s);
-  // U2[b][j] = sum_a Binv[b][a] V[a][j]
-  for (int bb = 0; bb < dc; bb += 16)
-    for (int j = tid; j < npad; j += NT)
-    {
-      double acc[16];
-#pragma unroll
-      for (int b = 0; b < 16; ++b)
-        acc[b] = 0.0;
-      for (int a = 0; a < dc; ++a)
-      {
-        const double va = (double)V[(size_t)a * npad + j];
-#pragma unroll
-        for (int b = 0; b < 16; ++b)
-          if (bb + b < dc)
-            acc[b] += B[(bb + b) * k + a] * va;
-      }
-#pragma unroll
-      for (int b = 0; b < 16; ++b)
-        if (bb + b < dc)
-          wv.U2[(size_t)(bb + b) * npad + j] = (T)acc[b];
-    }
-  __syncthreads();
-  T* As = smem;                        // [BM][BK+1]
-  T* Us = As + BM * (BK + 1);          // [MAXK][BK+1]
-  T* tm = Us + MAXK * (BK + 1);        // [BM][MAXK+1]
-  constexpr int MD = 16;               // d-values per thread in GEMM1 (nw >= 4)
-  const int nvec = npad / VW;
-  for (int i0 = 0; i0 < n; i0 += BM)
-  {
-    const int rows = min(BM, n - i0);
-    // GEMM1: tm[i][d] = sum_j Ainv[i0+i][j] U[d][j]; thread (i = lane, d = wid + m*nw)
-    T acc[MD];
-#pragma unroll
-    for (int mm = 0; mm < MD; ++mm)
-      acc[mm] = T(0);
-    for (int j0 = 0; j0 < npad; j0 += BK)
-    {
-      for (int idx = tid; idx < BM * BK; idx += NT)
-      {
-        const int i = idx / BK, kk = idx % BK;
-        As[i * (BK + 1) + kk] = (i < rows && j0 + kk < npad) ? A[(size_t)(i0 + i) * npad + j0 + kk] : T(0);
-      }
-      for (int idx = tid; idx < dc * BK; idx += NT)
-      {
-        const int d = idx / BK, kk = idx % BK;
-        Us[d * (BK + 1) + kk] = (j0 + kk < npad) ? U[(size_t)d * npad + j0 + kk] : T(0);
-      }
-      __syncthreads();
-#pragma unroll 4
-      for (int kk = 0; kk < BK; ++kk)
-      {
-        const T a = As[lane * (BK + 1) + kk];
-#pragma unroll
-        for (int mm = 0; mm < MD; ++mm)
-        {
-          const int d = wid + mm * nw;
-          if (d < dc)
-            acc[mm] += a * Us[d * (BK + 1) + kk];
-        }
-      }
-      __syncthreads();
-    }
-#pragma unroll
-    for (int mm = 0; mm < MD; ++mm)
-    {
-      const int d = wid + mm * nw;
-      if (d < dc)
-        tm[lane * (MAXK + 1) + d] = acc[mm] - ((dl[d] == i0 + lane) ? T(1) : T(0));
-    }
-    __syncthreads();
-    // GEMM3: Ainv[i0+i][j] -= sum_d tm[i][d] U2[d][j], 8 rows per pass
-    for (int q = tid; q < nvec; q += NT)
-      for (int rg = 0; rg < rows; rg += 8)
-      {
-        T c[8][VW];
-#pragma unroll
-        for (int rr = 0; rr < 8; ++rr)
-#pragma unroll
-          for (int e = 0; e < VW; ++e)
-            c[rr][e] = T(0);
-        for (int d = 0; d < dc; ++d)
-        {
-          Vt u2 = reinterpret_cast<const Vt*>(wv.U2 + (size_t)d * npad)[q];
-#pragma unroll
-          for (int rr = 0; rr < 8; ++rr)
-          {
-            const T t = tm[(rg + rr) * (MAXK + 1) + d];
-#pragma unroll
-            for (int e = 0; e < VW; ++e)
-              c[rr][e] += t * reinterpret_cast<T*>(&u2)[e];
-          }
-        }
-#pragma unroll
-        for (int rr = 0; rr < 8; ++rr)
-          if (rg + rr < rows)
-          {
-            Vt* ap = reinterpret_cast<Vt*>(A + (size_t)(i0 + rg + rr) * npad) + q;
-            Vt a   = *ap;
-#pragma unroll
-            for (int e = 0; e < VW; ++e)
-              reinterpret_cast<T*>(&a)[e] -= c[rr][e];
-            *ap = a;
-          }
-      }
-    __syncthreads();
-  }
-  if (tid == 0)
-    wv.dcount[s] = 0;
-  __syncthreads();
-  phase_mark(m, PH_FLUSH);
-}
+#include "flush.cuh"
 
 // DiracDeterminant::acceptMove + DelayedUpdate::acceptRow.  psiV (and the
 // derivative rows when `partial`) come from the move scratch.  Block-wide.
@@ -672,13 +541,20 @@ __device__ void det_accept(const WV<T>& wv, MoveSmem& m, int s, int r, double ra
   const T* Vs = wv.v(s);
   for (int d = wid; d <= dc; d += nw)
   {
-    const T* vd = Vs + (size_t)d * npad;
-    double acc  = 0.0;
-    for (int j = lane; j < npad; j += 32)
-      acc += (double)(vd[j] * wv.psiV[j]);
-    acc = warp_sum(acc);
+    const Vt* vd = reinterpret_cast<const Vt*>(Vs + (size_t)d * npad);
+    const Vt* pv = reinterpret_cast<const Vt*>(wv.psiV);
+    T acc        = T(0);
+#pragma unroll 4
+    for (int jv = lane; jv < nvec; jv += 32)
+    {
+      const Vt x = vd[jv], y = pv[jv];
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+        acc += reinterpret_cast<const T*>(&x)[e] * reinterpret_cast<const T*>(&y)[e];
+    }
+    const double sum = warp_sum((double)acc);
     if (lane == 0)
-      m.p[d] = -acc;
+      m.p[d] = -sum;
   }
   __syncthreads();
   double* B = wv.binv(s);
@@ -730,8 +606,8 @@ template <typename T> __device__ __forceinline__ int ion_group(const SysSmem<T>&
 
 // partial J1 sums over the ions for a position: curAt, grad[3], lap
 // (OneBodyJastrow::computeU3 + accumulateGL; the AB row is always flipped)
-template <typename T>
-__device__ void j1_partials(const SysSmem<T>& ss, const T* __restrict__ ions /*[3][I]*/, const double* pos, double* part)
+template <typename T, typename A>
+__device__ void j1_partials(const SysSmem<T>& ss, const T* __restrict__ ions /*[3][I]*/, const double* pos, A* part)
 {
   const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];
   for (int c = threadIdx.x; c < ss.n_ions; c += blockDim.x)
@@ -744,11 +620,11 @@ __device__ void j1_partials(const SysSmem<T>& ss, const T* __restrict__ ions /*[
     {
       T u, du, d2u;
       functor_vgl(f, r, u, du, d2u);
-      part[0] += (double)u;
-      part[1] += (double)(du * dx);
-      part[2] += (double)(du * dy);
-      part[3] += (double)(du * dz);
-      part[4] += (double)(d2u + T(2) * du);
+      part[0] += (A)u;
+      part[1] += (A)(du * dx);
+      part[2] += (A)(du * dy);
+      part[3] += (A)(du * dz);
+      part[4] += (A)(d2u + T(2) * du);
     }
   }
 }
@@ -768,34 +644,50 @@ __device__ void j1_value(const SysSmem<T>& ss, const T* __restrict__ ions, const
 
 // partial J2 sums over the electrons for electron iel moved to pos:
 // sum u, sum du*dr (TwoBodyJastrow::ratioGrad with the move row, flip = iel)
-template <typename T>
+template <typename T, typename A>
 __device__ void j2_partials(const SysSmem<T>& ss, const T* __restrict__ Rs, int Npad, int iel, const double* pos,
-                            double* part, bool grads)
+                            A* part, bool grads)
 {
   const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];
   const int gi = iel < ss.n_up ? 0 : 1;
-  for (int j = threadIdx.x; j < ss.n_elec; j += blockDim.x)
+  const int N = ss.n_elec, NT = blockDim.x;
+  for (int j0 = threadIdx.x; j0 < N; j0 += 4 * NT)
   {
-    if (j == iel)
-      continue;
-    const T flip = j < iel ? T(1) : T(-1);
-    T dx = (Rs[j] - px) * flip, dy = (Rs[Npad + j] - py) * flip, dz = (Rs[2 * Npad + j] - pz) * flip;
-    const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
-    const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
-    if (r < f.cutoff)
+    T rx[4], ry[4], rz[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
     {
-      if (grads)
+      const int j   = j0 + u * NT;
+      const bool ok = j < N;
+      rx[u]         = ok ? Rs[j] : T(0);
+      ry[u]         = ok ? Rs[Npad + j] : T(0);
+      rz[u]         = ok ? Rs[2 * Npad + j] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+    {
+      const int j = j0 + u * NT;
+      if (j >= N || j == iel)
+        continue;
+      const T flip = j < iel ? T(1) : T(-1);
+      T dx = (rx[u] - px) * flip, dy = (ry[u] - py) * flip, dz = (rz[u] - pz) * flip;
+      const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+      const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+      if (r < f.cutoff)
       {
-        T u, du, d2u;
-        functor_vgl(f, r, u, du, d2u);
-        dx *= flip, dy *= flip, dz *= flip;
-        part[0] += (double)u;
-        part[1] += (double)(du * dx);
-        part[2] += (double)(du * dy);
-        part[3] += (double)(du * dz);
+        if (grads)
+        {
+          T uu, du, d2u;
+          functor_vgl(f, r, uu, du, d2u);
+          dx *= flip, dy *= flip, dz *= flip;
+          part[0] += (A)uu;
+          part[1] += (A)(du * dx);
+          part[2] += (A)(du * dy);
+          part[3] += (A)(du * dz);
+        }
+        else
+          part[0] += (A)functor_v(f, r);
       }
-      else
-        part[0] += (double)functor_v(f, r);
     }
   }
 }
@@ -810,39 +702,63 @@ __device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, in
   const int gi = iel < ss.n_up ? 0 : 1;
   const int Npad = wv.Npad, N = wv.N;
   const T* Rs = wv.Rs;
-  double part[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int j = threadIdx.x; j < N; j += blockDim.x)
+  const int NT = blockDim.x;
+  T part[4] = {T(0), T(0), T(0), T(0)};
+  for (int j0 = threadIdx.x; j0 < N; j0 += 2 * NT)
   {
-    if (j == iel)
-      continue;
-    const T flip = j < iel ? T(1) : T(-1);
-    const T rx = Rs[j], ry = Rs[Npad + j], rz = Rs[2 * Npad + j];
-    const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
-    T odx = (rx - ox) * flip, ody = (ry - oy) * flip, odz = (rz - oz) * flip;
-    const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
-    odx *= flip, ody *= flip, odz *= flip;
-    T ndx = (rx - nx) * flip, ndy = (ry - ny) * flip, ndz = (rz - nz) * flip;
-    const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
-    ndx *= flip, ndy *= flip, ndz *= flip;
-    T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
-    if (ro < f.cutoff)
-      functor_vgl(f, ro, uo, duo, d2uo);
-    if (rn < f.cutoff)
-      functor_vgl(f, rn, un, dun, d2un);
-    const T newl = d2un + T(2) * dun;
-    const T dl   = d2uo + T(2) * duo - newl;
-    wv.Uat[j] += un - uo;
-    wv.d2Uat[j] += dl;
-    part[0] -= (double)newl;
-    const T ng0 = dun * ndx, ng1 = dun * ndy, ng2 = dun * ndz;
-    wv.dUat[j] -= ng0 - duo * odx;
-    wv.dUat[N + j] -= ng1 - duo * ody;
-    wv.dUat[2 * N + j] -= ng2 - duo * odz;
-    part[1] += (double)ng0;
-    part[2] += (double)ng1;
-    part[3] += (double)ng2;
+    // issue every load of this thread's two electrons first
+    T rx[2], ry[2], rz[2], ua[2], la[2], g0[2], g1[2], g2[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+    {
+      const int j   = j0 + u * NT;
+      const bool ok = j < N;
+      rx[u]         = ok ? Rs[j] : T(0);
+      ry[u]         = ok ? Rs[Npad + j] : T(0);
+      rz[u]         = ok ? Rs[2 * Npad + j] : T(0);
+      ua[u]         = ok ? wv.Uat[j] : T(0);
+      la[u]         = ok ? wv.d2Uat[j] : T(0);
+      g0[u]         = ok ? wv.dUat[j] : T(0);
+      g1[u]         = ok ? wv.dUat[N + j] : T(0);
+      g2[u]         = ok ? wv.dUat[2 * N + j] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+    {
+      const int j = j0 + u * NT;
+      if (j >= N || j == iel)
+        continue;
+      const T flip = j < iel ? T(1) : T(-1);
+      const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+      T odx = (rx[u] - ox) * flip, ody = (ry[u] - oy) * flip, odz = (rz[u] - oz) * flip;
+      const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
+      odx *= flip, ody *= flip, odz *= flip;
+      T ndx = (rx[u] - nx) * flip, ndy = (ry[u] - ny) * flip, ndz = (rz[u] - nz) * flip;
+      const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
+      ndx *= flip, ndy *= flip, ndz *= flip;
+      T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
+      if (ro < f.cutoff)
+        functor_vgl(f, ro, uo, duo, d2uo);
+      if (rn < f.cutoff)
+        functor_vgl(f, rn, un, dun, d2un);
+      const T newl = d2un + T(2) * dun;
+      const T dl   = d2uo + T(2) * duo - newl;
+      wv.Uat[j]   = ua[u] + (un - uo);
+      wv.d2Uat[j] = la[u] + dl;
+      part[0] -= newl;
+      const T ng0 = dun * ndx, ng1 = dun * ndy, ng2 = dun * ndz;
+      wv.dUat[j]         = g0[u] - (ng0 - duo * odx);
+      wv.dUat[N + j]     = g1[u] - (ng1 - duo * ody);
+      wv.dUat[2 * N + j] = g2[u] - (ng2 - duo * odz);
+      part[1] += ng0;
+      part[2] += ng1;
+      part[3] += ng2;
+    }
   }
-  block_sum<4>(part, m.red, m.sums);
+  {
+    double dpart[4] = {(double)part[0], (double)part[1], (double)part[2], (double)part[3]};
+    block_sum<4>(dpart, m.red, m.sums);
+  }
   if (threadIdx.x == 0)
   {
     wv.jlog[1] += (double)wv.Uat[iel] - m.curUat;
@@ -1039,10 +955,12 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
       spline_locate(sys, m.pos_new, sp);
   }
   __syncthreads();
-  double part[16];
+  // per-thread partial sums cover a few terms each: accumulate in the walker
+  // precision, widen to FP64 for the block reduction
+  T part[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i)
-    part[i] = 0.0;
+    part[i] = T(0);
   phase_mark(m, PH_REDUCE);
   if (DET)
   {
@@ -1062,7 +980,7 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
         Vt g = reinterpret_cast<const Vt*>(dprow + (size_t)c * npad)[q];
 #pragma unroll
         for (int e = 0; e < VW; ++e)
-          part[4 + c] += (double)(ivp[e] * reinterpret_cast<T*>(&g)[e]);
+          part[4 + c] += ivp[e] * reinterpret_cast<T*>(&g)[e];
       }
       SplineOut<T> o;
       spline_eval<T, false>(coefs, xs, ys, zs, sp, dinv, q * VW, o);
@@ -1075,10 +993,10 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
         reinterpret_cast<T*>(&gyv)[e] = o.gy[e];
         reinterpret_cast<T*>(&gzv)[e] = o.gz[e];
         reinterpret_cast<T*>(&lv)[e]  = trace_lap ? o.hxx[e] + o.hyy[e] + o.hzz[e] : o.hxx[e];
-        part[0] += (double)(ivp[e] * o.v[e]);
-        part[1] += (double)(ivp[e] * o.gx[e]);
-        part[2] += (double)(ivp[e] * o.gy[e]);
-        part[3] += (double)(ivp[e] * o.gz[e]);
+        part[0] += ivp[e] * o.v[e];
+        part[1] += ivp[e] * o.gx[e];
+        part[2] += ivp[e] * o.gy[e];
+        part[3] += ivp[e] * o.gz[e];
       }
       reinterpret_cast<Vt*>(wv.psiV)[q]            = pv;
       reinterpret_cast<Vt*>(wv.dpsiV)[q]           = gxv;
@@ -1093,7 +1011,13 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
   if (J2)
     j2_partials(ss, wv.Rs, wv.Npad, iel, m.pos_new, part + 12, true);
   phase_mark(m, PH_JASTROW);
-  block_sum<16>(part, m.red, m.sums);
+  {
+    double dpart[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      dpart[i] = (double)part[i];
+    block_sum<16>(dpart, m.red, m.sums);
+  }
   if (tid == 0)
   {
     const double* S = m.sums;

@@ -97,7 +97,8 @@ struct DevWalkers
   void* psiV;      // [W][npad]
   void* dpsiV;     // [W][3][npad]
   void* d2psiV;    // [W][npad]
-  void* U2;        // [W][k][npad] flush scratch
+  void* U2;        // [W][k][npad] flush scratch (Binv V)
+  void* tm;        // [W][n][k] flush scratch (Ainv U^T - E)
   double* lu;      // [W][2][n][npad] FP64 Slater matrices for the LU (lazily)
   MoveState* ms;   // [W]
   double* G;       // [W][N][3]

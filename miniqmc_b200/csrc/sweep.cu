@@ -103,13 +103,14 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
   if (fp32)
   {
     set_smem_attr<float>();
-    sweep_kernel<float><<<total_blocks, threads, flush_smem_bytes<float>(), st>>>(d_tasks, n_tasks, n_substeps, accept);
+    sweep_kernel<float><<<total_blocks, threads, flush_smem_bytes_for<float>(threads, max_k), st>>>(
+        d_tasks, n_tasks, n_substeps, accept);
   }
   else
   {
     set_smem_attr<double>();
-    sweep_kernel<double>
-        <<<total_blocks, threads, flush_smem_bytes<double>(), st>>>(d_tasks, n_tasks, n_substeps, accept);
+    sweep_kernel<double><<<total_blocks, threads, flush_smem_bytes_for<double>(threads, max_k), st>>>(
+        d_tasks, n_tasks, n_substeps, accept);
   }
   return cudaGetLastError();
 }
