@@ -278,6 +278,11 @@ int qmc_walkers_phase_times(qmc_walkers* w, double* ms, int* n_phases);
  * test_dirac_det.cpp). */
 typedef struct qmc_detengine_s qmc_detengine;
 int qmc_detengine_create(int n, int delay, qmc_detengine** out);
+/* Same engine with the matrices held in the given precision: QMC_PREC_FP64,
+ * or QMC_PREC_MIXED (FP32 Ainv/U/V/psiV rows as in the mixed sweep, FP64
+ * k x k Binv and FP64 inverse/log-det).  qmc_detengine_create is this with
+ * QMC_PREC_FP64. */
+int qmc_detengine_create_prec(int n, int delay, int precision, qmc_detengine** out);
 int qmc_detengine_destroy(qmc_detengine* e);
 /* DiracMatrix::invert_transpose(logdetT = a): psiM = (a^{-1})^T, log|det a|
  * and its phase (0 or pi). */

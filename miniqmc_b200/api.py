@@ -348,11 +348,14 @@ class Walkers:
 class DetEngine:
     """DelayedUpdate + DiracMatrix on one n x n inverse (DelayedUpdate.h:28-231)."""
 
-    def __init__(self, lib, n, delay):
+    def __init__(self, lib, n, delay, precision=None):
         self.lib = lib
         self.n = n
         h = C.c_void_p()
-        lib.call('detengine_create', n, delay, C.byref(h))
+        if precision is None:
+            lib.call('detengine_create', n, delay, C.byref(h))
+        else:
+            lib.call('detengine_create_prec', n, delay, precision, C.byref(h))
         self.h = h
 
     def close(self):

@@ -98,6 +98,7 @@ PRODUCT_ONLY = {
     'pset_update': (I, [P]),
     'pset_set_active': (I, [P, I]),
     'pset_done': (I, [P]),
+    'detengine_create_prec': (I, [I, I, I, C.POINTER(P)]),
     'sweep_async': (I, [P, I, I, D, I]),
     'walkers_sync': (I, [P]),
     'sweep_results': (I, [P, C.POINTER(C.c_int64), PD]),

@@ -266,6 +266,7 @@ int qmc_system_create(const qmc_system_desc* d, int precision, qmc_system** out)
   std::memset(&h, 0, sizeof(h));
   std::memcpy(h.lattice, d->lattice, sizeof(h.lattice));
   qmc_host::bconds(d->lattice, h.rb, h.gb, h.corners);
+  h.mi_scale2 = qmc_host::min_metric_eigenvalue(h.rb) * (1.0 - 1e-6);
   qmc_host::inverse3(d->spo_lattice, h.spoG);
   for (int k = 0; k < 3; ++k)
   {
@@ -1037,6 +1038,9 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
   task.trace       = trace ? w->d_trace : nullptr;
   task.first_block = 0;
   task.timers      = w->d_timers;
+  // next-move L2 prefetch only while the batch's in-flight stencils (16 rows
+  // of 4 npad coefficients per walker) stay well inside the 126 MB L2
+  task.prefetch = (double)W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8) <= 32.0e6;
   CK(cudaMemcpyAsync(w->d_task, &task, sizeof(task), cudaMemcpyHostToDevice, w->stream));
   for (int step = 0; step < n_steps; ++step)
   {
@@ -1113,7 +1117,22 @@ struct qmc_detengine_s
   qmc_walkers_s w;
 };
 
-int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
+static void to_dev_elems(const qmc_walkers_s* w, const double* src, size_t n, std::vector<unsigned char>& buf)
+{
+  const size_t es = w->fp32 ? 4 : 8;
+  buf.assign(n * es, 0);
+  for (size_t i = 0; i < n; ++i)
+    if (w->fp32)
+      reinterpret_cast<float*>(buf.data())[i] = (float)src[i];
+    else
+      reinterpret_cast<double*>(buf.data())[i] = src[i];
+}
+static double dev_elem(const qmc_walkers_s* w, const std::vector<unsigned char>& buf, size_t i)
+{
+  return w->fp32 ? (double)reinterpret_cast<const float*>(buf.data())[i] : reinterpret_cast<const double*>(buf.data())[i];
+}
+
+int qmc_detengine_create_prec(int n, int delay, int precision, qmc_detengine_s** out)
 {
   if (!out || n < 1 || delay < 1 || delay > 64 || delay > n)
     return fail(QMC_ERR_ARG, "bad engine size");
@@ -1122,33 +1141,34 @@ int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
   DevWalkers& d = w->dw;
   std::memset(&d, 0, sizeof(d));
   d.W = 1, d.N = n, d.Npad = round_up(n, 32), d.n = n, d.npad = round_up(n, 32), d.I = 0, d.k = delay;
-  w->fp32 = false;
-  const size_t np = d.npad, K = delay;
-  auto& L         = w->allocs;
-  auto& B         = w->bytes;
-  int st          = 0;
-  auto Dm         = [&](void** p, size_t c) {
-    double* q = nullptr;
-    int r     = dalloc(L, B, &q, c);
-    *p        = q;
+  w->fp32          = precision == QMC_PREC_MIXED;
+  const size_t es  = w->fp32 ? 4 : 8;
+  const size_t np  = d.npad, K = delay;
+  auto& L          = w->allocs;
+  auto& B          = w->bytes;
+  int st           = 0;
+  auto Tm          = [&](void** p, size_t c) {
+    unsigned char* q = nullptr;
+    int r            = dalloc(L, B, &q, c * es);
+    *p               = q;
     return r;
   };
-  st |= Dm(&d.Ainv, 2 * n * np);
-  st |= Dm(&d.dpsiM, 2 * 3 * n * np);
-  st |= Dm(&d.d2psiM, 2 * n * np);
-  st |= Dm(&d.U, 2 * K * np);
-  st |= Dm(&d.V, 2 * K * np);
+  st |= Tm(&d.Ainv, 2 * n * np);
+  st |= Tm(&d.dpsiM, 2 * 3 * n * np);
+  st |= Tm(&d.d2psiM, 2 * n * np);
+  st |= Tm(&d.U, 2 * K * np);
+  st |= Tm(&d.V, 2 * K * np);
   st |= dalloc(L, B, &d.Binv, 2 * K * K);
   st |= dalloc(L, B, &d.delay_list, 2 * K);
   st |= dalloc(L, B, &d.delay_count, 2);
   st |= dalloc(L, B, &d.det_log, 2);
   st |= dalloc(L, B, &d.det_phase, 2);
-  st |= Dm(&d.invRow, np);
-  st |= Dm(&d.psiV, np);
-  st |= Dm(&d.dpsiV, 3 * np);
-  st |= Dm(&d.d2psiV, np);
-  st |= Dm(&d.U2, K * np);
-  st |= Dm(&d.tm, n * K);
+  st |= Tm(&d.invRow, np);
+  st |= Tm(&d.psiV, np);
+  st |= Tm(&d.dpsiV, 3 * np);
+  st |= Tm(&d.d2psiV, np);
+  st |= Tm(&d.U2, K * np);
+  st |= Tm(&d.tm, n * K);
   st |= dalloc(L, B, &d.lu, 2 * n * np);
   st |= dalloc(L, B, &d.status, 1);
   st |= dalloc(L, B, &d.ms, 1);
@@ -1162,6 +1182,10 @@ int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
   w->own_stream = true;
   *out          = e;
   return QMC_OK;
+}
+int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
+{
+  return qmc_detengine_create_prec(n, delay, QMC_PREC_FP64, out);
 }
 int qmc_detengine_destroy(qmc_detengine_s* e)
 {
@@ -1182,7 +1206,7 @@ int qmc_detengine_invert_transpose(qmc_detengine_s* e, const double* a, double* 
     for (size_t j = 0; j < n; ++j)
       m[i * np + j] = a[i * n + j];
   CK(cudaMemcpyAsync(w->dw.lu, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, w->stream));
-  CK(launch_gj_inverse(false, nullptr, w->dw, 256, 1, w->stream));
+  CK(launch_gj_inverse(w->fp32, nullptr, w->dw, 256, 1, w->stream));
   double lg = 0, ph = 0;
   CK(cudaMemcpyAsync(&lg, w->dw.det_log, sizeof(double), cudaMemcpyDeviceToHost, w->stream));
   CK(cudaMemcpyAsync(&ph, w->dw.det_phase, sizeof(double), cudaMemcpyDeviceToHost, w->stream));
@@ -1198,10 +1222,13 @@ int qmc_detengine_get_inv_row(qmc_detengine_s* e, int row, double* inv_row)
   if (!e || !inv_row || row < 0 || row >= e->w.dw.n)
     return fail(QMC_ERR_ARG, "bad arguments");
   auto* w = &e->w;
-  CK(launch_det_engine(false, DETENG_GET_INV_ROW, w->dw, row, w->dw.k, w->stream));
-  CK(cudaMemcpyAsync(inv_row, w->dw.invRow, w->dw.n * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(launch_det_engine(w->fp32, DETENG_GET_INV_ROW, w->dw, row, w->dw.k, w->stream));
+  std::vector<unsigned char> buf(w->dw.n * (w->fp32 ? 4 : 8));
+  CK(cudaMemcpyAsync(buf.data(), w->dw.invRow, buf.size(), cudaMemcpyDeviceToHost, w->stream));
   CK(cudaStreamSynchronize(w->stream));
-  return QMC_OK;
+  for (int i = 0; i < w->dw.n; ++i)
+    inv_row[i] = dev_elem(w, buf, i);
+  return device_status(w);
 }
 int qmc_detengine_accept_row(qmc_detengine_s* e, int row, const double* psiv)
 {
@@ -1210,19 +1237,21 @@ int qmc_detengine_accept_row(qmc_detengine_s* e, int row, const double* psiv)
   auto* w = &e->w;
   std::vector<double> p(w->dw.npad, 0.0);
   std::memcpy(p.data(), psiv, w->dw.n * sizeof(double));
-  CK(cudaMemcpyAsync(w->dw.psiV, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice, w->stream));
-  CK(launch_det_engine(false, DETENG_ACCEPT_ROW, w->dw, row, w->dw.k, w->stream));
+  std::vector<unsigned char> buf;
+  to_dev_elems(w, p.data(), p.size(), buf);
+  CK(cudaMemcpyAsync(w->dw.psiV, buf.data(), buf.size(), cudaMemcpyHostToDevice, w->stream));
+  CK(launch_det_engine(w->fp32, DETENG_ACCEPT_ROW, w->dw, row, w->dw.k, w->stream));
   CK(cudaStreamSynchronize(w->stream));
-  return QMC_OK;
+  return device_status(w);
 }
 int qmc_detengine_update_inv_mat(qmc_detengine_s* e)
 {
   if (!e)
     return fail(QMC_ERR_ARG, "null pointer");
   auto* w = &e->w;
-  CK(launch_det_engine(false, DETENG_UPDATE, w->dw, 0, w->dw.k, w->stream));
+  CK(launch_det_engine(w->fp32, DETENG_UPDATE, w->dw, 0, w->dw.k, w->stream));
   CK(cudaStreamSynchronize(w->stream));
-  return QMC_OK;
+  return device_status(w);
 }
 int qmc_detengine_get_ainv(qmc_detengine_s* e, double* ainv)
 {
@@ -1230,11 +1259,11 @@ int qmc_detengine_get_ainv(qmc_detengine_s* e, double* ainv)
     return fail(QMC_ERR_ARG, "null pointer");
   auto* w        = &e->w;
   const size_t n = w->dw.n, np = w->dw.npad;
-  std::vector<double> m(n * np);
-  CK(cudaMemcpy(m.data(), w->dw.Ainv, m.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<unsigned char> buf(n * np * (w->fp32 ? 4 : 8));
+  CK(cudaMemcpy(buf.data(), w->dw.Ainv, buf.size(), cudaMemcpyDeviceToHost));
   for (size_t i = 0; i < n; ++i)
     for (size_t j = 0; j < n; ++j)
-      ainv[i * n + j] = m[i * np + j];
+      ainv[i * n + j] = dev_elem(w, buf, i * np + j);
   return QMC_OK;
 }
 

@@ -36,6 +36,7 @@ template <typename T> struct FunctorT
 template <typename T> struct SysSmem
 {
   T rb[9], gb[9], cn[24];
+  T mi_scale2;
   FunctorT<T> j1[QMC_MAX_ION_GROUPS], j2uu, j2ud;
   int gfirst[QMC_MAX_ION_GROUPS], glast[QMC_MAX_ION_GROUPS];
   int n_groups, n_ions, n_elec, n_up, norb, npad, comp, lap_mode;
@@ -54,6 +55,7 @@ struct MoveSmem
   double pos_old[3], pos_new[3];
   double p[MAXK + 1], wv[MAXK + 1], col[MAXK + 1];
   double ratio_det, curAt, curLap, curGrad[3], curUat, y;
+  long long next_base;
   int accept, dc, ok;
   // per-phase device timers (thread 0, clock64 at phase boundaries)
   int timing;
@@ -110,13 +112,15 @@ template <typename T> struct WV
   double* G;
   double* L;
   unsigned* status;
+  double* bsm;  // Binv of spin bsm_spin held in shared memory (fused sweep), or null
+  int bsm_spin;
 
   __device__ T* ainv(int s) const { return Ainv + (size_t)s * n * npad; }
   __device__ T* dpsi(int s) const { return dpsiM + (size_t)s * n * 3 * npad; }
   __device__ T* d2psi(int s) const { return d2psiM + (size_t)s * n * npad; }
   __device__ T* u(int s) const { return U + (size_t)s * k * npad; }
   __device__ T* v(int s) const { return V + (size_t)s * k * npad; }
-  __device__ double* binv(int s) const { return Binv + (size_t)s * k * k; }
+  __device__ double* binv(int s) const { return (bsm && s == bsm_spin) ? bsm : Binv + (size_t)s * k * k; }
   __device__ int* dl(int s) const { return dlist + s * k; }
 };
 
@@ -159,6 +163,8 @@ template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
   v.G         = d.G + (size_t)w * d.N * 3;
   v.L         = d.L + (size_t)w * d.N;
   v.status    = d.status;
+  v.bsm       = nullptr;
+  v.bsm_spin  = -1;
   return v;
 }
 
@@ -196,8 +202,25 @@ template <typename T> __device__ void load_sys(const DevSystem* __restrict__ s, 
     ss.j2ud.n = s->j2ud.n, ss.j2ud.cutoff = (T)s->j2ud.cutoff, ss.j2ud.dinv = (T)s->j2ud.dinv;
     ss.n_groups = s->n_groups, ss.n_ions = s->n_ions, ss.n_elec = s->n_elec, ss.n_up = s->n_up;
     ss.norb = s->norb, ss.npad = s->npad, ss.comp = s->comp, ss.lap_mode = s->lap_mode;
+    ss.mi_scale2 = (T)s->mi_scale2;
   }
   __syncthreads();
+}
+
+// true when every periodic image of the displacement is at least sqrt(rc2)
+// away, so the pair is outside the cutoff whatever image the corner search
+// would pick (see DevSystem::mi_scale2); exact, no false positives
+template <typename T>
+__device__ __forceinline__ bool beyond_cutoff(T dx, T dy, T dz, const T* __restrict__ gb, T scale2, T rc2)
+{
+  T f0 = dx * gb[0] + dy * gb[3] + dz * gb[6];
+  T f1 = dx * gb[1] + dy * gb[4] + dz * gb[7];
+  T f2 = dx * gb[2] + dy * gb[5] + dz * gb[8];
+  f0 -= floor(f0);
+  f1 -= floor(f1);
+  f2 -= floor(f2);
+  const T m0 = min(f0, T(1) - f0), m1 = min(f1, T(1) - f1), m2 = min(f2, T(1) - f2);
+  return scale2 * (m0 * m0 + m1 * m1 + m2 * m2) >= rc2;
 }
 
 // ------------------------------------------------------ minimum image --
@@ -318,6 +341,35 @@ template <typename T> __device__ void spline_locate(const DevSystem* __restrict_
     sp.d2a[d][3] = (T)(1.0 * t + 0.0);
   }
   sp.base = base;
+}
+
+// element offset of the stencil corner for a Cartesian point (the index part
+// of spline_locate, used to prefetch the next move's coefficients)
+__device__ inline long long spline_base(const DevSystem* __restrict__ s, const double* pos)
+{
+  long long base             = 0;
+  const long long strides[3] = {s->xs, s->ys, s->zs};
+  for (int d = 0; d < 3; ++d)
+  {
+    double u = pos[0] * s->spoG[d] + pos[1] * s->spoG[3 + d] + pos[2] * s->spoG[6 + d];
+    if (-DBL_EPSILON < u && u < 0)
+      u = 0.0;
+    else
+      u -= floor(u);
+    const double x = u * s->dinv[d];
+    int ind        = x < 0 ? 0 : (int)floor(x);
+    if (ind > s->grid[d] - 1)
+      ind = s->grid[d] - 1;
+    base += (long long)ind * strides[d];
+  }
+  return base;
+}
+
+// L2 prefetch of `bytes` (multiple of 16) at a 16-byte aligned address,
+// issued to the bulk-copy (TMA) engine; no register or shared memory used
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes)
+{
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 template <typename T> struct SplineOut
@@ -613,9 +665,11 @@ __device__ void j1_partials(const SysSmem<T>& ss, const T* __restrict__ ions /*[
   for (int c = threadIdx.x; c < ss.n_ions; c += blockDim.x)
   {
     T dx = (ions[c] - px) * T(-1), dy = (ions[ss.n_ions + c] - py) * T(-1), dz = (ions[2 * ss.n_ions + c] - pz) * T(-1);
+    const FunctorT<T>& f = ss.j1[ion_group(ss, c)];
+    if (beyond_cutoff(dx, dy, dz, ss.gb, ss.mi_scale2, f.cutoff * f.cutoff))
+      continue;
     const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
     dx *= T(-1), dy *= T(-1), dz *= T(-1);
-    const FunctorT<T>& f = ss.j1[ion_group(ss, c)];
     if (r < f.cutoff)
     {
       T u, du, d2u;
@@ -671,8 +725,10 @@ __device__ void j2_partials(const SysSmem<T>& ss, const T* __restrict__ Rs, int 
         continue;
       const T flip = j < iel ? T(1) : T(-1);
       T dx = (rx[u] - px) * flip, dy = (ry[u] - py) * flip, dz = (rz[u] - pz) * flip;
-      const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
       const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+      if (beyond_cutoff(dx, dy, dz, ss.gb, ss.mi_scale2, f.cutoff * f.cutoff))
+        continue;
+      const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
       if (r < f.cutoff)
       {
         if (grads)
@@ -730,17 +786,24 @@ __device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, in
         continue;
       const T flip = j < iel ? T(1) : T(-1);
       const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
-      T odx = (rx[u] - ox) * flip, ody = (ry[u] - oy) * flip, odz = (rz[u] - oz) * flip;
-      const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
-      odx *= flip, ody *= flip, odz *= flip;
-      T ndx = (rx[u] - nx) * flip, ndy = (ry[u] - ny) * flip, ndz = (rz[u] - nz) * flip;
-      const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
-      ndx *= flip, ndy *= flip, ndz *= flip;
+      const T rc2 = f.cutoff * f.cutoff;
       T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
-      if (ro < f.cutoff)
-        functor_vgl(f, ro, uo, duo, d2uo);
-      if (rn < f.cutoff)
-        functor_vgl(f, rn, un, dun, d2un);
+      T odx = (rx[u] - ox) * flip, ody = (ry[u] - oy) * flip, odz = (rz[u] - oz) * flip;
+      if (!beyond_cutoff(odx, ody, odz, ss.gb, ss.mi_scale2, rc2))
+      {
+        const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
+        odx *= flip, ody *= flip, odz *= flip;
+        if (ro < f.cutoff)
+          functor_vgl(f, ro, uo, duo, d2uo);
+      }
+      T ndx = (rx[u] - nx) * flip, ndy = (ry[u] - ny) * flip, ndz = (rz[u] - nz) * flip;
+      if (!beyond_cutoff(ndx, ndy, ndz, ss.gb, ss.mi_scale2, rc2))
+      {
+        const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
+        ndx *= flip, ndy *= flip, ndz *= flip;
+        if (rn < f.cutoff)
+          functor_vgl(f, rn, un, dun, d2un);
+      }
       const T newl = d2un + T(2) * dun;
       const T dl   = d2uo + T(2) * duo - newl;
       wv.Uat[j]   = ua[u] + (un - uo);
@@ -934,7 +997,7 @@ template <typename T> __device__ void rng_substep(const WV<T>& wv, int N)
 template <typename T>
 __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys, const WV<T>& wv, MoveSmem& m,
                         SplineSmem<T>& sp, const T* __restrict__ ions, int iel, double accept_thr, double ur,
-                        const double* dlt, double* trace, T* smem)
+                        const double* dlt, double* trace, T* smem, bool has_next)
 {
   using Vt         = typename Vec16<T>::type;
   constexpr int VW = Vec16<T>::width;
@@ -952,9 +1015,36 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
     m.accept = ur < accept_thr;
     m.dc     = DET ? wv.dcount[s] : 0;
     if (DET)
+    {
       spline_locate(sys, m.pos_new, sp);
+      if (has_next)
+      {
+        // the next electron's current position does not change during this
+        // move, so its proposed position and stencil are known now
+        double pn[3];
+        for (int c = 0; c < 3; ++c)
+          pn[c] = wv.R[3 * (iel + 1) + c] + dlt[3 + c];
+        m.next_base = spline_base(sys, pn);
+      }
+    }
   }
   __syncthreads();
+  if (DET && has_next && tid < 18)
+  {
+    // warm L2 with the next move's 16 stencil rows and its inverse and
+    // gradient rows while this move runs
+    if (tid < 16)
+      prefetch_l2((const T*)sys->coefs + m.next_base + (tid >> 2) * sys->xs + (tid & 3) * sys->ys,
+                  (unsigned)(4 * sys->zs * sizeof(T)));
+    else
+    {
+      const int i2 = iel + 1, s2 = i2 < ss.n_up ? 0 : 1, r2 = i2 - (s2 ? ss.n_up : 0);
+      if (tid == 16)
+        prefetch_l2(wv.ainv(s2) + (size_t)r2 * npad, (unsigned)(npad * sizeof(T)));
+      else
+        prefetch_l2(wv.dpsi(s2) + (size_t)r2 * 3 * npad, (unsigned)(3 * npad * sizeof(T)));
+    }
+  }
   // per-thread partial sums cover a few terms each: accumulate in the walker
   // precision, widen to FP64 for the block reduction
   T part[16];

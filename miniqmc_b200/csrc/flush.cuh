@@ -32,6 +32,11 @@ template <typename T> __host__ __device__ constexpr size_t flush_smem_bytes()
 {
   return flush_smem_bytes_for<T>(256, 64);
 }
+// shared-memory bytes of the active spin's k x k Binv in the fused sweep
+__host__ __device__ constexpr size_t bsm_bytes(int k)
+{
+  return ((size_t)k * k * sizeof(double) + 15) / 16 * 16;
+}
 
 template <typename T> __device__ void flush(const WV<T>& wv, MoveSmem& m, int s, T* smem)
 {

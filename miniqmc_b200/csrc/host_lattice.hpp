@@ -138,6 +138,43 @@ inline void bconds(const double* R, double* rb9, double* gb9, double* corners24)
   }
 }
 
+// smallest eigenvalue of the symmetric 3x3 matrix rb rb^T (cyclic Jacobi)
+inline double min_metric_eigenvalue(const double* rb)
+{
+  double a[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      a[i][j] = rb[3 * i] * rb[3 * j] + rb[3 * i + 1] * rb[3 * j + 1] + rb[3 * i + 2] * rb[3 * j + 2];
+  for (int sweep = 0; sweep < 60; ++sweep)
+  {
+    double off = std::abs(a[0][1]) + std::abs(a[0][2]) + std::abs(a[1][2]);
+    if (off < 1e-300)
+      break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q)
+      {
+        if (std::abs(a[p][q]) < 1e-300)
+          continue;
+        const double theta = (a[q][q] - a[p][p]) / (2 * a[p][q]);
+        const double t     = (theta >= 0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1));
+        const double c = 1 / std::sqrt(t * t + 1), s = t * c;
+        for (int k = 0; k < 3; ++k)
+        {
+          const double akp = a[k][p], akq = a[k][q];
+          a[k][p]          = c * akp - s * akq;
+          a[k][q]          = s * akp + c * akq;
+        }
+        for (int k = 0; k < 3; ++k)
+        {
+          const double apk = a[p][k], aqk = a[q][k];
+          a[p][k]          = c * apk - s * aqk;
+          a[q][k]          = s * apk + c * aqk;
+        }
+      }
+  }
+  return std::min(a[0][0], std::min(a[1][1], a[2][2]));
+}
+
 // r = dot(u, R) (ConvertPosUnit, FastParticleOperators.h:44-56)
 inline void to_cart(const double* R, const double* u, double* r)
 {

@@ -35,6 +35,7 @@ struct SweepTask
   const double* delta;  // device [W][nsub][N][3]
   double* trace;        // device [W][nsub][N][8] or null
   int first_block;      // first CTA of this task in the launch
+  int prefetch;         // warm L2 with the next move's coefficients
 };
 
 struct LaunchCfg

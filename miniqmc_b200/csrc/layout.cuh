@@ -34,6 +34,11 @@ struct DevSystem
   // simulation cell: reduced basis, its inverse and the 8 image corners
   // (DTD_BConds<T,3,PPPG+SOA_OFFSET>, ParticleBConds.h:106-151)
   double rb[9], gb[9], corners[24];
+  // lower bound of |f . rb|^2 / |f|^2 over fractional vectors f (smallest
+  // eigenvalue of rb rb^T, slightly shrunk): pairs whose wrapped fractional
+  // displacement is at least rc / sqrt(mi_scale2) from every cell corner
+  // have every image beyond rc and skip the corner search
+  double mi_scale2;
   double lattice[9];
   // orbital cell: toUnit = r . spoG (CrystalLattice.h:180-196)
   double spoG[9];

@@ -20,8 +20,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   __shared__ MoveSmem m;
   __shared__ SplineSmem<T> sp;
   extern __shared__ __align__(16) unsigned char dyn[];
-  T* smem = reinterpret_cast<T*>(dyn);
-  int t   = 0;
+  int t = 0;
   while (t + 1 < n_tasks && (int)blockIdx.x >= tasks[t + 1].first_block)
     ++t;
   const SweepTask& task = tasks[t];
@@ -30,10 +29,23 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
     return;
   const DevSystem* sys = task.sys;
   load_sys(sys, ss);
-  const WV<T> wv = make_wv<T>(task.dw, w);
-  const int N    = wv.N;
-  const T* ions  = (const T*)sys->ion_soa;
-  long long acc  = 0;
+  WV<T> wv      = make_wv<T>(task.dw, w);
+  const int N   = wv.N;
+  const T* ions = (const T*)sys->ion_soa;
+  long long acc = 0;
+  const bool DET = ss.comp & QMC_WF_DET;
+  // dynamic shared memory: [Binv of the active spin (k x k FP64)][flush scratch]
+  const int k = wv.k;
+  T* smem     = reinterpret_cast<T*>(dyn + bsm_bytes(k));
+  auto load_binv = [&](int spin) {
+    const double* g = wv.Binv + (size_t)spin * k * k;
+    double* b       = reinterpret_cast<double*>(dyn);
+    for (int i = threadIdx.x; i < k * k; i += blockDim.x)
+      b[i] = g[i];
+    wv.bsm      = b;
+    wv.bsm_spin = spin;
+    __syncthreads();
+  };
   if (threadIdx.x == 0)
   {
     m.timing = task.timers != nullptr;
@@ -58,18 +70,30 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
       urp = task.ur + ((size_t)w * n_substeps + l) * N;
       dp  = task.delta + ((size_t)w * n_substeps + l) * 3 * N;
     }
+    if (DET)
+      load_binv(0);
     for (int iel = 0; iel < N; ++iel)
     {
+      if (DET && iel == ss.n_up)
+      {
+        // completeUpdates of the up determinant, taken as soon as its last
+        // electron has moved: the down-spin moves never read it, so this is
+        // the same arithmetic as flushing both at the end of the substep
+        flush(wv, m, 0, smem);
+        load_binv(1);
+      }
       double* tr = task.trace ? task.trace + (((size_t)w * n_substeps + l) * N + iel) * 8 : nullptr;
-      do_move(ss, sys, wv, m, sp, ions, iel, accept_thr, urp[iel], dp + 3 * iel, tr, smem);
+      do_move(ss, sys, wv, m, sp, ions, iel, accept_thr, urp[iel], dp + 3 * iel, tr, smem,
+              task.prefetch && iel + 1 < N);
       acc += m.accept ? 1 : 0;
       __syncthreads(); // m.accept is rewritten by the next move
     }
     phase_mark(m, PH_REDUCE);
-    if (ss.comp & QMC_WF_DET)
+    if (DET)
     {
       flush(wv, m, 0, smem);
       flush(wv, m, 1, smem);
+      wv.bsm = nullptr;
     }
     phase_mark(m, PH_COMPLETE);
   }
@@ -84,13 +108,13 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   }
 }
 
-template <typename T> static void set_smem_attr()
+template <typename T> static void set_smem_attr(size_t bytes)
 {
-  static bool done = false;
-  if (!done)
+  static size_t done = 0;
+  if (bytes > done)
   {
-    cudaFuncSetAttribute(sweep_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flush_smem_bytes<T>());
-    done = true;
+    cudaFuncSetAttribute(sweep_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done = bytes;
   }
 }
 
@@ -102,15 +126,15 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
     return cudaErrorInvalidValue;
   if (fp32)
   {
-    set_smem_attr<float>();
-    sweep_kernel<float><<<total_blocks, threads, flush_smem_bytes_for<float>(threads, max_k), st>>>(
-        d_tasks, n_tasks, n_substeps, accept);
+    const size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<float>(threads, max_k);
+    set_smem_attr<float>(bytes);
+    sweep_kernel<float><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept);
   }
   else
   {
-    set_smem_attr<double>();
-    sweep_kernel<double><<<total_blocks, threads, flush_smem_bytes_for<double>(threads, max_k), st>>>(
-        d_tasks, n_tasks, n_substeps, accept);
+    const size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<double>(threads, max_k);
+    set_smem_attr<double>(bytes);
+    sweep_kernel<double><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept);
   }
   return cudaGetLastError();
 }
