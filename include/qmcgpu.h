@@ -293,6 +293,33 @@ int qmc_detengine_accept_row(qmc_detengine* e, int row, const double* psiv);
 int qmc_detengine_update_inv_mat(qmc_detengine* e);
 int qmc_detengine_get_ainv(qmc_detengine* e, double* ainv);
 
+/* Allocation-free inverse.  No reference counterpart: the reference always
+ * inverts into memory its DiracMatrix owns.  This is the FP64 Gauss-Jordan
+ * of qmc_detengine_invert_transpose on caller-owned device memory: a and
+ * psim are n x n row-major FP64 device buffers (row stride n), psim =
+ * (a^{-1})^T, *logdet = log|det a| and *phase = 0 or pi (either may be null);
+ * results equal qmc_detengine_invert_transpose's bit for bit.
+ *
+ * It calls no cudaMalloc, cudaFree or allocating library routine.  This is
+ * for host codes that cannot take a device allocation mid-run.  One kind
+ * reserves the device memory up front in its own pool, so an extra
+ * cudaMalloc escapes its accounting or fails outright.  Another is a
+ * latency-bound loop: cudaFree waits for the whole device, stalling every
+ * stream of the process.
+ *
+ * The working copy of the matrix lives in one static device array per
+ * device, which limits n to QMC_NOALLOC_MAX_N (768: 4.5 MiB).  A larger n
+ * returns QMC_ERR_ARG.  The first call on each device, made with that
+ * device current, looks the array up (cudaGetSymbolAddress).  Make that
+ * first call before any stream capture.  Calls on one device share the
+ * array, so calls that overlap (other streams or host threads) race: the
+ * caller must serialise them.  The call waits for `stream` (a cudaStream_t,
+ * null for the default stream) to finish.  QMC_ERR_SINGULAR on a zero
+ * pivot. */
+#define QMC_NOALLOC_MAX_N 768
+int qmc_invert_transpose_noalloc(int n, const double* a, double* psim, double* logdet, double* phase,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,7 @@ STATUS = {0: 'QMC_OK', 1: 'QMC_ERR_ARG', 2: 'QMC_ERR_CUDA', 3: 'QMC_ERR_OOM', 4:
           5: 'QMC_ERR_NONFINITE', 6: 'QMC_ERR_TIMEOUT', 7: 'QMC_ERR_STATE', 8: 'QMC_ERR_NODEVICE',
           9: 'QMC_ERR_ADMISSION'}
 PREC_FP64, PREC_MIXED = 0, 1
+NOALLOC_MAX_N = 768  # largest n of qmc_invert_transpose_noalloc
 FILL_USER, FILL_REFERENCE, FILL_UNIFORM = 0, 1, 2
 LAP_HXX, LAP_TRACE = 0, 1
 WF_DET, WF_J1, WF_J2, WF_ALL = 1, 2, 4, 7
@@ -99,6 +100,7 @@ PRODUCT_ONLY = {
     'pset_set_active': (I, [P, I]),
     'pset_done': (I, [P]),
     'detengine_create_prec': (I, [I, I, I, C.POINTER(P)]),
+    'invert_transpose_noalloc': (I, [I, P, P, PD, PD, P]),
     'sweep_async': (I, [P, I, I, D, I]),
     'walkers_sync': (I, [P]),
     'sweep_results': (I, [P, C.POINTER(C.c_int64), PD]),

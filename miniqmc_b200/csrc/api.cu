@@ -9,6 +9,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1264,6 +1265,88 @@ int qmc_detengine_get_ainv(qmc_detengine_s* e, double* ainv)
   for (size_t i = 0; i < n; ++i)
     for (size_t j = 0; j < n; ++j)
       ainv[i * n + j] = dev_elem(w, buf, i * np + j);
+  return QMC_OK;
+}
+
+// ------------------------------------------- allocation-free inverse --
+} // extern "C"
+
+// Working storage of qmc_invert_transpose_noalloc: the FP64 working copy of
+// the matrix (row stride n) followed by four words (log|det|, phase, the
+// delay count the inverse kernel resets, the device error bits).  It lives
+// in the library's static device memory, one copy per device, so the call
+// needs no cudaMalloc; its size fixes the largest n.
+static constexpr size_t kNoallocLU = (size_t)QMC_NOALLOC_MAX_N * QMC_NOALLOC_MAX_N;
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocLU + 4];
+
+static std::mutex g_noalloc_mu;
+static constexpr int kNoallocDevices = 64;
+static void* g_noalloc_base[kNoallocDevices];
+
+// Device address of the static scratch on the current device, looked up
+// once per device (the set-up step: it may load the library's device code)
+static int noalloc_scratch(double** out)
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocDevices)
+    return fail(QMC_ERR_CUDA, "device ordinal beyond the scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_base[dev])
+  {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_base[dev] = p;
+  }
+  *out = static_cast<double*>(g_noalloc_base[dev]);
+  return QMC_OK;
+}
+
+extern "C" {
+
+int qmc_invert_transpose_noalloc(int n, const double* a, double* psim, double* logdet, double* phase,
+                                 void* stream)
+{
+  if (n < 1 || n > QMC_NOALLOC_MAX_N)
+    return fail(QMC_ERR_ARG, "qmc_invert_transpose_noalloc: n = " + std::to_string(n) +
+                                 " is outside 1.." + std::to_string(QMC_NOALLOC_MAX_N) +
+                                 ", the size of the static scratch");
+  if (!a || !psim)
+    return fail(QMC_ERR_ARG, "qmc_invert_transpose_noalloc: null device pointer");
+  double* base = nullptr;
+  if (int r = noalloc_scratch(&base))
+    return r;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* words   = base + kNoallocLU;
+  unsigned* stat  = reinterpret_cast<unsigned*>(words + 3);
+  // a one-walker, one-spin view whose matrices are the caller's buffers and
+  // the static scratch (row stride n)
+  DevWalkers v;
+  std::memset(&v, 0, sizeof(v));
+  v.W = 1, v.N = n, v.Npad = n, v.n = n, v.npad = n, v.k = 1;
+  v.lu          = base;
+  v.Ainv        = psim;
+  v.det_log     = words;
+  v.det_phase   = words + 1;
+  v.delay_count = reinterpret_cast<int*>(words + 2);
+  v.status      = stat;
+  // the error bits are only ever OR-ed in by the kernel: clear them first
+  CK(cudaMemsetAsync(stat, 0, sizeof(unsigned), st));
+  CK(cudaMemcpyAsync(base, a, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CK(launch_gj_inverse(false, nullptr, v, 256, 1, st));
+  double hw[4];
+  CK(cudaMemcpyAsync(hw, words, sizeof(hw), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (logdet)
+    *logdet = hw[0];
+  if (phase)
+    *phase = hw[1];
+  unsigned bits = 0;
+  std::memcpy(&bits, &hw[3], sizeof(bits));
+  if (bits & DEV_ERR_SINGULAR)
+    return fail(QMC_ERR_SINGULAR, "zero pivot in the FP64 inverse");
+  if (bits)
+    return fail(QMC_ERR_CUDA, "device error bits set");
   return QMC_OK;
 }
 
