@@ -50,6 +50,8 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-walkers', type=int, default=0)
+    ap.add_argument('--plain-steps', type=int, default=4,
+                    help='walker-steps of the plain FP64 form (1 walker per launch, rank-1) to time; 0 = skip')
     return ap.parse_args()
 
 
@@ -127,6 +129,43 @@ def build_workload(lib, args, capi, api, device_rng_seeds):
     walkers = api.Walkers(system, args.walkers, args.delay)
     walkers.init_random(device_rng_seeds)
     return spec, system, walkers
+
+
+# DRAM bytes per electron move of sweep_kernel<float> measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum = 34.23 GB over one launch of
+# 64 walkers x 1536 moves, NiO 4x4x2, grid 74x74x37, k=32, mixed); the
+# bench's traffic figure scales it by the moves of one launch
+MEASURED_TRAFFIC_PER_MOVE = 34.228e9 / (64 * 1536)
+
+
+def plain_fp64_form(lib, args, api, capi, stream_cls):
+    """The plain GPU form of the same system: FP64 table and walker state,
+    one walker per launch, delay rank 1 (Sherman-Morrison), walkers run one
+    after another.  Returns (electron-moves/s, ms per walker-step)."""
+    import torch
+    tiling = tuple(int(x) for x in args.tiling.split(','))
+    grid = tuple(int(x) for x in args.grid.split(','))
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=grid, fill=capi.FILL_UNIFORM, spo_seed=11,
+                          jastrow='synthetic')
+    system = api.System(lib, spec, capi.PREC_FP64)
+    w = api.Walkers(system, 1, 1)
+    w.init_random(np.array([1009], dtype=np.uint32))
+    stream = stream_cls()
+    lib.call('walkers_set_stream', w.h, C.c_void_p(stream.cuda_stream))
+    w.evaluate_log()
+    lib.call('sweep_async', w.h, 1, 1, 0.5, 0)  # warm-up
+    lib.call('walkers_sync', w.h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.plain_steps):
+        lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
+    e1.record(stream)
+    lib.call('walkers_sync', w.h)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.plain_steps
+    w.close()
+    system.close()
+    return spec.n_elec / (ms / 1e3), ms
 
 
 def cpu_baseline(args, n_threads, sample_walkers):
@@ -249,9 +288,7 @@ def main():
     # e2e through the public API: host random streams in, results out
     e2e = None
     if not args.no_e2e:
-        pin = torch.empty((2, W, 1, N, 4), dtype=torch.float64, pin_memory=True)
         rs = np.random.default_rng(5 + rank)
-        urb = pin[0, :, :, :, 0].numpy()
         ur = np.ascontiguousarray(rs.uniform(size=(1, W, 1, N)))
         de = np.ascontiguousarray(rs.normal(size=(1, W, 1, N, 3)))
         pin_ur = torch.from_numpy(ur).pin_memory().numpy()
@@ -276,8 +313,17 @@ def main():
     avg_launch_ms = float(np.mean(kernel_ms))
     achieved = bpm * W * N / (avg_launch_ms / 1e3) / 1e9
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
-                'frac': achieved / pk['hbm_gbs'], 'traffic': None,
+                'frac': achieved / pk['hbm_gbs'],
+                'traffic': (MEASURED_TRAFFIC_PER_MOVE * W * N
+                            if (args.precision == 'mixed' and args.delay == 32) else None),
+                'traffic_source': 'ncu dram bytes per move (64 walkers, grid 74x74x37) x moves per launch',
                 'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm, 'kernel': 'sweep_kernel<float>'}
+    plain = None
+    if rank == 0 and world == 1 and args.plain_steps > 0:
+        pv, pms = plain_fp64_form(lib, args, api, capi, torch.cuda.Stream)
+        plain = {'value': pv, 'unit': 'electron-moves/s', 'ms_per_walker_step': pms,
+                 'form': 'FP64, 1 walker per launch, delay rank 1, walkers in sequence',
+                 'walker_steps_timed': args.plain_steps, 'value_over_plain': value / pv}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ncpu = os.cpu_count() or 1
@@ -294,17 +340,25 @@ def main():
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'f32' if args.precision == 'mixed' else 'f64', 'data': 'synthetic',
             'config': {'workload': 'NiO %s of the 4-atom cell: %d atoms, %d e-, %d orbitals/spin, grid %s '
-                                   'FP32 table, %d walkers/GPU, delay %d, %s'
-                                   % (args.tiling, I, N, n, args.grid, W, k, args.precision),
-                       'walkers_per_gpu': W, 'l2': 'inputs larger than L2 (5.4 GB spline table, '
-                                                    '%.1f GB walker state)' % (walkers_bytes(lib, walkers) / 1e9),
+                                   '%s table, %d walkers/GPU, delay %d, %s'
+                                   % (args.tiling, I, N, n, args.grid, 'FP32' if s == 4 else 'FP64', W, k,
+                                      args.precision),
+                       'walkers_per_gpu': W,
+                       'l2': 'inputs larger than L2 (%.2f GB spline table, %.1f GB walker state)'
+                             % (system_bytes(lib, system) / 1e9, walkers_bytes(lib, walkers) / 1e9),
                        'acceptance': a, 'parallelism': 'replicas x%d' % world},
-            'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk,
+            'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk, 'plain_fp64': plain,
             'gpu_launches': launches,
         }
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def system_bytes(lib, system):
+    b = C.c_size_t()
+    lib.call('system_bytes', system.h, C.byref(b))
+    return b.value
 
 
 def walkers_bytes(lib, walkers):
