@@ -50,6 +50,8 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-walkers', type=int, default=0)
+    ap.add_argument('--flush', default='tc', choices=['tc', 'simt'],
+                    help='Woodbury flush on the tensor cores (tcgen05 3xTF32) or the CUDA cores (FP32 FMA)')
     ap.add_argument('--plain-steps', type=int, default=4,
                     help='walker-steps of the plain FP64 form (1 walker per launch, rank-1) to time; 0 = skip')
     return ap.parse_args()
@@ -237,6 +239,8 @@ def main():
     spec, system, walkers = build_workload(lib, args, capi, api, seeds)
     stream = torch.cuda.Stream()
     lib.call('walkers_set_stream', walkers.h, C.c_void_p(stream.cuda_stream))
+    if args.precision == 'mixed':
+        lib.call('walkers_set_tensor_cores', walkers.h, 1 if args.flush == 'tc' else 0)
     walkers.evaluate_log()
     W, N = args.walkers, spec.n_elec
     count = C.c_int64()
@@ -346,7 +350,8 @@ def main():
                        'walkers_per_gpu': W,
                        'l2': 'inputs larger than L2 (%.2f GB spline table, %.1f GB walker state)'
                              % (system_bytes(lib, system) / 1e9, walkers_bytes(lib, walkers) / 1e9),
-                       'acceptance': a, 'parallelism': 'replicas x%d' % world},
+                       'acceptance': a, 'parallelism': 'replicas x%d' % world,
+                       'flush': args.flush if args.precision == 'mixed' else 'simt'},
             'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk, 'plain_fp64': plain,
             'gpu_launches': launches,
         }

@@ -270,6 +270,14 @@ int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count);
  * [6] Woodbury flush, [7] J2 accept, [8] position update,
  * [9] completeUpdates, [10] evaluateGL.  n_phases receives 11. */
 int qmc_walkers_enable_timers(qmc_walkers* w, int enable);
+
+/* Woodbury flush on the tensor cores (tcgen05, 3xTF32 with FP32
+ * accumulation) or on the CUDA cores (FP32 FMA).  The tensor-core flush is
+ * on by default wherever it applies: FP32 walkers with the determinant,
+ * delay rank <= 32 and >= 128 threads per walker (480 or more orbitals per
+ * spin).  QMC_ERR_ARG when asked for where it does not apply.  Both compute
+ * DelayedUpdate::updateInvMat (DelayedUpdate.h:184-191). */
+int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable);
 int qmc_walkers_phase_times(qmc_walkers* w, double* ms, int* n_phases);
 
 /* DelayedUpdate + DiracMatrix on one n x n inverse, FP64 on the device
@@ -292,6 +300,9 @@ int qmc_detengine_get_inv_row(qmc_detengine* e, int row, double* inv_row);
 int qmc_detengine_accept_row(qmc_detengine* e, int row, const double* psiv);
 int qmc_detengine_update_inv_mat(qmc_detengine* e);
 int qmc_detengine_get_ainv(qmc_detengine* e, double* ainv);
+/* The engine's flushes on the tensor cores (FP32 engines with delay rank
+ * <= 32; on by default there) or on the CUDA cores. */
+int qmc_detengine_set_tensor_cores(qmc_detengine* e, int enable);
 
 /* Allocation-free inverse.  No reference counterpart: the reference always
  * inverts into memory its DiracMatrix owns.  This is the FP64 Gauss-Jordan

@@ -100,6 +100,8 @@ PRODUCT_ONLY = {
     'pset_set_active': (I, [P, I]),
     'pset_done': (I, [P]),
     'detengine_create_prec': (I, [I, I, I, C.POINTER(P)]),
+    'detengine_set_tensor_cores': (I, [P, I]),
+    'walkers_set_tensor_cores': (I, [P, I]),
     'invert_transpose_noalloc': (I, [I, P, P, PD, PD, P]),
     'sweep_async': (I, [P, I, I, D, I]),
     'walkers_sync': (I, [P]),

@@ -59,7 +59,13 @@ struct qmc_walkers_s
   double* d_rows  = nullptr;
   size_t cap_rows = 0;
   long long* d_timers = nullptr;
+  bool tc_capable = false; // FP32, >= 128 threads, k <= 32, determinant on
+  bool use_tc     = false; // Woodbury flushes on the tensor cores
 };
+
+// the tensor-core flush keeps (Binv V)^T as 32-row hi/lo tiles of up to 32
+// delays: 2 x 32 floats per padded orbital and walker
+static size_t tc_image_floats(int npad) { return (size_t)2 * 32 * npad; }
 
 template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes, P** p, size_t count)
 {
@@ -89,6 +95,8 @@ static int device_status(qmc_walkers* w)
       return fail(QMC_ERR_SINGULAR, "zero pivot in the FP64 inverse of a Slater matrix");
     if (st & DEV_ERR_NONFINITE)
       return fail(QMC_ERR_NONFINITE, "non-finite wavefunction ratio");
+    if (st & DEV_ERR_TIMEOUT)
+      return fail(QMC_ERR_TIMEOUT, "a bounded wait on the tensor-core pipeline gave up");
     if (st & DEV_ERR_STATE)
       return fail(QMC_ERR_STATE, "move protocol violated (no proposed move for this electron)");
     return fail(QMC_ERR_CUDA, "device error bits set");
@@ -564,6 +572,17 @@ int qmc_walkers_create(qmc_system* s, int n_walkers, int delay_rank, qmc_walkers
   const int vw   = w->fp32 ? 4 : 2;
   const int nvec = s->h.npad / vw;
   w->threads     = std::min(256, std::max(std::max(64, 2 * delay_rank), round_up(nvec, 32)));
+  w->tc_capable  = w->fp32 && w->threads >= 128 && delay_rank <= 32 && (s->h.comp & QMC_WF_DET);
+  if (w->tc_capable)
+  {
+    if (dalloc(w->allocs, w->bytes, &w->dw.tci, (size_t)n_walkers * tc_image_floats(w->dw.npad)))
+    {
+      free_walkers(w);
+      delete w;
+      return QMC_ERR_OOM;
+    }
+    w->use_tc = true;
+  }
   cudaError_t e  = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess)
   {
@@ -611,6 +630,16 @@ int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count)
   if (!w || !count)
     return fail(QMC_ERR_ARG, "null pointer");
   *count = w->launches;
+  return QMC_OK;
+}
+int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  if (enable && !w->tc_capable)
+    return fail(QMC_ERR_ARG, "tensor-core flush needs FP32 walkers, the determinant, delay rank <= 32 and >= 128 "
+                             "threads per walker (480 or more orbitals per spin in FP32 give that)");
+  w->use_tc = enable != 0;
   return QMC_OK;
 }
 int qmc_walkers_enable_timers(qmc_walkers* w, int enable)
@@ -1052,7 +1081,8 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
       CK(cudaMemcpyAsync(w->d_delta, delta + step * blk * 3, 3 * blk * sizeof(double), cudaMemcpyHostToDevice,
                          w->stream));
     }
-    CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k, w->stream));
+    CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k, w->stream,
+                    w->use_tc));
     w->launches++;
     if (trace)
       CK(cudaMemcpyAsync(trace + (size_t)step * W * n_substeps * N * 8, w->d_trace,
@@ -1173,6 +1203,12 @@ int qmc_detengine_create_prec(int n, int delay, int precision, qmc_detengine_s**
   st |= dalloc(L, B, &d.lu, 2 * n * np);
   st |= dalloc(L, B, &d.status, 1);
   st |= dalloc(L, B, &d.ms, 1);
+  w->tc_capable = w->fp32 && delay <= 32;
+  if (w->tc_capable)
+  {
+    st |= dalloc(L, B, &d.tci, tc_image_floats(d.npad));
+    w->use_tc = true;
+  }
   if (st)
   {
     free_walkers(w);
@@ -1187,6 +1223,15 @@ int qmc_detengine_create_prec(int n, int delay, int precision, qmc_detengine_s**
 int qmc_detengine_create(int n, int delay, qmc_detengine_s** out)
 {
   return qmc_detengine_create_prec(n, delay, QMC_PREC_FP64, out);
+}
+int qmc_detengine_set_tensor_cores(qmc_detengine_s* e, int enable)
+{
+  if (!e)
+    return fail(QMC_ERR_ARG, "null handle");
+  if (enable && !e->w.tc_capable)
+    return fail(QMC_ERR_ARG, "tensor-core flush needs an FP32 engine with delay rank <= 32");
+  e->w.use_tc = enable != 0;
+  return QMC_OK;
 }
 int qmc_detengine_destroy(qmc_detengine_s* e)
 {
@@ -1223,7 +1268,7 @@ int qmc_detengine_get_inv_row(qmc_detengine_s* e, int row, double* inv_row)
   if (!e || !inv_row || row < 0 || row >= e->w.dw.n)
     return fail(QMC_ERR_ARG, "bad arguments");
   auto* w = &e->w;
-  CK(launch_det_engine(w->fp32, DETENG_GET_INV_ROW, w->dw, row, w->dw.k, w->stream));
+  CK(launch_det_engine(w->fp32, DETENG_GET_INV_ROW, w->dw, row, w->dw.k, w->stream, w->use_tc));
   std::vector<unsigned char> buf(w->dw.n * (w->fp32 ? 4 : 8));
   CK(cudaMemcpyAsync(buf.data(), w->dw.invRow, buf.size(), cudaMemcpyDeviceToHost, w->stream));
   CK(cudaStreamSynchronize(w->stream));
@@ -1241,7 +1286,7 @@ int qmc_detengine_accept_row(qmc_detengine_s* e, int row, const double* psiv)
   std::vector<unsigned char> buf;
   to_dev_elems(w, p.data(), p.size(), buf);
   CK(cudaMemcpyAsync(w->dw.psiV, buf.data(), buf.size(), cudaMemcpyHostToDevice, w->stream));
-  CK(launch_det_engine(w->fp32, DETENG_ACCEPT_ROW, w->dw, row, w->dw.k, w->stream));
+  CK(launch_det_engine(w->fp32, DETENG_ACCEPT_ROW, w->dw, row, w->dw.k, w->stream, w->use_tc));
   CK(cudaStreamSynchronize(w->stream));
   return device_status(w);
 }
@@ -1250,7 +1295,7 @@ int qmc_detengine_update_inv_mat(qmc_detengine_s* e)
   if (!e)
     return fail(QMC_ERR_ARG, "null pointer");
   auto* w = &e->w;
-  CK(launch_det_engine(w->fp32, DETENG_UPDATE, w->dw, 0, w->dw.k, w->stream));
+  CK(launch_det_engine(w->fp32, DETENG_UPDATE, w->dw, 0, w->dw.k, w->stream, w->use_tc));
   CK(cudaStreamSynchronize(w->stream));
   return device_status(w);
 }

@@ -16,7 +16,8 @@ enum : unsigned
   DEV_ERR_SINGULAR  = 1u,
   DEV_ERR_NONFINITE = 2u,
   DEV_ERR_INDEX     = 4u,
-  DEV_ERR_STATE     = 8u
+  DEV_ERR_STATE     = 8u,
+  DEV_ERR_TIMEOUT   = 16u // a bounded wait on the tensor-core pipeline gave up
 };
 
 constexpr double kPi = 3.14159265358979323846;

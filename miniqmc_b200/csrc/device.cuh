@@ -19,6 +19,7 @@
 //   inverse + log|det|        DiracMatrix.h:25-38, 93-119 (Gauss-Jordan here)
 #pragma once
 #include "kernels.cuh"
+#include "tc.cuh"
 
 #include <cfloat>
 
@@ -57,6 +58,11 @@ struct MoveSmem
   double ratio_det, curAt, curLap, curGrad[3], curUat, y;
   long long next_base;
   int accept, dc, ok;
+  // tensor-core flush state: commit barriers (GEMM1 stages 0/1, GEMM2
+  // accumulators 0/1), their phase bits, the TMEM base, the abort flag
+  unsigned long long tc_bar[4];
+  unsigned tc_phase, tc_tmem;
+  int tc_on, tc_abort;
   // per-phase device timers (thread 0, clock64 at phase boundaries)
   int timing;
   long long tstamp;
@@ -107,6 +113,7 @@ template <typename T> struct WV
   T* d2psiV;
   T* U2;
   T* tm;
+  float* tci;
   double* lu;
   MoveState* ms;
   double* G;
@@ -158,6 +165,7 @@ template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
   v.d2psiV    = (T*)d.d2psiV + (size_t)w * d.npad;
   v.U2        = (T*)d.U2 + (size_t)w * kn;
   v.tm        = (T*)d.tm + (size_t)w * d.n * d.k;
+  v.tci       = d.tci ? d.tci + (size_t)w * 2 * 32 * d.npad : nullptr;
   v.lu        = d.lu ? d.lu + (size_t)w * 2 * nn : nullptr;
   v.ms        = d.ms + w;
   v.G         = d.G + (size_t)w * d.N * 3;

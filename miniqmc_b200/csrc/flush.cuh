@@ -38,8 +38,16 @@ __host__ __device__ constexpr size_t bsm_bytes(int k)
   return ((size_t)k * k * sizeof(double) + 15) / 16 * 16;
 }
 
+#include "flush_tc.cuh"
+
 template <typename T> __device__ void flush(const WV<T>& wv, MoveSmem& m, int s, T* smem)
 {
+  if constexpr (sizeof(T) == 4)
+    if (m.tc_on)
+    {
+      flush_tc(wv, m, s, smem);
+      return;
+    }
   using Vt         = typename Vec16<T>::type;
   constexpr int VW = Vec16<T>::width;
   constexpr int BK = FlushCfg<T>::BK, KC = FlushCfg<T>::KC, BN = FlushCfg<T>::BN;

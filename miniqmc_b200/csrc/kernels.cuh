@@ -46,8 +46,10 @@ struct LaunchCfg
 
 // fused sweep: one MC step (n_substeps x N moves + completeUpdates, then
 // evaluateGL) for every walker of every task
+// tc: FP32 Woodbury flushes on the tensor cores (every task has dw.tci,
+// k <= 32, threads >= 128)
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
-                         double accept, int threads, int max_npad, int max_k, cudaStream_t st);
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc);
 
 // evaluateLog pieces
 cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu,
@@ -90,7 +92,9 @@ cudaError_t launch_spo_points(bool fp32, const DevSystem* sys, int n_pos, const 
                               double* g, double* h, bool values_only, cudaStream_t st);
 
 // DelayedUpdate engine on one matrix (W = 1 batch view)
-cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, int max_k, cudaStream_t st);
+// tc: FP32 Woodbury flush on the tensor cores (needs dw.tci, k <= 32)
+cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, int max_k, cudaStream_t st,
+                              bool tc);
 enum DetEngineOp
 {
   DETENG_GET_INV_ROW = 0,

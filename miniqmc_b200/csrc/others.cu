@@ -29,6 +29,9 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
   const T* ions = (const T*)sys->ion_soa;
   if (tid == 0)
   {
+    m.tc_on    = 0;
+    m.tc_abort = 0;
+    m.timing   = 0;
     s_invrow   = ms->invrow_id[s];
     s_partial  = ms->partial[s];
     s_jpartial = ms->j_partial;
@@ -647,12 +650,19 @@ __global__ void __launch_bounds__(256) spo_points_kernel(const DevSystem* __rest
 }
 
 // DelayedUpdate engine on spin 0 of walker 0 of a batch view
-template <typename T> __global__ void __launch_bounds__(256) det_engine_kernel(DevWalkers dw, int op, int row)
+template <typename T>
+__global__ void __launch_bounds__(256) det_engine_kernel(DevWalkers dw, int op, int row, int tc)
 {
   __shared__ MoveSmem m;
   extern __shared__ __align__(16) unsigned char dyn[];
   T* smem        = reinterpret_cast<T*>(dyn);
   const WV<T> wv = make_wv<T>(dw, 0);
+  if (threadIdx.x == 0)
+    m.timing = 0;
+  if constexpr (sizeof(T) == 4)
+    tc_begin(m, op == DETENG_GET_INV_ROW ? 0 : tc); // accept_row flushes when the delay fills
+  else
+    tc_none(m);
   if (op == DETENG_GET_INV_ROW)
     get_inv_row(wv, m, 0, row, wv.dcount[0]);
   else if (op == DETENG_ACCEPT_ROW)
@@ -663,6 +673,8 @@ template <typename T> __global__ void __launch_bounds__(256) det_engine_kernel(D
   }
   else
     flush(wv, m, 0, smem);
+  if constexpr (sizeof(T) == 4)
+    tc_end(m);
 }
 
 // ----------------------------------------------------------- launchers --
@@ -760,19 +772,23 @@ cudaError_t launch_spo_points(bool fp32, const DevSystem* sys, int n_pos, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, int max_k, cudaStream_t st)
+cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, int max_k, cudaStream_t st, bool tc)
 {
   if (max_k > MAXK)
     return cudaErrorInvalidValue;
+  if (tc && (!fp32 || max_k > TC_KD))
+    return cudaErrorInvalidValue;
   if (fp32)
   {
-    allow_smem(det_engine_kernel<float>, flush_smem_bytes<float>());
-    det_engine_kernel<float><<<1, 256, flush_smem_bytes<float>(), st>>>(dw, op, row);
+    const size_t bytes = tc && tc_flush_smem_bytes() > flush_smem_bytes<float>() ? tc_flush_smem_bytes()
+                                                                                 : flush_smem_bytes<float>();
+    allow_smem(det_engine_kernel<float>, bytes);
+    det_engine_kernel<float><<<1, 256, bytes, st>>>(dw, op, row, tc ? 1 : 0);
   }
   else
   {
     allow_smem(det_engine_kernel<double>, flush_smem_bytes<double>());
-    det_engine_kernel<double><<<1, 256, flush_smem_bytes<double>(), st>>>(dw, op, row);
+    det_engine_kernel<double><<<1, 256, flush_smem_bytes<double>(), st>>>(dw, op, row, 0);
   }
   return cudaGetLastError();
 }

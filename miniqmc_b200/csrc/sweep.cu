@@ -14,7 +14,7 @@ namespace qmc
 {
 template <typename T>
 __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restrict__ tasks, int n_tasks, int n_substeps,
-                                                    double accept_thr)
+                                                    double accept_thr, int tc)
 {
   __shared__ SysSmem<T> ss;
   __shared__ MoveSmem m;
@@ -53,8 +53,11 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
     for (int p = 0; p < NPHASE; ++p)
       m.tacc[p] = 0;
   }
-  __syncthreads();
-  for (int l = 0; l < n_substeps; ++l)
+  if constexpr (sizeof(T) == 4)
+    tc_begin(m, tc && DET);
+  else
+    tc_none(m);
+  for (int l = 0; l < n_substeps && !m.tc_abort; ++l)
   {
     const double* urp;
     const double* dp;
@@ -87,6 +90,8 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
               task.prefetch && iel + 1 < N);
       acc += m.accept ? 1 : 0;
       __syncthreads(); // m.accept is rewritten by the next move
+      if (m.tc_abort)
+        break;
     }
     phase_mark(m, PH_REDUCE);
     if (DET)
@@ -97,6 +102,8 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
     }
     phase_mark(m, PH_COMPLETE);
   }
+  if constexpr (sizeof(T) == 4)
+    tc_end(m);
   evaluate_gl(ss, wv, m, task.dw.logpsi + w);
   phase_mark(m, PH_GL);
   if (threadIdx.x == 0)
@@ -119,22 +126,24 @@ template <typename T> static void set_smem_attr(size_t bytes)
 }
 
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
-                         double accept, int threads, int max_npad, int max_k, cudaStream_t st)
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc)
 {
   (void)max_npad;
-  if (max_k > MAXK)
+  if (max_k > MAXK || (tc && (!fp32 || max_k > TC_KD || threads < 128)))
     return cudaErrorInvalidValue;
   if (fp32)
   {
-    const size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<float>(threads, max_k);
+    size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<float>(threads, max_k);
+    if (tc && tc_flush_smem_bytes() > bytes)
+      bytes = tc_flush_smem_bytes(); // the tiles overlay the cached Binv
     set_smem_attr<float>(bytes);
-    sweep_kernel<float><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept);
+    sweep_kernel<float><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc ? 1 : 0);
   }
   else
   {
     const size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<double>(threads, max_k);
     set_smem_attr<double>(bytes);
-    sweep_kernel<double><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept);
+    sweep_kernel<double><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, 0);
   }
   return cudaGetLastError();
 }

@@ -1,0 +1,123 @@
+"""The Woodbury flush on the tensor cores (tcgen05, 3xTF32 with FP32
+accumulation) against the FP64 oracle and against the CUDA-core FP32 flush
+on the same inputs (DelayedUpdate::updateInvMat, DelayedUpdate.h:184-191)."""
+import numpy as np
+import pytest
+
+from miniqmc_b200 import api, capi
+from tests import gpu_helpers as H
+from tests.test_gpu_parity import elem_rel, rel_err
+
+pytestmark = pytest.mark.gpu
+
+# Both FP32 flushes sit at FP32 rounding amplified by the conditioning of
+# the updated matrix, which varies with the update sequence (measured for
+# the CUDA-core flush: 5e-6 to 6e-5 of the largest entry on these cases), so
+# the absolute bound only separates rounding from a wrong flush (error of
+# order 1).  A 3xTF32 product carries ~2^-22 relative error per term (the
+# dropped lo*lo term and the TF32 rounding of lo) against 2^-24 for an FP32
+# FMA, so the tensor-core flush may sit a few times above the CUDA-core one
+# on the same inputs (measured 1x to 2x): that ratio is the sharp check.
+RTOL_FLUSH = 3e-4
+TC_OVER_SIMT = 8.0
+
+
+def _engines(n, delay, rng):
+    a = rng.standard_normal((n, n)) + 3 * np.eye(n)
+    tc = api.DetEngine(H.product(), n, delay, capi.PREC_MIXED)
+    simt = api.DetEngine(H.product(), n, delay, capi.PREC_MIXED)
+    H.product().call('detengine_set_tensor_cores', simt.h, 0)
+    o = api.DetEngine(H.oracle(), n, delay)
+    for e in (tc, simt, o):
+        e.invert_transpose(a)
+    return tc, simt, o
+
+
+@pytest.mark.parametrize('n,delay,dc', [(256, 32, 32), (200, 32, 20), (300, 16, 11), (768, 32, 32),
+                                        (130, 16, 16)])
+def test_engine_flush(n, delay, dc):
+    """dc = delay: the flush inside acceptRow; dc < delay: updateInvMat of a
+    partial delay (Kd = 16 or 32 with zero-padded delays); n not a multiple
+    of 128: masked rows of the last 128-row block."""
+    rng = np.random.default_rng(n + dc)
+    tc, simt, o = _engines(n, delay, rng)
+    for r in rng.choice(n, size=dc, replace=False):
+        v = rng.standard_normal(n)
+        v[r] += 3.0
+        for e in (tc, simt, o):
+            e.get_inv_row(int(r))  # DiracDeterminant's ratio: fills row dc of Binv
+            e.accept_row(int(r), v)
+    for e in (tc, simt, o):
+        e.update_inv_mat()
+    ref = o.ainv()
+    e_tc, e_simt = rel_err(tc.ainv(), ref), rel_err(simt.ainv(), ref)
+    assert e_tc < RTOL_FLUSH, (e_tc, e_simt)
+    assert e_tc < TC_OVER_SIMT * max(e_simt, 1e-7), (e_tc, e_simt)
+    for r in (0, n // 2, n - 1):
+        assert rel_err(tc.get_inv_row(r), o.get_inv_row(r)) < RTOL_FLUSH
+
+
+def test_engine_flush_rejects_where_not_applicable():
+    e = api.DetEngine(H.product(), 64, 4)  # FP64 engine: CUDA cores only
+    with pytest.raises(api.QMCError):
+        H.product().call('detengine_set_tensor_cores', e.h, 1)
+
+
+def _nio128_pair(precision, tensor_cores=None):
+    """NiO 4x4x2 (768 orbitals per spin: 192 threads per walker), delay 32,
+    on a 24x24x12 grid: the periodic spline space (nx ny nz functions) must
+    be well above 768 for the Slater matrices to be regular."""
+    gw, ow = H.make_pair(precision=precision, walkers=1, delay=32, tiling=(4, 4, 2), grid=(24, 24, 12),
+                         jastrow='synthetic')
+    if tensor_cores is not None:
+        H.product().call('walkers_set_tensor_cores', gw.h, 1 if tensor_cores else 0)
+    return gw, ow
+
+
+def _logratio_err(r, ro):
+    return np.abs(np.log(np.abs(r['trace'][..., 0])) - np.log(np.abs(ro['trace'][..., 0]))).ravel()
+
+
+def test_sweep_nio128_fp64_matches_oracle():
+    """The plain FP64 form at the NiO-128 size: one MC step of 1536 moves
+    with delay 32 against the FP64 oracle (measured log-ratio median 9e-11,
+    p99 1e-8; the tail is near-node moves)."""
+    seeds = H.oracle_primes(1)
+    gw, ow = _nio128_pair(capi.PREC_FP64)
+    lg, lo = gw.evaluate_log(), ow.evaluate_log()
+    assert elem_rel(lg, lo).max() < 1e-12
+    ur, de = H.host_streams(seeds, gw.N, 1, 1)
+    rg = gw.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    ro = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    assert np.array_equal(rg['trace'][..., 7], ro['trace'][..., 7])
+    assert np.array_equal(rg['accepted'], ro['accepted'])
+    lr = _logratio_err(rg, ro)
+    assert np.median(lr) < 1e-9, np.median(lr)
+    assert np.percentile(lr, 99) < 1e-6, np.percentile(lr, 99)
+    assert elem_rel(rg['logpsi'], ro['logpsi']).max() < 1e-10
+
+
+def test_sweep_nio128_tensor_core_flush():
+    """The mixed form at the NiO-128 size with its flushes on the tensor
+    cores, against the FP64 oracle and against the same sweep with the
+    CUDA-core flush, on the same streams.  At this size the error of both is
+    set by the FP32 orbital evaluation amplified by the conditioning of the
+    768 x 768 Slater matrices (the initial FP32 inverse already differs from
+    the FP64 one by ~1e-5 of its largest entry; measured log-ratio median
+    9e-4 with the CUDA-core flush); the 3xTF32 flush may add a few times
+    that (measured 1.6x)."""
+    seeds = H.oracle_primes(1)
+    g_tc, ow = _nio128_pair(capi.PREC_MIXED, True)
+    g_simt, _ = _nio128_pair(capi.PREC_MIXED, False)
+    lg = [w.evaluate_log() for w in (g_tc, g_simt, ow)]
+    assert elem_rel(lg[0], lg[2]).max() < 1e-7
+    ur, de = H.host_streams(seeds, g_tc.N, 1, 1)
+    r_tc = g_tc.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    r_simt = g_simt.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    r_o = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    assert np.array_equal(r_tc['trace'][..., 7], r_o['trace'][..., 7])
+    assert np.array_equal(r_tc['accepted'], r_o['accepted'])
+    lt, ls = _logratio_err(r_tc, r_o), _logratio_err(r_simt, r_o)
+    assert np.median(lt) < 1e-2, np.median(lt)
+    assert np.median(lt) < 4 * max(np.median(ls), 1e-7), (np.median(lt), np.median(ls))
+    assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-4
