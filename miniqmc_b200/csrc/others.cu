@@ -496,6 +496,212 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
   }
 }
 
+// Blocked form of the same inverse for n <= GJB_MAX_N: the sweep operator
+// applied to 32-column panels.  Rows are never swapped; pivot rows are
+// tracked (piv[c] = row that pivots column c).  For a panel C with pivot
+// rows P the block exchange of (P, C) is
+//     A[:, C]  <- F        (the panel after unblocked Gauss-Jordan on it)
+//     A[i, J]  <- [i not in P] A[i, J] + sum_k F[i][k] A[P_k, J]   (J not in C)
+// so each panel costs one pass over the matrix instead of 32.  The panel
+// lives in shared memory.  A pivot of magnitude <= n eps max|A| counts as
+// zero (numerically singular).  At the end A holds the exchanged matrix:
+// A^{-1}[a][b] = M[piv[a]][pinv[b]], so psiM[i][j] = M[piv[j]][pinv[i]];
+// the sign of det A is the pivots' sign times the parity of piv.
+constexpr int GJB_B = 32;      // panel width
+constexpr int GJB_FS = GJB_B + 1; // padded panel row (conflict-free row-per-thread access)
+__host__ __device__ constexpr size_t gjb_smem_bytes(int n)
+{
+  return (size_t)n * GJB_FS * sizeof(double) + (size_t)GJB_B * 32 * sizeof(double) + (size_t)2 * n * sizeof(int);
+}
+constexpr size_t GJB_MAX_SMEM = 220 * 1024;
+
+template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kernel(DevWalkers dw)
+{
+  extern __shared__ __align__(16) unsigned char dyn[];
+  const int n = dw.n, npad = dw.npad;
+  double* F = reinterpret_cast<double*>(dyn);   // [n][GJB_FS] panel
+  double* R = F + (size_t)n * GJB_FS;            // [GJB_B][32] pivot rows of one column chunk
+  int* piv  = reinterpret_cast<int*>(R + GJB_B * 32); // [n] pivot row of each column
+  int* pinv = piv + n;                                 // [n] column pivoted by each row, -1 while free
+  __shared__ double s_val[32];
+  __shared__ int s_idx[32];
+  __shared__ double s_logdet, s_tiny;
+  __shared__ int s_neg, s_sing, s_p;
+  const int s = blockIdx.x, w = blockIdx.y, tid = threadIdx.x, NT = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const WV<T> wv = make_wv<T>(dw, w);
+  double* M = wv.lu + (size_t)s * n * npad;
+
+  // threshold for a zero pivot: n eps max|A|
+  double mx = 0.0;
+  for (int i = tid; i < n; i += NT)
+  {
+    pinv[i] = -1;
+    const double* row = M + (size_t)i * npad;
+    for (int j = 0; j < n; ++j)
+      mx = fmax(mx, fabs(row[j]));
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0)
+    s_val[wid] = mx;
+  __syncthreads();
+  if (tid == 0)
+  {
+    double v = 0.0;
+    for (int q = 0; q < nw; ++q)
+      v = fmax(v, s_val[q]);
+    s_tiny   = (double)n * DBL_EPSILON * v;
+    s_logdet = 0.0;
+    s_neg    = 0;
+    s_sing   = 0;
+  }
+  __syncthreads();
+  const double tiny = s_tiny;
+
+  for (int c0 = 0; c0 < n; c0 += GJB_B)
+  {
+    const int bw = min(GJB_B, n - c0);
+    for (int idx = tid; idx < n * GJB_B; idx += NT)
+    {
+      const int i = idx / GJB_B, kk = idx % GJB_B;
+      F[i * GJB_FS + kk] = kk < bw ? M[(size_t)i * npad + c0 + kk] : 0.0;
+    }
+    __syncthreads();
+    // ---- unblocked Gauss-Jordan on the panel
+    for (int kk = 0; kk < bw; ++kk)
+    {
+      double bv = -1.0;
+      int bi    = n;
+      for (int i = tid; i < n; i += NT)
+        if (pinv[i] < 0)
+        {
+          const double v = fabs(F[i * GJB_FS + kk]);
+          if (v > bv)
+            bv = v, bi = i;
+        }
+      for (int o = 16; o > 0; o >>= 1)
+      {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi    = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi))
+          bv = ov, bi = oi;
+      }
+      if (lane == 0)
+        s_val[wid] = bv, s_idx[wid] = bi;
+      __syncthreads();
+      if (tid == 0)
+      {
+        double v = s_val[0];
+        int p    = s_idx[0];
+        for (int q = 1; q < nw; ++q)
+          if (s_val[q] > v || (s_val[q] == v && s_idx[q] < p))
+            v = s_val[q], p = s_idx[q];
+        const double pv = F[p * GJB_FS + kk];
+        piv[c0 + kk]    = p;
+        pinv[p]         = c0 + kk;
+        s_p             = p;
+        if (!(fabs(pv) > tiny))
+          s_sing = 1;
+        else
+        {
+          s_logdet += log(fabs(pv));
+          if (pv < 0)
+            s_neg ^= 1;
+        }
+      }
+      __syncthreads();
+      const int p     = s_p;
+      const double pv = F[p * GJB_FS + kk];
+      if (!(fabs(pv) > tiny))
+        continue; // zero pivot: reported, column left as is
+      const double rp = 1.0 / pv;
+      __syncthreads(); // every thread has read pv before the pivot row changes
+      if (tid < bw)
+        F[p * GJB_FS + tid] = tid == kk ? rp : F[p * GJB_FS + tid] * rp;
+      __syncthreads();
+      for (int i = tid; i < n; i += NT)
+        if (i != p)
+        {
+          double* fi     = F + i * GJB_FS;
+          const double f = fi[kk];
+          for (int q = 0; q < bw; ++q)
+            fi[q] = q == kk ? -f * rp : fi[q] - f * F[p * GJB_FS + q];
+        }
+      __syncthreads();
+    }
+    // ---- the other columns, in chunks of 32: A[:, J] <- [i not in P] A[:, J] + F A[P, J]
+    for (int j0 = 0; j0 < n; j0 += 32)
+    {
+      if (j0 == c0)
+        continue;
+      const int jw = min(32, n - j0);
+      for (int idx = tid; idx < GJB_B * 32; idx += NT)
+      {
+        const int k = idx >> 5, jj = idx & 31;
+        R[idx]      = (k < bw && jj < jw) ? M[(size_t)piv[c0 + k] * npad + j0 + jj] : 0.0;
+      }
+      __syncthreads();
+      double r[GJB_B];
+#pragma unroll
+      for (int k = 0; k < GJB_B; ++k)
+        r[k] = R[k * 32 + lane];
+      if (lane < jw)
+        for (int i = wid; i < n; i += nw)
+        {
+          const int c     = pinv[i];
+          double* mi      = M + (size_t)i * npad + j0 + lane;
+          double acc      = (c >= c0 && c < c0 + bw) ? 0.0 : *mi;
+          const double* fi = F + i * GJB_FS;
+#pragma unroll
+          for (int k = 0; k < GJB_B; ++k)
+            acc = fma(fi[k], r[k], acc);
+          *mi = acc;
+        }
+      __syncthreads(); // the next chunk's pivot rows are read from M
+    }
+    for (int idx = tid; idx < n * bw; idx += NT)
+    {
+      const int i = idx / bw, kk = idx % bw;
+      M[(size_t)i * npad + c0 + kk] = F[i * GJB_FS + kk];
+    }
+    __syncthreads();
+  }
+  // psiM[i][j] = A^{-1}[j][i] = M[piv[j]][pinv[i]]
+  T* out = wv.ainv(s);
+  for (int i = wid; i < n; i += nw)
+  {
+    const int ci = pinv[i];
+    for (int j = lane; j < n; j += 32)
+      out[(size_t)i * npad + j] = (T)M[(size_t)piv[j] * npad + ci];
+  }
+  __syncthreads();
+  if (tid == 0)
+  {
+    // parity of the permutation c -> piv[c] from its cycles
+    int odd = 0;
+    for (int c = 0; c < n; ++c)
+    {
+      if (piv[c] < 0)
+        continue;
+      int j = c, len = 0;
+      while (piv[j] >= 0)
+      {
+        const int nx = piv[j];
+        piv[j]       = -1;
+        j            = nx;
+        ++len;
+      }
+      odd ^= (len - 1) & 1;
+    }
+    wv.det_log[s]   = s_logdet;
+    wv.det_phase[s] = (s_neg ^ odd) ? kPi : 0.0;
+    wv.dcount[s]    = 0;
+    if (s_sing)
+      atomicOr(wv.status, DEV_ERR_SINGULAR);
+  }
+}
+
 // J1 / J2 from scratch (OneBodyJastrow::recompute, TwoBodyJastrow::recompute):
 // warp per electron over its full rows.
 template <typename T>
@@ -718,6 +924,21 @@ cudaError_t launch_gj_inverse(bool fp32, const DevSystem* sys, const DevWalkers&
 {
   (void)sys;
   dim3 grid(n_spins, dw.W);
+  const size_t bsm = gjb_smem_bytes(dw.n);
+  if (bsm <= GJB_MAX_SMEM)
+  {
+    if (fp32)
+    {
+      allow_smem(gj_blocked_kernel<float>, bsm);
+      gj_blocked_kernel<float><<<grid, 512, bsm, st>>>(dw);
+    }
+    else
+    {
+      allow_smem(gj_blocked_kernel<double>, bsm);
+      gj_blocked_kernel<double><<<grid, 512, bsm, st>>>(dw);
+    }
+    return cudaGetLastError();
+  }
   const size_t smem = (size_t)dw.n * (sizeof(double) + sizeof(int));
   if (fp32)
   {
