@@ -7,7 +7,9 @@ Workload (default): NiO tiled 4x4x2 from the 4-atom cell -- 128 atoms,
 coefficients (5.4 GB), 512 walkers, delay rank 32, mixed precision.  One
 "step" is one MC step of miniqmc's driver loop over the whole batch: 1536
 single-electron moves per walker (evalGrad, makeMove, ratioGrad, threshold
-accept, delayed Woodbury flushes, completeUpdates) then evaluateGL.  Inputs
+accept, delayed Woodbury flushes on the tensor cores, completeUpdates)
+then evaluateGL; after every 8th step the inverses are rebuilt in FP64
+(SPO matrix + blocked Gauss-Jordan), as the configuration asks.  Inputs
 are synthetic (uniform spline coefficients from SplitMix64 seed 11,
 synthetic Jastrows, electrons from each walker's mt19937 stream).
 
@@ -38,7 +40,7 @@ MEASURED_PEAKS = os.path.join(REPO, 'MEASURED_PEAKS.json')
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--steps', type=int, default=8)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--tiling', default='4,4,2')
@@ -46,7 +48,8 @@ def parse():
     ap.add_argument('--walkers', type=int, default=512)
     ap.add_argument('--delay', type=int, default=32)
     ap.add_argument('--precision', default='mixed', choices=['mixed', 'fp64'])
-    ap.add_argument('--recompute-every', type=int, default=0)
+    ap.add_argument('--recompute-every', type=int, default=8,
+                    help='FP64 refresh of the inverses every this many MC steps (0 = never)')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-walkers', type=int, default=0)
@@ -297,11 +300,11 @@ def main():
         de = np.ascontiguousarray(rs.normal(size=(1, W, 1, N, 3)))
         pin_ur = torch.from_numpy(ur).pin_memory().numpy()
         pin_de = torch.from_numpy(de).pin_memory().numpy()
-        walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de)  # warm
+        walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de, recompute_every=args.recompute_every)  # warm
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de)
+            walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de, recompute_every=args.recompute_every)
         barrier()
         dt = time.perf_counter() - t0
         tt = torch.tensor([dt], device='cuda')
@@ -314,14 +317,22 @@ def main():
     n, I, k = spec.n_orb, spec.n_ions, args.delay
     s = 4 if args.precision == 'mixed' else 8
     bpm = algorithmic_bytes_per_move(n, N, I, k, s, a)
-    avg_launch_ms = float(np.mean(kernel_ms))
+    # the sweep kernel's own launch time: steps that also ran the periodic
+    # FP64 refresh of the inverses are left out (reported as recompute_ms)
+    R = args.recompute_every
+    refresh = [R > 0 and (args.warmup + i + 1) % R == 0 for i in range(args.steps)]
+    sweep_ms = [t for t, r in zip(kernel_ms, refresh) if not r] or kernel_ms
+    refresh_ms = [t for t, r in zip(kernel_ms, refresh) if r]
+    avg_launch_ms = float(np.mean(sweep_ms))
+    recompute_ms = float(np.mean(refresh_ms)) - avg_launch_ms if refresh_ms else None
     achieved = bpm * W * N / (avg_launch_ms / 1e3) / 1e9
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
                 'frac': achieved / pk['hbm_gbs'],
                 'traffic': (MEASURED_TRAFFIC_PER_MOVE * W * N
                             if (args.precision == 'mixed' and args.delay == 32) else None),
                 'traffic_source': 'ncu dram bytes per move (64 walkers, grid 74x74x37) x moves per launch',
-                'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm, 'kernel': 'sweep_kernel<float>'}
+                'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm,
+                'kernel': 'sweep_kernel<%s>' % ('float' if s == 4 else 'double'), 'launch_ms': avg_launch_ms}
     plain = None
     if rank == 0 and world == 1 and args.plain_steps > 0:
         pv, pms = plain_fp64_form(lib, args, api, capi, torch.cuda.Stream)
@@ -351,7 +362,8 @@ def main():
                        'l2': 'inputs larger than L2 (%.2f GB spline table, %.1f GB walker state)'
                              % (system_bytes(lib, system) / 1e9, walkers_bytes(lib, walkers) / 1e9),
                        'acceptance': a, 'parallelism': 'replicas x%d' % world,
-                       'flush': args.flush if args.precision == 'mixed' else 'simt'},
+                       'flush': args.flush if args.precision == 'mixed' else 'simt',
+                       'recompute_every': args.recompute_every, 'recompute_ms': recompute_ms},
             'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk, 'plain_fp64': plain,
             'gpu_launches': launches,
         }

@@ -243,8 +243,9 @@ typedef struct {
   int rng_mode;           /* QMC_RNG_*                                         */
   const double* ur;       /* QMC_RNG_HOST: [n_steps][W][n_substeps][N]         */
   const double* delta;    /* QMC_RNG_HOST: [n_steps][W][n_substeps][N][3]      */
-  int recompute_every;    /* FP64 LU refresh of the inverse every this many
-                             steps (0 = never)                                */
+  int recompute_every;    /* FP64 LU refresh of the inverse after every
+                             recompute_every-th MC step of the batch, counted
+                             over all sweep calls since creation (0 = never) */
   double* trace;          /* optional [n_steps][W][n_substeps][N][8]:
                              ratio, grad_new[3], grad_now[3], accepted        */
   int64_t* n_accepted;    /* optional [W] accepted-move counts (sum of steps) */

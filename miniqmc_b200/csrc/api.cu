@@ -51,6 +51,7 @@ struct qmc_walkers_s
   std::vector<void*> allocs;
   size_t bytes      = 0;
   int64_t launches  = 0;
+  int64_t steps_done = 0; // MC steps swept by this batch over all calls
   SweepTask* d_task = nullptr;
   double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;
   size_t cap_rng = 0, cap_trace = 0;
@@ -1087,7 +1088,8 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
     if (trace)
       CK(cudaMemcpyAsync(trace + (size_t)step * W * n_substeps * N * 8, w->d_trace,
                          W * n_substeps * N * 8 * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
-    if (recompute_every > 0 && (step + 1) % recompute_every == 0 && (w->sys->h.comp & QMC_WF_DET))
+    ++w->steps_done;
+    if (recompute_every > 0 && w->steps_done % recompute_every == 0 && (w->sys->h.comp & QMC_WF_DET))
     {
       int st = recompute_dets(w);
       if (st)

@@ -768,9 +768,14 @@ __device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, in
   const T* Rs = wv.Rs;
   const int NT = blockDim.x;
   T part[4] = {T(0), T(0), T(0), T(0)};
+  // a pair beyond the cutoff at both the old and the new position adds
+  // exact zeros to Uat, dUat and d2Uat (TwoBodyJastrow.h:307-353 updates
+  // every entry with new - old), so only pairs within the cutoff at either
+  // position are written back (about 3 % of the electrons in NiO cells);
+  // the loads are still issued up front so that one memory round trip
+  // covers the whole batch
   for (int j0 = threadIdx.x; j0 < N; j0 += 2 * NT)
   {
-    // issue every load of this thread's two electrons first
     T rx[2], ry[2], rz[2], ua[2], la[2], g0[2], g1[2], g2[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u)
@@ -795,23 +800,27 @@ __device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, in
       const T flip = j < iel ? T(1) : T(-1);
       const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
       const T rc2 = f.cutoff * f.cutoff;
-      T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
       T odx = (rx[u] - ox) * flip, ody = (ry[u] - oy) * flip, odz = (rz[u] - oz) * flip;
-      if (!beyond_cutoff(odx, ody, odz, ss.gb, ss.mi_scale2, rc2))
+      T ndx = (rx[u] - nx) * flip, ndy = (ry[u] - ny) * flip, ndz = (rz[u] - nz) * flip;
+      const bool o_in = !beyond_cutoff(odx, ody, odz, ss.gb, ss.mi_scale2, rc2);
+      const bool n_in = !beyond_cutoff(ndx, ndy, ndz, ss.gb, ss.mi_scale2, rc2);
+      if (!o_in && !n_in)
+        continue;
+      T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
+      if (o_in)
       {
         const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
-        odx *= flip, ody *= flip, odz *= flip;
         if (ro < f.cutoff)
           functor_vgl(f, ro, uo, duo, d2uo);
       }
-      T ndx = (rx[u] - nx) * flip, ndy = (ry[u] - ny) * flip, ndz = (rz[u] - nz) * flip;
-      if (!beyond_cutoff(ndx, ndy, ndz, ss.gb, ss.mi_scale2, rc2))
+      odx *= flip, ody *= flip, odz *= flip;
+      if (n_in)
       {
         const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
-        ndx *= flip, ndy *= flip, ndz *= flip;
         if (rn < f.cutoff)
           functor_vgl(f, rn, un, dun, d2un);
       }
+      ndx *= flip, ndy *= flip, ndz *= flip;
       const T newl = d2un + T(2) * dun;
       const T dl   = d2uo + T(2) * duo - newl;
       wv.Uat[j]   = ua[u] + (un - uo);
@@ -1037,6 +1046,12 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
     }
   }
   __syncthreads();
+  // this move's 16 stencil rows start towards L2 now, so that their HBM
+  // latency overlaps getInvRow (they may already be there when the next
+  // move was prefetched during the previous one)
+  if (DET && tid >= 32 && tid < 48)
+    prefetch_l2((const T*)sys->coefs + sp.base + ((tid - 32) >> 2) * sys->xs + ((tid - 32) & 3) * sys->ys,
+                (unsigned)(4 * sys->zs * sizeof(T)));
   if (DET && has_next && tid < 18)
   {
     // warm L2 with the next move's 16 stencil rows and its inverse and
