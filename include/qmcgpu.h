@@ -279,6 +279,75 @@ int qmc_walkers_enable_timers(qmc_walkers* w, int enable);
  * spin).  QMC_ERR_ARG when asked for where it does not apply.  Both compute
  * DelayedUpdate::updateInvMat (DelayedUpdate.h:184-191). */
 int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable);
+/* Threads (one CTA) per walker: a multiple of 32 in [max(64, 2 delay), 256];
+ * the default covers the padded orbitals with 16-byte vectors.  The kernels
+ * stride over any block size; >= 128 is needed for the tensor-core flush. */
+int qmc_walkers_set_threads(qmc_walkers* w, int threads);
+int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* tensor_cores);
+
+/* Batch groups (no reference counterpart: the reference's flex_ batch,
+ * miniqmc_sync_move.cpp:432-521, holds movers of one system).  A group
+ * advances batches of possibly different systems and electron counts, all of
+ * one precision, with ONE fused launch per MC step covering every walker of
+ * every batch; each walker keeps its own device RNG stream, so a batch's
+ * trajectory does not depend on what else is in the group (given the same
+ * threads per walker).  While the group exists its batches run on the
+ * group's stream.  With use_graph, the launch is captured once as a CUDA
+ * graph (per n_substeps / accept) and replayed each step. */
+typedef struct qmc_group_s qmc_group;
+int qmc_group_create(qmc_walkers* const* batches, int n_batches, qmc_group** out);
+int qmc_group_destroy(qmc_group* g);
+/* launch block size: at least every batch's own threads per walker */
+int qmc_group_set_threads(qmc_group* g, int threads);
+int qmc_group_use_graph(qmc_group* g, int enable);
+/* n_steps MC steps (device RNG streams) of every batch; asynchronous.
+ * recompute_every: FP64 refresh of a batch's inverses after every
+ * recompute_every-th step of that batch (0 = never). */
+int qmc_group_sweep(qmc_group* g, int n_steps, int n_substeps, double accept, int recompute_every);
+int qmc_group_sync(qmc_group* g);
+int qmc_group_stats(const qmc_group* g, int* threads, int64_t* launches, int64_t* graph_launches);
+
+/* Autotuner (no reference counterpart): times n_steps sweeps of n_walkers
+ * walkers of `sys` for each delay rank in `delays` x threads per walker
+ * {default, 128, 192, 256 above it} x flush engine {CUDA cores, tensor cores
+ * where it applies}, and returns the fastest in `best` (all timings in
+ * results[0 .. min(n, max_results)), n in *n_results). */
+typedef struct {
+  int delay;
+  int threads;
+  int tensor_cores;
+  double ms_per_step;
+} qmc_tune_result;
+int qmc_autotune(qmc_system* sys, int n_walkers, const int* delays, int n_delays, int n_steps,
+                 qmc_tune_result* results, int max_results, int* n_results, qmc_tune_result* best);
+
+/* Request loop (no reference counterpart).  Jobs (system, walkers, steps,
+ * delay rank, seed) are submitted as they arrive; each tick admits, in
+ * arrival order, every waiting job whose device footprint fits the memory
+ * budget now (walkers created, seeded and evaluated on the device), moves
+ * every walker of every running job by one MC step in ONE shared launch
+ * (block size `threads` for all jobs, so a job's results are the same alone
+ * and in any mix), and retires jobs that reached their steps (results read
+ * back, memory released).  Times are seconds since the server was created;
+ * latency = t_done - t_submit. */
+enum { QMC_JOB_WAITING = 0, QMC_JOB_RUNNING = 1, QMC_JOB_DONE = 2, QMC_JOB_FAILED = 3 };
+typedef struct {
+  int state;          /* QMC_JOB_*                                       */
+  int status;         /* QMC_OK or the failure of a failed job           */
+  int steps_done;
+  int64_t n_accepted; /* accepted moves over all walkers and steps       */
+  double logpsi_mean; /* mean log|psi| of the walkers after the last step */
+  double t_submit, t_start, t_done;
+} qmc_job_info;
+typedef struct qmc_server_s qmc_server;
+int qmc_server_create(size_t memory_budget, int threads, int recompute_every, qmc_server** out);
+int qmc_server_destroy(qmc_server* s);
+/* QMC_ERR_ADMISSION if the job alone exceeds the budget */
+int qmc_server_submit(qmc_server* s, qmc_system* sys, int n_walkers, int n_steps, int delay, uint32_t seed,
+                      int64_t* job);
+int qmc_server_tick(qmc_server* s, int* n_running, int* n_waiting);
+int qmc_server_job(qmc_server* s, int64_t job, qmc_job_info* info);
+int qmc_server_stats(const qmc_server* s, size_t* bytes_in_use, int64_t* launches, int64_t* electron_moves);
 int qmc_walkers_phase_times(qmc_walkers* w, double* ms, int* n_phases);
 
 /* DelayedUpdate + DiracMatrix on one n x n inverse, FP64 on the device

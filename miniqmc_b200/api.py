@@ -391,3 +391,101 @@ class DetEngine:
         m = np.zeros((self.n, self.n))
         self.lib.call('detengine_get_ainv', self.h, _pd(m))
         return m
+
+
+class Group:
+    """Several walker batches (possibly of different systems) advanced by one
+    fused launch per MC step (qmc_group_*)."""
+
+    def __init__(self, lib, batches):
+        self.lib = lib
+        self.batches = list(batches)
+        arr = (C.c_void_p * len(self.batches))(*[b.h.value if isinstance(b.h, C.c_void_p) else b.h
+                                                  for b in self.batches])
+        h = C.c_void_p()
+        lib.call('group_create', arr, len(self.batches), C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call('group_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_threads(self, threads):
+        self.lib.call('group_set_threads', self.h, threads)
+
+    def use_graph(self, enable=True):
+        self.lib.call('group_use_graph', self.h, 1 if enable else 0)
+
+    def sweep(self, n_steps=1, n_substeps=1, accept=0.5, recompute_every=0):
+        self.lib.call('group_sweep', self.h, n_steps, n_substeps, accept, recompute_every)
+
+    def sync(self):
+        self.lib.call('group_sync', self.h)
+
+    def stats(self):
+        t, l, gl = C.c_int(), C.c_int64(), C.c_int64()
+        self.lib.call('group_stats', self.h, C.byref(t), C.byref(l), C.byref(gl))
+        return dict(threads=t.value, launches=l.value, graph_launches=gl.value)
+
+
+def autotune(lib, system, n_walkers, delays=(8, 16, 32), n_steps=2):
+    """qmc_autotune: (best, all) as dicts."""
+    d = (C.c_int * len(delays))(*delays)
+    res = (capi.TuneResult * 64)()
+    n = C.c_int()
+    best = capi.TuneResult()
+    lib.call('autotune', system.h, n_walkers, d, len(delays), n_steps, res, 64, C.byref(n), C.byref(best))
+
+    def as_dict(r):
+        return dict(delay=r.delay, threads=r.threads, tensor_cores=r.tensor_cores, ms_per_step=r.ms_per_step)
+    return as_dict(best), [as_dict(res[i]) for i in range(min(n.value, 64))]
+
+
+class Server:
+    """The request loop (qmc_server_*): jobs admitted by device footprint,
+    every running job's walkers moved by one shared launch per tick."""
+
+    def __init__(self, lib, memory_budget, threads=128, recompute_every=0):
+        self.lib = lib
+        h = C.c_void_p()
+        lib.call('server_create', C.c_size_t(int(memory_budget)), threads, recompute_every, C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call('server_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, system, n_walkers, n_steps, delay, seed):
+        j = C.c_int64()
+        self.lib.call('server_submit', self.h, system.h, n_walkers, n_steps, delay, C.c_uint32(seed), C.byref(j))
+        return j.value
+
+    def tick(self):
+        r, w = C.c_int(), C.c_int()
+        self.lib.call('server_tick', self.h, C.byref(r), C.byref(w))
+        return r.value, w.value
+
+    def job(self, job_id):
+        info = capi.JobInfo()
+        self.lib.call('server_job', self.h, C.c_int64(job_id), C.byref(info))
+        return dict(state=info.state, status=info.status, steps_done=info.steps_done, n_accepted=info.n_accepted,
+                    logpsi_mean=info.logpsi_mean, t_submit=info.t_submit, t_start=info.t_start, t_done=info.t_done)
+
+    def stats(self):
+        b, l, m = C.c_size_t(), C.c_int64(), C.c_int64()
+        self.lib.call('server_stats', self.h, C.byref(b), C.byref(l), C.byref(m))
+        return dict(bytes_in_use=b.value, launches=l.value, electron_moves=m.value)

@@ -44,6 +44,19 @@ class SweepOpts(C.Structure):
                 ('n_accepted', C.POINTER(C.c_int64)), ('logpsi', C.POINTER(C.c_double))]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [('delay', C.c_int), ('threads', C.c_int), ('tensor_cores', C.c_int), ('ms_per_step', C.c_double)]
+
+
+JOB_WAITING, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+class JobInfo(C.Structure):
+    _fields_ = [('state', C.c_int), ('status', C.c_int), ('steps_done', C.c_int), ('n_accepted', C.c_int64),
+                ('logpsi_mean', C.c_double), ('t_submit', C.c_double), ('t_start', C.c_double),
+                ('t_done', C.c_double)]
+
+
 P = C.c_void_p
 PD = C.POINTER(C.c_double)
 PI = C.POINTER(C.c_int)
@@ -102,6 +115,22 @@ PRODUCT_ONLY = {
     'detengine_create_prec': (I, [I, I, I, C.POINTER(P)]),
     'detengine_set_tensor_cores': (I, [P, I]),
     'walkers_set_tensor_cores': (I, [P, I]),
+    'walkers_set_threads': (I, [P, I]),
+    'walkers_get_config': (I, [P, PI, PI, PI]),
+    'group_create': (I, [C.POINTER(P), I, C.POINTER(P)]),
+    'group_destroy': (I, [P]),
+    'group_set_threads': (I, [P, I]),
+    'group_use_graph': (I, [P, I]),
+    'group_sweep': (I, [P, I, I, D, I]),
+    'group_sync': (I, [P]),
+    'group_stats': (I, [P, PI, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    'autotune': (I, [P, I, PI, I, I, C.POINTER(TuneResult), I, PI, C.POINTER(TuneResult)]),
+    'server_create': (I, [C.c_size_t, I, I, C.POINTER(P)]),
+    'server_destroy': (I, [P]),
+    'server_submit': (I, [P, P, I, I, I, C.c_uint32, C.POINTER(C.c_int64)]),
+    'server_tick': (I, [P, PI, PI]),
+    'server_job': (I, [P, C.c_int64, C.POINTER(JobInfo)]),
+    'server_stats': (I, [P, C.POINTER(C.c_size_t), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     'invert_transpose_noalloc': (I, [I, P, P, PD, PD, P]),
     'sweep_async': (I, [P, I, I, D, I]),
     'walkers_sync': (I, [P]),

@@ -4,8 +4,8 @@
 // records a message retrievable with qmc_last_error(); nothing here exits the
 // process.  All compute runs in the kernels of sweep.cu / others.cu; there
 // is no host fallback for any hot-path operation.
+#include "host_api.hpp"
 #include "host_lattice.hpp"
-#include "kernels.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -15,64 +15,27 @@
 
 using namespace qmc;
 
-static thread_local std::string g_err;
+thread_local std::string g_err;
 
-static int fail(int code, const std::string& msg)
+int fail(int code, const std::string& msg)
 {
   g_err = msg;
   return code;
 }
-#define CK(call)                                                                                          \
-  do                                                                                                      \
-  {                                                                                                       \
-    cudaError_t e_ = (call);                                                                              \
-    if (e_ != cudaSuccess)                                                                                \
-      return fail(e_ == cudaErrorMemoryAllocation ? QMC_ERR_OOM : QMC_ERR_CUDA,                           \
-                  std::string(#call) + ": " + cudaGetErrorString(e_));                                    \
-  } while (0)
 
-struct qmc_system_s
-{
-  DevSystem h;          // host mirror with device pointers
-  DevSystem* d = nullptr;
-  bool fp32    = false;
-  std::vector<void*> allocs;
-  size_t bytes = 0;
-};
-
-struct qmc_walkers_s
-{
-  qmc_system* sys = nullptr;
-  DevWalkers dw{};
-  bool fp32   = false;
-  int threads = 128;
-  cudaStream_t stream = nullptr;
-  bool own_stream     = false;
-  std::vector<void*> allocs;
-  size_t bytes      = 0;
-  int64_t launches  = 0;
-  int64_t steps_done = 0; // MC steps swept by this batch over all calls
-  SweepTask* d_task = nullptr;
-  double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;
-  size_t cap_rng = 0, cap_trace = 0;
-  double* d_displ = nullptr;
-  int* d_flags    = nullptr;
-  double* d_rows  = nullptr;
-  size_t cap_rows = 0;
-  long long* d_timers = nullptr;
-  bool tc_capable = false; // FP32, >= 128 threads, k <= 32, determinant on
-  bool use_tc     = false; // Woodbury flushes on the tensor cores
-};
-
-// the tensor-core flush keeps (Binv V)^T as 32-row hi/lo tiles of up to 32
-// delays: 2 x 32 floats per padded orbital and walker
-static size_t tc_image_floats(int npad) { return (size_t)2 * 32 * npad; }
+// set while walkers_footprint sizes a batch: dalloc only counts bytes
+static thread_local bool g_dry = false;
 
 template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes, P** p, size_t count)
 {
   *p = nullptr;
   if (count == 0)
     count = 1;
+  if (g_dry)
+  {
+    bytes += count * sizeof(P);
+    return QMC_OK;
+  }
   cudaError_t e = cudaMalloc((void**)p, count * sizeof(P));
   if (e != cudaSuccess)
     return fail(QMC_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
@@ -84,7 +47,7 @@ template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes,
   return QMC_OK;
 }
 
-static int device_status(qmc_walkers* w)
+int device_status(qmc_walkers* w)
 {
   unsigned st = 0;
   CK(cudaMemcpyAsync(&st, w->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost, w->stream));
@@ -526,6 +489,8 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   d.lu = nullptr;
   if (st)
     return QMC_ERR_OOM;
+  if (g_dry)
+    return QMC_OK;
   std::vector<MoveState> ms(W);
   for (auto& m : ms)
   {
@@ -538,6 +503,26 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   CK(cudaMemcpy(d.ms, ms.data(), W * sizeof(MoveState), cudaMemcpyHostToDevice));
   return QMC_OK;
 }
+
+} // extern "C"
+
+size_t walkers_footprint(qmc_system* s, int W, int k)
+{
+  qmc_walkers_s t;
+  t.sys  = s;
+  t.fp32 = s->fp32;
+  g_dry  = true;
+  alloc_walkers(&t, s, W, k);
+  g_dry = false;
+  const int nvec    = s->h.npad / (s->fp32 ? 4 : 2);
+  const int threads = std::min(256, std::max(std::max(64, 2 * k), round_up(nvec, 32)));
+  size_t b          = t.bytes + (size_t)W * 2 * s->h.norb * s->h.npad * sizeof(double); // FP64 inverse scratch
+  if (s->fp32 && threads >= 128 && k <= 32 && (s->h.comp & QMC_WF_DET))
+    b += (size_t)W * tc_image_floats(s->h.npad) * sizeof(float);
+  return b;
+}
+
+extern "C" {
 
 static void free_walkers(qmc_walkers* w)
 {
@@ -633,11 +618,35 @@ int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count)
   *count = w->launches;
   return QMC_OK;
 }
+int qmc_walkers_set_threads(qmc_walkers* w, int threads)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  const int k = w->dw.k;
+  if (threads % 32 || threads < std::max(64, 2 * k) || threads > 256)
+    return fail(QMC_ERR_ARG, "threads per walker must be a multiple of 32 in [max(64, 2 delay), 256]");
+  if (w->use_tc && threads < 128)
+    return fail(QMC_ERR_ARG, "the tensor-core flush needs >= 128 threads per walker; switch it off first");
+  w->threads = threads;
+  return QMC_OK;
+}
+int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* tensor_cores)
+{
+  if (!w)
+    return fail(QMC_ERR_ARG, "null handle");
+  if (threads)
+    *threads = w->threads;
+  if (delay)
+    *delay = w->dw.k;
+  if (tensor_cores)
+    *tensor_cores = w->use_tc ? 1 : 0;
+  return QMC_OK;
+}
 int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable)
 {
   if (!w)
     return fail(QMC_ERR_ARG, "null handle");
-  if (enable && !w->tc_capable)
+  if (enable && (!w->tc_capable || w->threads < 128))
     return fail(QMC_ERR_ARG, "tensor-core flush needs FP32 walkers, the determinant, delay rank <= 32 and >= 128 "
                              "threads per walker (480 or more orbitals per spin in FP32 give that)");
   w->use_tc = enable != 0;
@@ -851,7 +860,9 @@ static int ensure_lu(qmc_walkers* w)
 }
 
 // FP64 refresh of both inverses from the current positions
-static int recompute_dets(qmc_walkers* w)
+} // extern "C"
+
+int recompute_dets(qmc_walkers* w)
 {
   int st = ensure_lu(w);
   if (st)
@@ -861,6 +872,8 @@ static int recompute_dets(qmc_walkers* w)
   w->launches += 2;
   return QMC_OK;
 }
+
+extern "C" {
 
 int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi)
 {
@@ -1060,18 +1073,11 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
       w->cap_trace = need;
     }
   }
-  SweepTask task{};
-  task.sys         = w->sys->d;
-  task.dw          = w->dw;
-  task.rng_mode    = rng_mode;
-  task.ur          = w->d_ur;
-  task.delta       = w->d_delta;
-  task.trace       = trace ? w->d_trace : nullptr;
-  task.first_block = 0;
-  task.timers      = w->d_timers;
-  // next-move L2 prefetch only while the batch's in-flight stencils (16 rows
-  // of 4 npad coefficients per walker) stay well inside the 126 MB L2
-  task.prefetch = (double)W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8) <= 32.0e6;
+  SweepTask task = sweep_task(w, 0);
+  task.rng_mode  = rng_mode;
+  task.ur        = w->d_ur;
+  task.delta     = w->d_delta;
+  task.trace     = trace ? w->d_trace : nullptr;
   CK(cudaMemcpyAsync(w->d_task, &task, sizeof(task), cudaMemcpyHostToDevice, w->stream));
   for (int step = 0; step < n_steps; ++step)
   {
@@ -1105,6 +1111,25 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
   }
   return QMC_OK;
 }
+
+} // extern "C"
+
+SweepTask sweep_task(qmc_walkers* w, int first_block)
+{
+  SweepTask task{};
+  task.sys         = w->sys->d;
+  task.dw          = w->dw;
+  task.rng_mode    = QMC_RNG_DEVICE;
+  task.first_block = first_block;
+  task.timers      = w->d_timers;
+  task.tc          = w->use_tc ? 1 : 0;
+  // next-move L2 prefetch only while the batch's in-flight stencils (16 rows
+  // of 4 npad coefficients per walker) stay well inside the 126 MB L2
+  task.prefetch = (double)w->dw.W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8) <= 32.0e6;
+  return task;
+}
+
+extern "C" {
 
 int qmc_sweep(qmc_walkers* w, const qmc_sweep_opts* o)
 {

@@ -1,0 +1,70 @@
+// host_api.hpp -- private host-side declarations shared by the C ABI's
+// translation units (api.cu: handles, verbs and sweeps; serve.cu: batch
+// groups, the autotuner and the request loop).
+#pragma once
+
+#include "kernels.cuh"
+#include "../../include/qmcgpu.h"
+
+#include <string>
+#include <vector>
+
+// last error message of the calling host thread (qmc_last_error)
+extern thread_local std::string g_err;
+int fail(int code, const std::string& msg);
+#define CK(call)                                                                                          \
+  do                                                                                                      \
+  {                                                                                                       \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? QMC_ERR_OOM : QMC_ERR_CUDA,                           \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                                    \
+  } while (0)
+
+struct qmc_system_s
+{
+  qmc::DevSystem h;       // host mirror with device pointers
+  qmc::DevSystem* d = nullptr;
+  bool fp32    = false;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+};
+
+struct qmc_walkers_s
+{
+  qmc_system* sys = nullptr;
+  qmc::DevWalkers dw{};
+  bool fp32   = false;
+  int threads = 128;
+  cudaStream_t stream = nullptr;
+  bool own_stream     = false;
+  std::vector<void*> allocs;
+  size_t bytes      = 0;
+  int64_t launches  = 0;
+  int64_t steps_done = 0; // MC steps swept by this batch over all calls
+  qmc::SweepTask* d_task = nullptr;
+  double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;
+  size_t cap_rng = 0, cap_trace = 0;
+  double* d_displ = nullptr;
+  int* d_flags    = nullptr;
+  double* d_rows  = nullptr;
+  size_t cap_rows = 0;
+  long long* d_timers = nullptr;
+  bool tc_capable = false; // FP32, >= 128 threads, k <= 32, determinant on
+  bool use_tc     = false; // Woodbury flushes on the tensor cores
+};
+
+// the tensor-core flush keeps (Binv V)^T as 32-row hi/lo tiles of up to 32
+// delays: 2 x 32 floats per padded orbital and walker
+inline size_t tc_image_floats(int npad) { return (size_t)2 * 32 * npad; }
+
+// device error bits of a batch -> status (and message); synchronises
+int device_status(qmc_walkers* w);
+// SPO matrices + FP64 inverse and log-det of every walker (evaluateLog's
+// determinant part, also the periodic refresh)
+int recompute_dets(qmc_walkers* w);
+// device bytes a batch of W walkers with delay k of system s will hold,
+// including the lazily allocated FP64 inverse scratch
+size_t walkers_footprint(qmc_system* s, int W, int k);
+// the sweep's SweepTask of a batch (device RNG streams)
+qmc::SweepTask sweep_task(qmc_walkers* w, int first_block);

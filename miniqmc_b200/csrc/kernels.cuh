@@ -36,6 +36,7 @@ struct SweepTask
   double* trace;        // device [W][nsub][N][8] or null
   int first_block;      // first CTA of this task in the launch
   int prefetch;         // warm L2 with the next move's coefficients
+  int tc;               // Woodbury flushes on the tensor cores (needs dw.tci)
 };
 
 struct LaunchCfg

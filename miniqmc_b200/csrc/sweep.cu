@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
       m.tacc[p] = 0;
   }
   if constexpr (sizeof(T) == 4)
-    tc_begin(m, tc && DET);
+    tc_begin(m, tc && task.tc && DET);
   else
     tc_none(m);
   for (int l = 0; l < n_substeps && !m.tc_abort; ++l)
@@ -129,7 +129,7 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
                          double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc)
 {
   (void)max_npad;
-  if (max_k > MAXK || (tc && (!fp32 || max_k > TC_KD || threads < 128)))
+  if (max_k > MAXK || (tc && (!fp32 || threads < 128))) // a task flushes on the tensor cores only if its k <= 32
     return cudaErrorInvalidValue;
   if (fp32)
   {

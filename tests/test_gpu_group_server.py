@@ -1,0 +1,127 @@
+"""Batch groups (several systems in one fused launch, optionally replayed
+from a CUDA graph), the autotuner and the request loop.  None of these has a
+reference counterpart: the checks are that each batch or job gives the same
+result as it does alone, and that admission follows the memory budget."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from miniqmc_b200 import api, capi
+from tests import gpu_helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(tiling, precision=capi.PREC_MIXED):
+    lib = H.product()
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=tuple(12 * t for t in tiling),
+                          fill=capi.FILL_UNIFORM, spo_seed=11, jastrow='synthetic')
+    return api.System(lib, spec, precision)
+
+
+def _batch(system, W, delay, seed0):
+    w = api.Walkers(system, W, delay)
+    w.init_random((np.arange(W, dtype=np.uint32) * 7919 + seed0).astype(np.uint32))
+    w.evaluate_log()
+    return w
+
+
+def _results(w):
+    acc = np.zeros(w.W, dtype=np.int64)
+    lp = np.zeros(w.W)
+    w.lib.call('sweep_results', w.h, acc.ctypes.data_as(C.POINTER(C.c_int64)), lp.ctypes.data_as(capi.PD))
+    return acc, lp, w.positions()
+
+
+@pytest.mark.parametrize('precision', [capi.PREC_MIXED, capi.PREC_FP64])
+def test_group_equals_batches_alone(precision):
+    """Two systems (48 and 96 electrons) in one launch per step, with the
+    periodic FP64 refresh, give bit-identical walkers to each batch alone."""
+    sa, sb = _system((1, 1, 1), precision), _system((2, 1, 1), precision)
+    alone = []
+    for sys_, W, k, seed in ((sa, 6, 4, 11), (sb, 5, 8, 101)):
+        w = _batch(sys_, W, k, seed)
+        w.lib.call('sweep_async', w.h, 3, 1, 0.5, 2)
+        alone.append(_results(w))
+    wa, wb = _batch(sa, 6, 4, 11), _batch(sb, 5, 8, 101)
+    g = api.Group(H.product(), [wa, wb])
+    g.sweep(3, 1, 0.5, recompute_every=2)
+    g.sync()
+    for w, ref in zip((wa, wb), alone):
+        got = _results(w)
+        assert np.array_equal(got[0], ref[0])
+        assert np.array_equal(got[1], ref[1])
+        assert np.array_equal(got[2], ref[2])
+    assert g.stats()['launches'] == 3
+
+
+def test_group_graph_replay_equals_eager():
+    sa, sb = _system((1, 1, 1)), _system((2, 1, 1))
+    out = []
+    for graph in (False, True):
+        ws = [_batch(sa, 4, 4, 7), _batch(sb, 3, 8, 9)]
+        g = api.Group(H.product(), ws)
+        g.use_graph(graph)
+        g.sweep(4, 1, 0.5)
+        g.sync()
+        out.append([_results(w) for w in ws])
+        st = g.stats()
+        assert st['graph_launches'] == (3 if graph else 0)  # the first step runs eagerly
+        g.close()
+    for a, b in zip(out[0], out[1]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+def test_autotune_returns_a_measured_candidate():
+    s = _system((2, 1, 1))
+    best, allr = api.autotune(H.product(), s, 16, delays=(4, 8), n_steps=1)
+    assert len(allr) >= 2 and best in allr
+    assert best['ms_per_step'] == min(r['ms_per_step'] for r in allr)
+    assert best['delay'] in (4, 8) and best['threads'] % 32 == 0
+
+
+def _run_server(server, jobs):
+    ids = [server.submit(*j) for j in jobs]
+    max_waiting = 0
+    for _ in range(10000):
+        running, waiting = server.tick()
+        max_waiting = max(max_waiting, waiting)
+        if running == 0 and waiting == 0:
+            break
+    infos = [server.job(i) for i in ids]
+    assert all(i['state'] == capi.JOB_DONE for i in infos), infos
+    return infos, max_waiting
+
+
+def test_server_results_alone_equal_in_the_mix():
+    lib = H.product()
+    sa, sb = _system((1, 1, 1)), _system((2, 1, 1))
+    jobs = [(sa, 8, 5, 4, 3), (sb, 4, 3, 8, 5), (sa, 3, 7, 4, 9)]
+    srv = api.Server(lib, 8 << 30, threads=128, recompute_every=4)
+    mix, _ = _run_server(srv, jobs)
+    for job, m in zip(jobs, mix):
+        alone, _ = _run_server(api.Server(lib, 8 << 30, threads=128, recompute_every=4), [job])
+        assert alone[0]['n_accepted'] == m['n_accepted']
+        assert alone[0]['logpsi_mean'] == m['logpsi_mean']
+        assert m['steps_done'] == job[2]
+        assert m['t_done'] >= m['t_start'] >= m['t_submit']
+
+
+def test_server_admission_follows_the_budget():
+    lib = H.product()
+    s = _system((2, 1, 1))
+    w = _batch(s, 8, 8, 1)
+    size = C.c_size_t()
+    lib.call('walkers_bytes', w.h, C.byref(size))
+    w.close()
+    srv = api.Server(lib, int(size.value * 1.5), threads=128)
+    infos, max_waiting = _run_server(srv, [(s, 8, 2, 8, 1), (s, 8, 2, 8, 2), (s, 8, 2, 8, 3)])
+    assert max_waiting >= 1  # one job's state at a time fits
+    starts = sorted(i['t_start'] for i in infos)
+    dones = sorted(i['t_done'] for i in infos)
+    assert starts[1] >= dones[0] and starts[2] >= dones[1]
+    with pytest.raises(api.QMCError) as ei:
+        srv.submit(s, 64, 2, 8, 4)
+    assert capi.STATUS[ei.value.status] == 'QMC_ERR_ADMISSION'
