@@ -53,6 +53,13 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-walkers', type=int, default=0)
+    ap.add_argument('--workload', default='nio128', choices=['nio128', 'uneven', 'serve'],
+                    help='nio128: the headline batch; uneven: three NiO systems in one autotuned, graph-replayed '
+                         'launch; serve: Poisson-arrival request loop')
+    ap.add_argument('--jobs', type=int, default=200, help='serve: number of jobs (the full configuration is 2000)')
+    ap.add_argument('--rate', type=float, default=20.0, help='serve: arrivals per second')
+    ap.add_argument('--budget-gb', type=float, default=100.0, help='serve: device memory budget of the server')
+    ap.add_argument('--no-tune', action='store_true', help='uneven: skip the autotuner (default launch settings)')
     ap.add_argument('--flush', default='tc', choices=['tc', 'simt'],
                     help='Woodbury flush on the tensor cores (tcgen05 3xTF32) or the CUDA cores (FP32 FMA)')
     ap.add_argument('--plain-steps', type=int, default=4,
@@ -197,6 +204,155 @@ def cpu_baseline(args, n_threads, sample_walkers):
                         % (sample_walkers, spec.n_elec, args.tiling, args.delay))
 
 
+def nio_system(lib, api, capi, tiling, precision):
+    """NiO tiling of the 4-atom cell with 37 grid points per cell edge (the
+    148x148x74 grid of the 4x4x2 cell), SplitMix64 coefficients, synthetic
+    Jastrows."""
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=tuple(37 * t for t in tiling),
+                          fill=capi.FILL_UNIFORM, spo_seed=11, jastrow='synthetic')
+    return spec, api.System(lib, spec, precision)
+
+
+def plain_rate(lib, api, capi, tiling, torch):
+    """electron-moves/s of the plain FP64 form (1 walker per launch, delay 1)
+    on one NiO tiling: one timed step after one warm-up step."""
+    spec, system = nio_system(lib, api, capi, tiling, capi.PREC_FP64)
+    w = api.Walkers(system, 1, 1)
+    w.init_random(np.array([1009], dtype=np.uint32))
+    w.evaluate_log()
+    lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
+    lib.call('walkers_sync', w.h)
+    t0 = time.perf_counter()
+    lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
+    lib.call('walkers_sync', w.h)
+    dt = time.perf_counter() - t0
+    w.close()
+    system.close()
+    return spec.n_elec / dt
+
+
+def run_extra_workload(args):
+    import torch
+    from miniqmc_b200 import api, capi
+    lib = api.Library()
+    lib.call('init', 0)
+    out = run_uneven(args, lib, api, capi, torch) if args.workload == 'uneven' else \
+        run_serve(args, lib, api, capi, torch)
+    print(json.dumps(out), flush=True)
+
+
+def run_uneven(args, lib, api, capi, torch):
+    """Three NiO systems in ONE fused launch per MC step: 256 walkers of the
+    2x2x1 cell (192 e-), 128 of 2x2x2 (384 e-), 64 of 4x2x2 (768 e-), each
+    with the delay rank, threads per walker and flush engine the autotuner
+    picked, the launch replayed from a CUDA graph."""
+    parts = [((2, 2, 1), 256), ((2, 2, 2), 128), ((4, 2, 2), 64)]
+    batches, systems, chosen = [], [], []
+    t_tune = 0.0
+    for tiling, W in parts:
+        spec, system = nio_system(lib, api, capi, tiling, capi.PREC_MIXED)
+        systems.append(system)
+        if args.no_tune:
+            best = {'delay': 16, 'threads': None, 'tensor_cores': None, 'ms_per_step': None}
+        else:
+            t0 = time.perf_counter()
+            best, _ = api.autotune(lib, system, W, delays=(8, 16, 32), n_steps=2)
+            t_tune += time.perf_counter() - t0
+        w = api.Walkers(system, W, best['delay'])
+        if best['threads'] is not None:
+            lib.call('walkers_set_tensor_cores', w.h, 0)
+            lib.call('walkers_set_threads', w.h, best['threads'])
+            if best['tensor_cores']:
+                lib.call('walkers_set_tensor_cores', w.h, 1)
+        w.init_random((np.arange(W, dtype=np.uint32) * 7919 + 1009).astype(np.uint32))
+        w.evaluate_log()
+        batches.append((spec, W, w))
+        chosen.append({'tiling': list(tiling), 'walkers': W, 'electrons': spec.n_elec, **best})
+    g = api.Group(lib, [b[2] for b in batches])
+    g.use_graph(True)
+    g.sweep(args.warmup, 1, 0.5, args.recompute_every)
+    g.sync()
+    stream = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.sweep(args.steps, 1, 0.5, args.recompute_every)
+    e1.record(stream)
+    g.sync()
+    ms = e0.elapsed_time(e1)
+    moves = sum(W * spec.n_elec for spec, W, _ in batches) * args.steps
+    st = g.stats()
+    g.close()
+    # the same batches launched one after another (one launch per batch per step)
+    t_sep = 0.0
+    for spec, W, w in batches:
+        s2 = torch.cuda.Stream()
+        lib.call('walkers_set_stream', w.h, C.c_void_p(s2.cuda_stream))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(s2)
+        lib.call('sweep_async', w.h, args.steps, 1, 0.5, args.recompute_every)
+        a1.record(s2)
+        lib.call('walkers_sync', w.h)
+        t_sep += a0.elapsed_time(a1)
+    return {'metric': 'electron-moves/s (uneven batch: 3 NiO systems in one launch)', 'value': moves / (ms / 1e3),
+            'unit': 'electron-moves/s', 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': ms / args.steps, 'higher_is_better': True, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'uneven', 'batches': chosen, 'launch_threads': st['threads'],
+                       'graph_launches': st['graph_launches'], 'recompute_every': args.recompute_every,
+                       'autotune_s': t_tune},
+            'separate_launches': {'value': moves / (t_sep / 1e3), 'ms_per_step': t_sep / args.steps}}
+
+
+def run_serve(args, lib, api, capi, torch):
+    """Request loop: jobs arrive as a Poisson process (seed 3) and are NiO
+    tilings (1,1,1)/(2,1,1)/(2,2,1)/(2,2,2)/(4,2,2) with probabilities
+    .3/.25/.2/.15/.1, 32-256 walkers, 5-50 steps, each with its own seed.
+    Reports p50/p99 latency (arrival to result) and the aggregate rate, next
+    to running the same jobs one at a time in the plain FP64 form (its time
+    from that form's rate measured on each tiling)."""
+    rng = np.random.default_rng(3)
+    tilings = [(1, 1, 1), (2, 1, 1), (2, 2, 1), (2, 2, 2), (4, 2, 2)]
+    n = args.jobs
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    kinds = rng.choice(len(tilings), size=n, p=[0.3, 0.25, 0.2, 0.15, 0.1])
+    walkers = rng.integers(32, 257, size=n)
+    steps = rng.integers(5, 51, size=n)
+    seeds = rng.integers(1, 2 ** 31 - 1, size=n)
+    systems = [nio_system(lib, api, capi, t, capi.PREC_MIXED) for t in tilings]
+    srv = api.Server(lib, args.budget_gb * 1e9, threads=128, recompute_every=8)
+    ids, lag = [], []
+    t0 = time.perf_counter()
+    sub = 0
+    while True:
+        now = time.perf_counter() - t0
+        while sub < n and arrivals[sub] <= now:
+            ids.append(srv.submit(systems[kinds[sub]][1], int(walkers[sub]), int(steps[sub]), 16, int(seeds[sub])))
+            lag.append(now - arrivals[sub])
+            sub += 1
+        running, waiting = srv.tick()
+        if sub == n and running == 0 and waiting == 0:
+            break
+        if running == 0 and waiting == 0 and sub < n:
+            time.sleep(max(0.0, arrivals[sub] - (time.perf_counter() - t0)))
+    wall = time.perf_counter() - t0
+    infos = [srv.job(i) for i in ids]
+    lat = np.array([inf['t_done'] - inf['t_submit'] + lg for inf, lg in zip(infos, lag)])
+    st = srv.stats()
+    rates = {t: plain_rate(lib, api, capi, t, torch) for t in tilings}
+    plain_s = sum(int(walkers[i]) * int(steps[i]) * systems[kinds[i]][0].n_elec / rates[tilings[kinds[i]]]
+                  for i in range(n))
+    return {'metric': 'p50/p99 job latency and electron-moves/s (request loop)',
+            'value': st['electron_moves'] / wall, 'unit': 'electron-moves/s', 'n_gpus': 1,
+            'latency_s': {'p50': float(np.percentile(lat, 50)), 'p99': float(np.percentile(lat, 99)),
+                          'max': float(lat.max())},
+            'jobs': n, 'failed': sum(inf['state'] != capi.JOB_DONE for inf in infos), 'wall_s': wall,
+            'launches': st['launches'], 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'serve', 'rate_per_s': args.rate, 'seed': 3, 'budget_gb': args.budget_gb,
+                       'threads': 128, 'delay': 16, 'recompute_every': 8},
+            'plain_fp64_one_at_a_time': {'estimated_s': plain_s, 'rates_moves_per_s':
+                                         {str(t): r for t, r in rates.items()},
+                                         'speedup_of_wall': plain_s / wall}}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -228,7 +384,16 @@ def main():
     world = int(os.environ.get('WORLD_SIZE', '1'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
     if args.impl == 'reference':
+        if args.workload != 'nio128':
+            if rank == 0:
+                print(json.dumps({'impl': 'reference', 'unavailable': 'the CPU reference arm covers the nio128 '
+                                  'workload only'}), flush=True)
+            return
         run_reference(args, rank, world)
+        return
+    if args.workload != 'nio128':
+        if rank == 0:
+            run_extra_workload(args)
         return
     import torch
     import torch.distributed as dist

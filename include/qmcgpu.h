@@ -306,6 +306,8 @@ int qmc_group_use_graph(qmc_group* g, int enable);
 int qmc_group_sweep(qmc_group* g, int n_steps, int n_substeps, double accept, int recompute_every);
 int qmc_group_sync(qmc_group* g);
 int qmc_group_stats(const qmc_group* g, int* threads, int64_t* launches, int64_t* graph_launches);
+/* the group's cudaStream_t (for events a caller records around its sweeps) */
+int qmc_group_stream(const qmc_group* g, void** stream);
 
 /* Autotuner (no reference counterpart): times n_steps sweeps of n_walkers
  * walkers of `sys` for each delay rank in `delays` x threads per walker

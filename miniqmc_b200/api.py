@@ -429,6 +429,11 @@ class Group:
     def sync(self):
         self.lib.call('group_sync', self.h)
 
+    def stream(self):
+        s = C.c_void_p()
+        self.lib.call('group_stream', self.h, C.byref(s))
+        return s.value
+
     def stats(self):
         t, l, gl = C.c_int(), C.c_int64(), C.c_int64()
         self.lib.call('group_stats', self.h, C.byref(t), C.byref(l), C.byref(gl))

@@ -123,6 +123,7 @@ PRODUCT_ONLY = {
     'group_use_graph': (I, [P, I]),
     'group_sweep': (I, [P, I, I, D, I]),
     'group_sync': (I, [P]),
+    'group_stream': (I, [P, C.POINTER(P)]),
     'group_stats': (I, [P, PI, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     'autotune': (I, [P, I, PI, I, I, C.POINTER(TuneResult), I, PI, C.POINTER(TuneResult)]),
     'server_create': (I, [C.c_size_t, I, I, C.POINTER(P)]),

@@ -266,6 +266,14 @@ int qmc_group_sync(qmc_group* g)
   return QMC_OK;
 }
 
+int qmc_group_stream(const qmc_group* g, void** stream)
+{
+  if (!g || !stream)
+    return fail(QMC_ERR_ARG, "null pointer");
+  *stream = g->stream;
+  return QMC_OK;
+}
+
 int qmc_group_stats(const qmc_group* g, int* threads, int64_t* launches, int64_t* graph_launches)
 {
   if (!g)
