@@ -204,6 +204,19 @@ def cpu_baseline(args, n_threads, sample_walkers):
                         % (sample_walkers, spec.n_elec, args.tiling, args.delay))
 
 
+def job_rate(moves_per_rank, seconds, world, device='cpu'):
+    """Whole-job rate of a replica run: every rank moved `moves_per_rank`
+    electrons; the job's time is the maximum over ranks (one all-reduce,
+    outside any timed region).  Returns (rate, max seconds)."""
+    import torch
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tmax = float(t.item())
+    return moves_per_rank * world / tmax, tmax
+
+
 def nio_system(lib, api, capi, tiling, precision):
     """NiO tiling of the 4-atom cell with 37 grid points per cell edge (the
     148x148x74 grid of the 4x4x2 cell), SplitMix64 coefficients, synthetic
@@ -449,12 +462,8 @@ def main():
     lib.call('sweep_results', walkers.h, acc.ctypes.data_as(C.POINTER(C.c_int64)), None)
     lib.call('walkers_launch_count', walkers.h, C.byref(count))
     launches = count.value - launches0
-    t = torch.tensor([ms_total], device='cuda')
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_total = float(t.item())
-    moves = W * N * args.steps * world
-    value = moves / (ms_total / 1e3)
+    value, tmax = job_rate(W * N * args.steps, ms_total / 1e3, world, device='cuda')
+    ms_total = tmax * 1e3
     a = float((acc - acc0).sum()) / (W * N * args.steps)
 
     # e2e through the public API: host random streams in, results out
@@ -472,10 +481,7 @@ def main():
             walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de, recompute_every=args.recompute_every)
         barrier()
         dt = time.perf_counter() - t0
-        tt = torch.tensor([dt], device='cuda')
-        if world > 1:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e = {'value': W * N * args.steps * world / float(tt.item()), 'unit': 'electron-moves/s',
+        e2e = {'value': job_rate(W * N * args.steps, dt, world, device='cuda')[0], 'unit': 'electron-moves/s',
                'h2d_bytes_per_step': int(ur.nbytes + de.nbytes), 'd2h_bytes_per_step': int(W * 16)}
 
     pk, pk_kind = peaks()
