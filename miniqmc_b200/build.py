@@ -1,10 +1,12 @@
-"""Build libqmcgpu.so in-tree with nvcc for sm_100a.
+"""Build libqmcgpu.so in-tree with nvcc for sm_100a, and the miniqmc driver.
 
     python miniqmc_b200/build.py [--force] [--verbose]
 
 Each .cu under miniqmc_b200/csrc compiles to an object in miniqmc_b200/_build
 (in parallel); the objects link into miniqmc_b200/libqmcgpu.so with the CUDA
 runtime linked statically, so the library needs only the driver at run time.
+miniqmc_b200/drivers/*.cpp (the miniqmc command-line driver on the C ABI)
+build with g++ into miniqmc_b200/bin/, linked against the in-tree library.
 """
 import argparse
 import concurrent.futures as cf
@@ -17,6 +19,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 BUILD = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libqmcgpu.so')
+DRIVERS = os.path.join(HERE, 'drivers')
+BIN = os.path.join(HERE, 'bin')
+CXX = os.environ.get('CXX', '/usr/bin/g++')
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
@@ -67,7 +72,24 @@ def build(force=False, verbose=False, extra_flags=()):
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError('link failed')
+    build_drivers(force)
     return LIB
+
+
+def build_drivers(force=False):
+    """Command-line drivers over the C ABI (no CUDA headers needed)."""
+    os.makedirs(BIN, exist_ok=True)
+    include = os.path.join(HERE, '..', 'include')
+    for src in sorted(glob.glob(os.path.join(DRIVERS, '*.cpp'))):
+        exe = os.path.join(BIN, os.path.basename(src)[:-4])
+        if not force and not _stale(exe, [src, LIB, os.path.join(include, 'qmcgpu.h')]):
+            continue
+        cmd = [CXX, '-O2', '-std=c++17', '-I', include, src, '-L', HERE, '-lqmcgpu',
+               '-Wl,-rpath,$ORIGIN/..', '-o', exe]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError('driver build failed: %s' % os.path.basename(src))
 
 
 if __name__ == '__main__':
