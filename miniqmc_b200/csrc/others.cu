@@ -646,17 +646,34 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
 #pragma unroll
       for (int k = 0; k < GJB_B; ++k)
         r[k] = R[k * 32 + lane];
+      // warp per row, lane per column; 4 rows per pass so that their loads
+      // are in flight together
       if (lane < jw)
-        for (int i = wid; i < n; i += nw)
+        for (int i0 = wid; i0 < n; i0 += 4 * nw)
         {
-          const int c     = pinv[i];
-          double* mi      = M + (size_t)i * npad + j0 + lane;
-          double acc      = (c >= c0 && c < c0 + bw) ? 0.0 : *mi;
-          const double* fi = F + i * GJB_FS;
+          double acc[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+          {
+            const int i = i0 + u * nw;
+            const int c = i < n ? pinv[i] : c0;
+            acc[u]      = (i >= n || (c >= c0 && c < c0 + bw)) ? 0.0 : M[(size_t)i * npad + j0 + lane];
+          }
 #pragma unroll
           for (int k = 0; k < GJB_B; ++k)
-            acc = fma(fi[k], r[k], acc);
-          *mi = acc;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+            {
+              const int i = min(i0 + u * nw, n - 1);
+              acc[u]      = fma(F[i * GJB_FS + k], r[k], acc[u]);
+            }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+          {
+            const int i = i0 + u * nw;
+            if (i < n)
+              M[(size_t)i * npad + j0 + lane] = acc[u];
+          }
         }
       __syncthreads(); // the next chunk's pivot rows are read from M
     }
