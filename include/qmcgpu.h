@@ -376,6 +376,24 @@ int qmc_detengine_get_ainv(qmc_detengine* e, double* ainv);
  * <= 32; on by default there) or on the CUDA cores. */
 int qmc_detengine_set_tensor_cores(qmc_detengine* e, int enable);
 
+/* Non-local pseudopotential ratios (NonLocalPP, the step after the
+ * diffusion in miniqmc.cpp:472-495): for every electron and every ion within
+ * rmax (minimum-image e-I distance), WaveFunction::ratio at the 12 points of
+ * NonLocalPP's quadrature sphere (NonLocalPP.hpp:61-80), rotated once per
+ * call by NonLocalPP::randomize from a stream seeded with 11 as every
+ * mover's is (NonLocalPP.hpp:58, 98-110).  Positions: QMC_NLPP_SPHERE
+ * R + displ + r rot_k (NonLocalPP::evaluate: the sphere around the ion);
+ * QMC_NLPP_DRIVER R + r rot_k - displ (the driver's makeMove), displ being
+ * DistanceTableBA's ion - electron.  Needs completeUpdates done (no pending
+ * delayed rows; QMC_ERR_STATE otherwise).  Outputs per walker: n_points and
+ * wsum = sum of ratio / 12; `ratios` (may be null) receives walker 0's
+ * ratios in (electron, ion, knot) order, at most max_ratios. */
+enum { QMC_NLPP_SPHERE = 0, QMC_NLPP_DRIVER = 1 };
+int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, double* wsum, double* ratios,
+                      int max_ratios);
+/* The rotated 12-point spheres of the first n_calls calls: out[n_calls][12][3]. */
+int qmc_nlpp_sphere(int n_calls, double* out);
+
 /* Allocation-free inverse.  No reference counterpart: the reference always
  * inverts into memory its DiracMatrix owns.  This is the FP64 Gauss-Jordan
  * of qmc_detengine_invert_transpose on caller-owned device memory: a and

@@ -305,6 +305,16 @@ class Walkers:
         self.lib.call('wf_evaluate_gl', self.h, _pd(G), _pd(L), _pd(lp))
         return G, L, lp
 
+    def nlpp(self, rmax=1.7, form=capi.NLPP_SPHERE, max_ratios=0):
+        """NonLocalPP ratios (qmc_nlpp_evaluate): (n_points[W], wsum[W],
+        walker 0's ratios or None)."""
+        n = np.zeros(self.W, dtype=np.int64)
+        ws = np.zeros(self.W)
+        r = np.zeros(max_ratios) if max_ratios else None
+        self.lib.call('nlpp_evaluate', self.h, rmax, form, n.ctypes.data_as(C.POINTER(C.c_int64)), _pd(ws),
+                      _pd(r) if r is not None else None, max_ratios)
+        return n, ws, r
+
     def components(self):
         c = np.zeros((self.W, 6))
         self.lib.call('wf_components', self.h, _pd(c))

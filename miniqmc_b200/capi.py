@@ -11,6 +11,7 @@ STATUS = {0: 'QMC_OK', 1: 'QMC_ERR_ARG', 2: 'QMC_ERR_CUDA', 3: 'QMC_ERR_OOM', 4:
           5: 'QMC_ERR_NONFINITE', 6: 'QMC_ERR_TIMEOUT', 7: 'QMC_ERR_STATE', 8: 'QMC_ERR_NODEVICE',
           9: 'QMC_ERR_ADMISSION'}
 PREC_FP64, PREC_MIXED = 0, 1
+NLPP_SPHERE, NLPP_DRIVER = 0, 1
 NOALLOC_MAX_N = 768  # largest n of qmc_invert_transpose_noalloc
 FILL_USER, FILL_REFERENCE, FILL_UNIFORM = 0, 1, 2
 LAP_HXX, LAP_TRACE = 0, 1
@@ -99,6 +100,8 @@ SIGNATURES = {
     'detengine_accept_row': (I, [P, I, PD]),
     'detengine_update_inv_mat': (I, [P]),
     'detengine_get_ainv': (I, [P, PD]),
+    'nlpp_evaluate': (I, [P, D, I, C.POINTER(C.c_int64), PD, PD, I]),
+    'nlpp_sphere': (I, [I, PD]),
 }
 
 # entry points only the product library exports

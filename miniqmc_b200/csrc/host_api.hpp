@@ -6,6 +6,7 @@
 #include "kernels.cuh"
 #include "../../include/qmcgpu.h"
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -42,6 +43,7 @@ struct qmc_walkers_s
   size_t bytes      = 0;
   int64_t launches  = 0;
   int64_t steps_done = 0; // MC steps swept by this batch over all calls
+  int64_t nlpp_calls = 0; // NonLocalPP sphere rotations drawn so far
   qmc::SweepTask* d_task = nullptr;
   double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;
   size_t cap_rng = 0, cap_trace = 0;

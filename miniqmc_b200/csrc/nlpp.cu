@@ -1,0 +1,332 @@
+// nlpp.cu -- non-local pseudopotential ratios (NonLocalPP, the step after
+// the diffusion in miniqmc's loop).
+//
+// For every electron jel and every ion iat whose minimum-image distance d is
+// below rmax, the wavefunction ratio psi(r') / psi(R) is evaluated at the 12
+// quadrature points of a sphere rotated at random once per call:
+//   QMC_NLPP_SPHERE  r' = R_jel + displ + d rot_k          (NonLocalPP::
+//                    evaluate, NonLocalPP.hpp:115-134: a sphere around the ion)
+//   QMC_NLPP_DRIVER  r' = R_jel + d rot_k - displ          (the miniqmc driver's
+//                    makeMove, miniqmc.cpp:472-495)
+// with displ the e-I displacement of DistanceTableBA (ion - electron through
+// DTD_BConds with every entry flipped, ParticleBConds.h:154-217).  The ratio
+// is WaveFunction::ratio (WaveFunction.cpp): the SPO values at r' dotted
+// with the electron's inverse row (DiracDeterminant::ratio; no delayed rows
+// are pending after completeUpdates), times exp(Vat - J1(r')) and
+// exp(Uat - J2(r')) (OneBodyJastrow / TwoBodyJastrow ratio).
+//
+// One CTA per walker.  Per electron the ions within rmax are gathered in
+// ascending order by a warp-ballot compaction; per ion the 12 knots are
+// evaluated together: every thread walks its 16-byte orbital vectors for all
+// 12 stencils (det partials in registers, warp-reduced), and the J1 / J2
+// pairs (ion or electron, knot) within the cutoff add into per-knot sums in
+// shared memory.
+#include "device.cuh"
+#include "host_api.hpp"
+
+#include <cmath>
+#include <random>
+
+namespace qmc
+{
+constexpr int NLPP_K     = 12; // quadrature points (NonLocalPP.hpp:61)
+constexpr int NLPP_MAXIN = 32; // ions within rmax of one electron
+
+struct NlppArgs
+{
+  double rot[NLPP_K][3]; // rotated unit vectors of this call
+  double rmax;
+  int form;
+  double* wsum;      // [W] sum of weight x ratio
+  long long* count;  // [W] points evaluated
+  double* ratios;    // walker 0: every ratio in (electron, ion, knot) order, or null
+  int max_ratios;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restrict__ sys, DevWalkers dw, NlppArgs a)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  __shared__ SysSmem<T> ss;
+  __shared__ SplineSmem<T> sk[NLPP_K];
+  __shared__ double vpos[NLPP_K][3];
+  __shared__ double sums[3 * NLPP_K];
+  __shared__ int s_n, wcnt[8], in_iat[NLPP_MAXIN];
+  __shared__ double in_d[NLPP_MAXIN], in_dx[NLPP_MAXIN][3];
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  load_sys(sys, ss);
+  const int w    = blockIdx.x;
+  const WV<T> wv = make_wv<T>(dw, w);
+  const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const int N = wv.N, I = ss.n_ions, npad = wv.npad, nvec = npad / VW;
+  const T* ions  = (const T*)sys->ion_soa;
+  const T* coefs = (const T*)sys->coefs;
+  if (DET && (wv.dcount[0] != 0 || wv.dcount[1] != 0))
+  {
+    if (tid == 0)
+      atomicOr(wv.status, DEV_ERR_STATE); // delayed rows pending: completeUpdates first
+    return;
+  }
+  double wsum     = 0.0;
+  long long cnt   = 0;
+  int n_out       = 0;
+  const double wk = 1.0 / NLPP_K;
+  for (int jel = 0; jel < N; ++jel)
+  {
+    const int s = jel < ss.n_up ? 0 : 1, r = jel - (s ? ss.n_up : 0);
+    const double ex = wv.R[3 * jel], ey = wv.R[3 * jel + 1], ez = wv.R[3 * jel + 2];
+    // ---- ions within rmax, in ascending order
+    if (tid == 0)
+      s_n = 0;
+    __syncthreads();
+    for (int c0 = 0; c0 < I; c0 += NT)
+    {
+      const int c = c0 + tid;
+      bool in     = false;
+      T dx = 0, dy = 0, dz = 0, rr = 0;
+      if (c < I)
+      {
+        dx = (ions[c] - (T)ex) * T(-1), dy = (ions[I + c] - (T)ey) * T(-1), dz = (ions[2 * I + c] - (T)ez) * T(-1);
+        rr = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+        dx *= T(-1), dy *= T(-1), dz *= T(-1);
+        in = rr < (T)a.rmax;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, in);
+      if (lane == 0)
+        wcnt[wid] = __popc(b);
+      __syncthreads();
+      int base = s_n;
+      for (int q = 0; q < wid; ++q)
+        base += wcnt[q];
+      const int pos = base + __popc(b & ((1u << lane) - 1u));
+      if (in)
+      {
+        if (pos < NLPP_MAXIN)
+        {
+          in_iat[pos]   = c;
+          in_d[pos]     = (double)rr;
+          in_dx[pos][0] = (double)dx, in_dx[pos][1] = (double)dy, in_dx[pos][2] = (double)dz;
+        }
+        else
+          atomicOr(wv.status, DEV_ERR_INDEX);
+      }
+      __syncthreads();
+      if (tid == 0)
+      {
+        int t = 0;
+        for (int q = 0; q < nw; ++q)
+          t += wcnt[q];
+        s_n += t;
+      }
+      __syncthreads();
+    }
+    const int n_in = min(s_n, NLPP_MAXIN);
+    for (int li = 0; li < n_in; ++li)
+    {
+      // ---- the 12 virtual positions and their stencils
+      if (tid < NLPP_K)
+      {
+        const int k     = tid;
+        const double d  = in_d[li];
+        const double sg = a.form == 0 ? 1.0 : -1.0;
+        vpos[k][0]      = ex + sg * in_dx[li][0] + d * a.rot[k][0];
+        vpos[k][1]      = ey + sg * in_dx[li][1] + d * a.rot[k][1];
+        vpos[k][2]      = ez + sg * in_dx[li][2] + d * a.rot[k][2];
+        if (DET)
+          spline_locate(sys, vpos[k], sk[k]);
+      }
+      if (tid < 3 * NLPP_K)
+        sums[tid] = 0.0;
+      __syncthreads();
+      // ---- determinant: SPO values at the 12 points . inverse row
+      if (DET)
+      {
+        T acc[NLPP_K];
+#pragma unroll
+        for (int k = 0; k < NLPP_K; ++k)
+          acc[k] = T(0);
+        const T* arow = wv.ainv(s) + (size_t)r * npad;
+        for (int q = tid; q < nvec; q += NT)
+        {
+          const Vt iv = reinterpret_cast<const Vt*>(arow)[q];
+#pragma unroll 1
+          for (int k = 0; k < NLPP_K; ++k)
+          {
+            T v[VW];
+            spline_eval_v<T>(coefs, sys->xs, sys->ys, sys->zs, sk[k], q * VW, v);
+#pragma unroll
+            for (int e = 0; e < VW; ++e)
+              acc[k] += reinterpret_cast<const T*>(&iv)[e] * v[e];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < NLPP_K; ++k)
+        {
+          const double sk2 = warp_sum((double)acc[k]);
+          if (lane == 0)
+            atomicAdd(&sums[k], sk2);
+        }
+      }
+      // ---- J1: ions within the cutoff of each point (AB row, flipped)
+      if (J1)
+        for (int idx = tid; idx < I * NLPP_K; idx += NT)
+        {
+          const int c = idx % I, k = idx / I;
+          T dx = (ions[c] - (T)vpos[k][0]) * T(-1), dy = (ions[I + c] - (T)vpos[k][1]) * T(-1),
+            dz = (ions[2 * I + c] - (T)vpos[k][2]) * T(-1);
+          const FunctorT<T>& f = ss.j1[ion_group(ss, c)];
+          if (beyond_cutoff(dx, dy, dz, ss.gb, ss.mi_scale2, f.cutoff * f.cutoff))
+            continue;
+          const T rr = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+          if (rr < f.cutoff)
+            atomicAdd(&sums[NLPP_K + k], (double)functor_v(f, rr));
+        }
+      // ---- J2: the other electrons within the cutoff of each point (AA row, flip at jel)
+      if (J2)
+      {
+        const int gi = jel < ss.n_up ? 0 : 1;
+        for (int idx = tid; idx < N * NLPP_K; idx += NT)
+        {
+          const int j = idx % N, k = idx / N;
+          if (j == jel)
+            continue;
+          const T flip = j < jel ? T(1) : T(-1);
+          T dx = (wv.Rs[j] - (T)vpos[k][0]) * flip, dy = (wv.Rs[wv.Npad + j] - (T)vpos[k][1]) * flip,
+            dz = (wv.Rs[2 * wv.Npad + j] - (T)vpos[k][2]) * flip;
+          const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+          if (beyond_cutoff(dx, dy, dz, ss.gb, ss.mi_scale2, f.cutoff * f.cutoff))
+            continue;
+          const T rr = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
+          if (rr < f.cutoff)
+            atomicAdd(&sums[2 * NLPP_K + k], (double)functor_v(f, rr));
+        }
+      }
+      __syncthreads();
+      if (tid == 0)
+      {
+        const double vat = J1 ? (double)wv.Vat[jel] : 0.0, uat = J2 ? (double)wv.Uat[jel] : 0.0;
+        for (int k = 0; k < NLPP_K; ++k)
+        {
+          double ratio = DET ? sums[k] : 1.0;
+          if (J1)
+            ratio *= exp(vat - sums[NLPP_K + k]);
+          if (J2)
+            ratio *= exp(uat - sums[2 * NLPP_K + k]);
+          wsum += wk * ratio;
+          ++cnt;
+          if (w == 0 && a.ratios && n_out < a.max_ratios)
+            a.ratios[n_out++] = ratio;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0)
+  {
+    a.wsum[w]  = wsum;
+    a.count[w] = cnt;
+  }
+}
+
+cudaError_t launch_nlpp(bool fp32, const DevSystem* sys, const DevWalkers& dw, const NlppArgs& a, int threads,
+                        cudaStream_t st)
+{
+  if (fp32)
+    nlpp_kernel<float><<<dw.W, threads, 0, st>>>(sys, dw, a);
+  else
+    nlpp_kernel<double><<<dw.W, threads, 0, st>>>(sys, dw, a);
+  return cudaGetLastError();
+}
+
+// NonLocalPP::randomize (NonLocalPP.hpp:98-110) on the 12-point sphere of
+// NonLocalPP's constructor (:61-80), call `call` (0-based) of a stream that
+// every mover seeds with 11 (:58, StdRandom::init): three uniforms per call
+void nlpp_sphere(int call, double out[NLPP_K][3])
+{
+  static const double g[NLPP_K][3] = {
+      {1.0, 0.0, 0.0},
+      {-1.0, 0.0, 0.0},
+      {0.4472135955, 0.894427191, 0.0},
+      {-0.4472135955, 0.7236067977, 0.5257311121},
+      {0.4472135955, 0.2763932023, 0.8506508084},
+      {-0.4472135955, -0.2763932023, 0.8506508084},
+      {0.4472135955, -0.7236067977, 0.5257311121},
+      {-0.4472135955, -0.894427191, 0.0},
+      {0.4472135955, -0.7236067977, -0.5257311121},
+      {-0.4472135955, -0.2763932023, -0.8506508084},
+      {0.4472135955, 0.2763932023, -0.8506508084},
+      {-0.4472135955, 0.7236067977, -0.5257311121}};
+  std::mt19937 gen(11u);
+  std::uniform_real_distribution<double> uni(0.0, 1.0);
+  double u[3] = {0, 0, 0};
+  for (int c = 0; c <= call; ++c)
+    for (int i = 0; i < 3; ++i)
+      u[i] = uni(gen);
+  const double twopi = 2 * M_PI;
+  const double phi = twopi * u[0], psi = twopi * u[1], cth = u[2] - 0.5;
+  const double sph = std::sin(phi), cph = std::cos(phi), sth = std::sqrt(1.0 - cth * cth), sps = std::sin(psi),
+               cps = std::cos(psi);
+  const double m[9] = {cph * cth * cps - sph * sps,  sph * cth * cps + cph * sps,  -sth * cps,
+                       -cph * cth * sps - sph * cps, -sph * cth * sps + cph * cps, sth * sps,
+                       cph * sth,                    sph * sth,                    cth};
+  for (int k = 0; k < NLPP_K; ++k)
+    for (int i = 0; i < 3; ++i)
+      out[k][i] = m[3 * i] * g[k][0] + m[3 * i + 1] * g[k][1] + m[3 * i + 2] * g[k][2];
+}
+
+} // namespace qmc
+
+using namespace qmc;
+
+extern "C" {
+
+int qmc_nlpp_sphere(int n_calls, double* out)
+{
+  if (n_calls < 1 || !out)
+    return fail(QMC_ERR_ARG, "bad arguments");
+  for (int c = 0; c < n_calls; ++c)
+    nlpp_sphere(c, reinterpret_cast<double(*)[3]>(out + (size_t)c * NLPP_K * 3));
+  return QMC_OK;
+}
+
+int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, double* wsum, double* ratios,
+                      int max_ratios)
+{
+  if (!w || rmax <= 0 || (form != QMC_NLPP_SPHERE && form != QMC_NLPP_DRIVER) || (ratios && max_ratios < 0))
+    return fail(QMC_ERR_ARG, "bad NLPP arguments");
+  const size_t W = w->dw.W;
+  NlppArgs a{};
+  nlpp_sphere((int)w->nlpp_calls, a.rot);
+  a.rmax       = rmax;
+  a.form       = form;
+  a.max_ratios = ratios ? max_ratios : 0;
+  double* d_w  = nullptr;
+  CK(cudaMallocAsync(&d_w, W * (sizeof(double) + sizeof(long long)) + (size_t)a.max_ratios * sizeof(double) + 8,
+                     w->stream));
+  a.wsum   = d_w;
+  a.count  = reinterpret_cast<long long*>(d_w + W);
+  a.ratios = a.max_ratios ? d_w + 2 * W : nullptr;
+  int threads = std::max(64, std::min(256, w->threads));
+  CK(launch_nlpp(w->fp32, w->sys->d, w->dw, a, threads, w->stream));
+  w->launches++;
+  w->nlpp_calls++;
+  std::vector<double> hw(W);
+  std::vector<long long> hc(W);
+  CK(cudaMemcpyAsync(hw.data(), a.wsum, W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(hc.data(), a.count, W * sizeof(long long), cudaMemcpyDeviceToHost, w->stream));
+  if (a.max_ratios)
+    CK(cudaMemcpyAsync(ratios, a.ratios, (size_t)a.max_ratios * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaFreeAsync(d_w, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  for (size_t i = 0; i < W; ++i)
+  {
+    if (wsum)
+      wsum[i] = hw[i];
+    if (n_points)
+      n_points[i] = hc[i];
+  }
+  return device_status(w);
+}
+
+} // extern "C"

@@ -27,6 +27,7 @@ struct oracle_walkers
   oracle_system* s;
   int W, k;
   std::vector<Walker> w;
+  int nlpp_calls = 0;
 };
 
 static Functor to_functor(const qmc_functor& f)
@@ -555,5 +556,34 @@ int oracle_detengine_get_ainv(oracle_detengine* e, double* ainv)
   return 0;
 }
 int oracle_detengine_delay_count(oracle_detengine* e) { return e->eng.delay_count; }
+
+int oracle_nlpp_sphere(int n_calls, double* out)
+{
+  for (int c = 0; c < n_calls; ++c)
+    nlpp_sphere(c, reinterpret_cast<double(*)[3]>(out + (size_t)c * 36));
+  return 0;
+}
+
+int oracle_nlpp_evaluate(oracle_walkers* o, double rmax, int form, int64_t* n_points, double* wsum, double* ratios,
+                         int max_ratios)
+{
+  double rot[12][3];
+  nlpp_sphere(o->nlpp_calls++, rot);
+  std::vector<double> out;
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < o->W; ++i)
+  {
+    long long cnt = 0;
+    const double s = o->w[i].nlpp(rmax, form, rot, cnt, (i == 0 && ratios) ? &out : nullptr);
+    if (wsum)
+      wsum[i] = s;
+    if (n_points)
+      n_points[i] = cnt;
+  }
+  if (ratios)
+    for (int j = 0; j < max_ratios && j < (int)out.size(); ++j)
+      ratios[j] = out[j];
+  return 0;
+}
 
 } // extern "C"

@@ -985,6 +985,42 @@ struct System
   Functor j2_uu, j2_ud;
 };
 
+// NonLocalPP's 12-point sphere (NonLocalPP.hpp:61-80) rotated by
+// NonLocalPP::randomize (:98-110) for call `call` of the stream that
+// NonLocalPP's constructor seeds with 11 (:58): three uniforms per call
+inline void nlpp_sphere(int call, double out[12][3])
+{
+  static const double g[12][3] = {{1.0, 0.0, 0.0},
+                                  {-1.0, 0.0, 0.0},
+                                  {0.4472135955, 0.894427191, 0.0},
+                                  {-0.4472135955, 0.7236067977, 0.5257311121},
+                                  {0.4472135955, 0.2763932023, 0.8506508084},
+                                  {-0.4472135955, -0.2763932023, 0.8506508084},
+                                  {0.4472135955, -0.7236067977, 0.5257311121},
+                                  {-0.4472135955, -0.894427191, 0.0},
+                                  {0.4472135955, -0.7236067977, -0.5257311121},
+                                  {-0.4472135955, -0.2763932023, -0.8506508084},
+                                  {0.4472135955, 0.2763932023, -0.8506508084},
+                                  {-0.4472135955, 0.7236067977, -0.5257311121}};
+  std::mt19937 gen(11u);
+  std::uniform_real_distribution<double> uni(0.0, 1.0);
+  double phi = 0, psi = 0, cth = 0;
+  for (int c = 0; c <= call; ++c)
+  {
+    phi = 2 * M_PI * uni(gen);
+    psi = 2 * M_PI * uni(gen);
+    cth = uni(gen) - 0.5;
+  }
+  const double sph = std::sin(phi), cph = std::cos(phi), sth = std::sqrt(1.0 - cth * cth);
+  const double sps = std::sin(psi), cps = std::cos(psi);
+  const double m[3][3] = {{cph * cth * cps - sph * sps, sph * cth * cps + cph * sps, -sth * cps},
+                          {-cph * cth * sps - sph * cps, -sph * cth * sps + cph * cps, sth * sps},
+                          {cph * sth, sph * sth, cth}};
+  for (int k = 0; k < 12; ++k)
+    for (int i = 0; i < 3; ++i)
+      out[k][i] = m[i][0] * g[k][0] + m[i][1] * g[k][1] + m[i][2] * g[k][2];
+}
+
 // --------------------------------------------------------- Walker state --
 struct Walker
 {
@@ -1487,6 +1523,39 @@ struct Walker
     return true;
   }
   void rejectMove_pset(int) { activePtcl = -1; }
+
+  // ---- NonLocalPP ratios (miniqmc.cpp:472-495, NonLocalPP.hpp:115-134) ----
+  // For every electron and every ion within rmax (the e-I row of
+  // DistanceTableBA: r and ion - electron), WaveFunction::ratio at the 12
+  // points of `rot`: form 0 puts them at R + displ + r rot_k
+  // (NonLocalPP::evaluate), form 1 at R + r rot_k - displ (the driver's
+  // makeMove).  Returns the sum of ratio / 12; appends the ratios.
+  double nlpp(double rmax, int form, const double (*rot)[3], long long& count, std::vector<double>* out)
+  {
+    const int N = sys->n_elec, I = sys->n_ions;
+    std::vector<double> r(I), dx(I), dy(I), dz(I);
+    double sum = 0.0;
+    for (int jel = 0; jel < N; ++jel)
+    {
+      ab_row(pos(jel), r.data(), dx.data(), dy.data(), dz.data());
+      for (int iat = 0; iat < I; ++iat)
+        if (r[iat] < rmax)
+          for (int k = 0; k < 12; ++k)
+          {
+            const double sg = form == 0 ? 1.0 : -1.0;
+            const Vec3 d{sg * dx[iat] + r[iat] * rot[k][0], sg * dy[iat] + r[iat] * rot[k][1],
+                         sg * dz[iat] + r[iat] * rot[k][2]};
+            makeMove(jel, d);
+            const double q = ratio(jel);
+            rejectMove_pset(jel);
+            sum += q / 12.0;
+            ++count;
+            if (out)
+              out->push_back(q);
+          }
+    }
+    return sum;
+  }
 
   // ---- WaveFunction (WaveFunction.cpp:178-279) ----
   bool evaluateLog()

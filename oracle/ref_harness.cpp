@@ -18,6 +18,7 @@
 #include <QMCWaveFunctions/Jastrow/BsplineFunctor.h>
 #include <QMCWaveFunctions/Jastrow/OneBodyJastrow.h>
 #include <QMCWaveFunctions/Jastrow/TwoBodyJastrow.h>
+#include <Drivers/NonLocalPP.hpp>
 #include <cstdio>
 #include <random>
 #include <string>
@@ -274,7 +275,23 @@ int main(int argc, char** argv)
     arr("spo_pos", pos.data(), pos.size());
     arr("spo_v", v.data(), v.size());
     arr("spo_g", g.data(), g.size());
-    arr("spo_h", h.data(), h.size(), false);
+    arr("spo_h", h.data(), h.size());
+  }
+  {
+    // NonLocalPP's rotated quadrature spheres of its first three randomize
+    // calls (its constructor reseeds its own stream with 11)
+    RandomGenerator<double> rng(7);
+    NonLocalPP<double> ecp(rng, ions);
+    ParticleSet::ParticlePos_t rot(ecp.size());
+    std::vector<double> v;
+    for (int c = 0; c < 3; ++c)
+    {
+      ecp.randomize(rot);
+      for (int k = 0; k < ecp.size(); ++k)
+        for (int d = 0; d < 3; ++d)
+          v.push_back(rot[k][d]);
+    }
+    arr("nlpp_spheres", v.data(), v.size(), false);
   }
   printf("}\n");
   return 0;

@@ -97,3 +97,13 @@ def test_splitmix_python_equals_oracle():
     orc = oracle_lib.library()
     for i in (0, 1, 17, 123456789):
         assert api.splitmix_uniform(11, i) == orc.fn['splitmix_uniform'](11, i)
+
+
+def test_nlpp_spheres_match_reference(prod):
+    """The product's host-side NonLocalPP sphere stream (no GPU needed)."""
+    import json
+    import os
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), 'golden', 'reference_dump.json')))
+    out = np.zeros(3 * 36)
+    prod.call('nlpp_sphere', 3, out.ctypes.data_as(capi.PD))
+    np.testing.assert_allclose(out, np.array(gold['nlpp_spheres']), rtol=0, atol=1e-15)
