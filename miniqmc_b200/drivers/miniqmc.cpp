@@ -19,7 +19,9 @@
 // -a (spline tiles) is accepted and ignored: the table is one tile per
 // walker CTA here.  -b (reference implementations) and -j (three-body
 // Jastrow) are not part of this library and stop the driver with a message.
-// The pseudopotential (NLPP) evaluation of the reference's loop is not built.
+// After the steps, the pseudopotential ratios of the reference's loop
+// (miniqmc.cpp:472-495) run once per step through qmc_nlpp_evaluate, with
+// -x as rmax and the driver's form of the virtual moves.
 #include "qmcgpu.h"
 
 #include <chrono>
@@ -240,11 +242,31 @@ int main(int argc, char** argv)
   o.recompute_every = refresh;
   o.n_accepted      = acc.data();
   o.logpsi          = logpsi.data();
-  double t_diff     = now_s();
-  st                = qmc_sweep(w, &o);
-  t_diff            = now_s() - t_diff;
-  if (st != QMC_OK && st != QMC_ERR_SINGULAR && check(st, "qmc_sweep"))
-    return 1;
+  // each MC step: the diffusion sweep, then the NLPP ratios of every walker
+  double t_diff = 0, t_ecp = 0;
+  int64_t nlpp_points = 0;
+  std::vector<int64_t> npts(nmovers);
+  std::vector<double> wsum(nmovers);
+  o.n_steps = 1;
+  std::vector<int64_t> acc_total(nmovers, 0);
+  for (int step = 0; step < nsteps; ++step)
+  {
+    double t0 = now_s();
+    st        = qmc_sweep(w, &o);
+    t_diff += now_s() - t0;
+    if (st != QMC_OK && st != QMC_ERR_SINGULAR && check(st, "qmc_sweep"))
+      return 1;
+    for (int i = 0; i < nmovers; ++i)
+      acc_total[i] += acc[i];
+    t0 = now_s();
+    st = qmc_nlpp_evaluate(w, rmax, QMC_NLPP_DRIVER, npts.data(), wsum.data(), nullptr, 0);
+    t_ecp += now_s() - t0;
+    if (st != QMC_OK && st != QMC_ERR_SINGULAR && check(st, "qmc_nlpp_evaluate"))
+      return 1;
+    for (int64_t p : npts)
+      nlpp_points += p;
+  }
+  acc = acc_total;
   const double t_total = now_s() - t_total0;
 
   int64_t accepted = 0;
@@ -257,6 +279,7 @@ int main(int argc, char** argv)
   std::printf("%-24s %12.5f %12.5f\n", "  Setup", t_setup, t_setup);
   std::printf("%-24s %12.5f %12.5f\n", "  Initialization", t_init, t_init);
   std::printf("%-24s %12.5f %12.5f\n", "  Diffusion", t_diff, t_diff);
+  std::printf("%-24s %12.5f %12.5f\n", "  Pseudopotential", t_ecp, t_ecp);
   if (verbose)
   {
     double lp = 0;
@@ -270,7 +293,10 @@ int main(int argc, char** argv)
               nmovers * std::pow((double)nels, 3) / t_total);
   std::printf("Diffusion throughput ( N_walkers * N_elec^3 / Diffusion time ) = %g\n",
               nmovers * std::pow((double)nels, 3) / t_diff);
+  std::printf("Pseudopotential throughput ( N_walkers * N_elec^2 / Pseudopotential time ) = %g\n",
+              nmovers * std::pow((double)nels, 2) / t_ecp);
   std::printf("Electron-moves/s ( N_walkers * steps * substeps * N_elec / Diffusion time ) = %g\n", moves / t_diff);
+  std::printf("NLPP ratios/s ( points / Pseudopotential time ) = %g\n", nlpp_points / t_ecp);
   std::printf("Accepted moves = %lld\n\n", (long long)accepted);
   qmc_walkers_destroy(w);
   qmc_system_destroy(sys);
