@@ -376,6 +376,25 @@ int qmc_detengine_get_ainv(qmc_detengine* e, double* ainv);
  * <= 32; on by default there) or on the CUDA cores. */
 int qmc_detengine_set_tensor_cores(qmc_detengine* e, int enable);
 
+/* Local kinetic energy of every walker, -1/2 sum_i (L_i + |G_i|^2), from
+ * the G and L of the last evaluateGL (WaveFunction.cpp:261-279; the fused
+ * sweep ends each step with it).  With the accepted-move counts of
+ * qmc_sweep_results (acceptance = accepted / (steps x substeps x N)) this is
+ * the VMC estimator the reference driver leaves out.  kinetic[W]. */
+int qmc_local_kinetic(qmc_walkers* w, double* kinetic);
+
+/* Checkpoint / restore of a batch (no reference counterpart: Walker.h is
+ * unused there).  The persistent walker state -- positions, inverses and
+ * orbital derivative rows, delayed-update state, log values, Jastrow
+ * arrays, RNG streams, move state, G, L, accepted counts, step and NLPP
+ * counters -- goes to / comes from a host buffer of
+ * qmc_walkers_checkpoint_bytes bytes.  Restore needs a batch of the same
+ * system, walker count, delay rank and precision; sweeping on from a
+ * restored batch gives exactly what the original would have. */
+int qmc_walkers_checkpoint_bytes(qmc_walkers* w, size_t* bytes);
+int qmc_walkers_checkpoint(qmc_walkers* w, void* buffer, size_t bytes);
+int qmc_walkers_restore(qmc_walkers* w, const void* buffer, size_t bytes);
+
 /* Non-local pseudopotential ratios (NonLocalPP, the step after the
  * diffusion in miniqmc.cpp:472-495): for every electron and every ion within
  * rmax (minimum-image e-I distance), WaveFunction::ratio at the 12 points of

@@ -305,6 +305,23 @@ class Walkers:
         self.lib.call('wf_evaluate_gl', self.h, _pd(G), _pd(L), _pd(lp))
         return G, L, lp
 
+    def local_kinetic(self):
+        ke = np.zeros(self.W)
+        self.lib.call('local_kinetic', self.h, _pd(ke))
+        return ke
+
+    def checkpoint(self):
+        """The batch's persistent state as bytes (qmc_walkers_checkpoint)."""
+        n = C.c_size_t()
+        self.lib.call('walkers_checkpoint_bytes', self.h, C.byref(n))
+        buf = (C.c_ubyte * n.value)()
+        self.lib.call('walkers_checkpoint', self.h, C.cast(buf, C.c_void_p), n)
+        return bytes(buf)
+
+    def restore(self, data):
+        buf = (C.c_ubyte * len(data)).from_buffer_copy(data)
+        self.lib.call('walkers_restore', self.h, C.cast(buf, C.c_void_p), C.c_size_t(len(data)))
+
     def nlpp(self, rmax=1.7, form=capi.NLPP_SPHERE, max_ratios=0):
         """NonLocalPP ratios (qmc_nlpp_evaluate): (n_points[W], wsum[W],
         walker 0's ratios or None)."""

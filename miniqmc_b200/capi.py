@@ -119,6 +119,10 @@ PRODUCT_ONLY = {
     'detengine_set_tensor_cores': (I, [P, I]),
     'walkers_set_tensor_cores': (I, [P, I]),
     'walkers_set_threads': (I, [P, I]),
+    'local_kinetic': (I, [P, PD]),
+    'walkers_checkpoint_bytes': (I, [P, C.POINTER(C.c_size_t)]),
+    'walkers_checkpoint': (I, [P, P, C.c_size_t]),
+    'walkers_restore': (I, [P, P, C.c_size_t]),
     'walkers_get_config': (I, [P, PI, PI, PI]),
     'group_create': (I, [C.POINTER(P), I, C.POINTER(P)]),
     'group_destroy': (I, [P]),
