@@ -45,7 +45,10 @@ enum {
   QMC_ERR_TIMEOUT = 6,   /* a bounded device wait ran out                   */
   QMC_ERR_STATE = 7,     /* call out of protocol order (e.g. accept w/o move)*/
   QMC_ERR_NODEVICE = 8,  /* no sm_100 device / library built for other arch */
-  QMC_ERR_ADMISSION = 9  /* job refused: does not fit the memory budget     */
+  QMC_ERR_ADMISSION = 9, /* job refused: does not fit the memory budget     */
+  QMC_ERR_CAPACITY = 10  /* a fixed-size device list overflowed (the J3
+                            electron lists of an ion, or the pairs of one
+                            move); the walker state is no longer valid     */
 };
 
 /* arithmetic forms */
@@ -72,9 +75,11 @@ enum {
   QMC_LAP_TRACE = 1  /* hxx + hyy + hzz                                      */
 };
 
-/* wavefunction factors (check_wfc -f Det / J1 / J2 tests them one by one,
- * check_wfc.cpp:152-156) */
-enum { QMC_WF_DET = 1, QMC_WF_J1 = 2, QMC_WF_J2 = 4, QMC_WF_ALL = 7 };
+/* wavefunction factors (check_wfc -f Det / J1 / J2 / J3 tests them one by
+ * one, check_wfc.cpp:152-156).  The three-body Jastrow is opt-in as in the
+ * reference (miniqmc -j, WaveFunction.cpp:97-100): QMC_WF_ALL and a zero
+ * mask mean Det * J1 * J2. */
+enum { QMC_WF_DET = 1, QMC_WF_J1 = 2, QMC_WF_J2 = 4, QMC_WF_ALL = 7, QMC_WF_J3 = 8 };
 
 /* random streams for the fused sweep */
 enum {
@@ -94,6 +99,17 @@ typedef struct {
   double delta_r_inv;
   double coefs[QMC_MAX_FUNCTOR_COEFS];
 } qmc_functor;
+
+/* A three-body (electron-electron-ion) polynomial functor after
+ * PolynomialFunctor3D::reset_gamma with N_eI = N_ee = 3 and C = 3
+ * (PolynomialFunctor3D.h:61-250): gamma[l*16 + m*4 + n] multiplies
+ * r_1I^l r_2I^m r_12^n, and the sum is cut off by ((r_1I - L)(r_2I - L))^3
+ * with L = cutoff / 2, the ion's cutoff radius (ThreeBodyJastrow.h:137-162). */
+#define QMC_J3_PARAMS 26
+typedef struct {
+  double cutoff;
+  double gamma[64];
+} qmc_j3_functor;
 
 /* Everything that defines one physical system (shared by all its walkers). */
 typedef struct {
@@ -116,6 +132,12 @@ typedef struct {
   qmc_functor j1[QMC_MAX_ION_GROUPS]; /* one per ion species                 */
   qmc_functor j2_uu;       /* same-spin pairs (uu and dd)                    */
   qmc_functor j2_ud;       /* opposite-spin pairs                            */
+  /* QMC_WF_J3 only: per ion species, the same-spin (uu, dd) and the
+   * opposite-spin (ud) functor (ThreeBodyJastrow::addFunc fills every spin
+   * pair with uu, then ud overwrites the unlike pairs).  All functors of a
+   * species share one cutoff. */
+  qmc_j3_functor j3_same[QMC_MAX_ION_GROUPS];
+  qmc_j3_functor j3_diff[QMC_MAX_ION_GROUPS];
 } qmc_system_desc;
 
 /* NiO builders -------------------------------------------------------- */
@@ -145,6 +167,15 @@ int qmc_nio_build(int cell, int na, int nb, int nc, int quirks, double* lattice,
  * Wigner-Seitz radius of the given cell: j1[0] = O, j1[1] = Ni. */
 int qmc_nio_jastrows(const double* lattice, qmc_functor* j1_O, qmc_functor* j1_Ni,
                      qmc_functor* j2_uu, qmc_functor* j2_ud);
+/* The reference's three-body tables (nio.hpp:171-245, buildJeeI), cutoff
+ * min(Wigner-Seitz radius, 4.8261684030): same[s] / diff[s] for ion species
+ * s = 0, 1 in the order buildJeeI adds them ("uuNi"/"udNi" to species 0,
+ * "uuO"/"udO" to species 1). */
+int qmc_nio_j3(const double* lattice, qmc_j3_functor* same, qmc_j3_functor* diff);
+/* PolynomialFunctor3D::reset_gamma: the 26 free parameters (in the
+ * reference's order) -> the 64 gammas satisfying the e-e cusp and the
+ * no-e-I-cusp constraints (PolynomialFunctor3D.h:113-250). */
+int qmc_j3_functor_setup(double rcut, const double* params, qmc_j3_functor* out);
 /* BsplineFunctor::setupParameters(n_params, rcut, cusp, params). */
 int qmc_functor_setup(int n_params, double rcut, double cusp, const double* params,
                       qmc_functor* out);
@@ -225,8 +256,8 @@ int qmc_wf_complete_updates(qmc_walkers* w);
 /* evaluateGL: G[W][N][3], L[W][N] (either may be NULL), logpsi[W]. */
 int qmc_wf_evaluate_gl(qmc_walkers* w, double* G, double* L, double* logpsi);
 /* Per-component log values and phases after the last evaluateLog /
- * accept / evaluateGL: comp[W][6] = {logdet_up, logdet_dn, phase_up,
- * phase_dn, logJ1, logJ2}. */
+ * accept / evaluateGL: comp[W][7] = {logdet_up, logdet_dn, phase_up,
+ * phase_dn, logJ1, logJ2, logJ3}. */
 int qmc_wf_components(qmc_walkers* w, double* comp);
 /* Slater-matrix inverse of one walker and spin: (A^{-1})^T, n_orb x n_orb
  * (DiracDeterminant::psiM), with any pending delayed update applied first. */

@@ -94,6 +94,21 @@ class Library:
         self.call('nio_jastrows', _pd(lat), *[C.byref(f) for f in fs])
         return dict(j1=[fs[0], fs[1]], j2_uu=fs[2], j2_ud=fs[3])
 
+    def nio_j3(self, lattice):
+        """buildJeeI's functors: dict(same=[species 0, 1], diff=[species 0, 1])."""
+        same = (capi.J3Functor * 2)()
+        diff = (capi.J3Functor * 2)()
+        lat = np.ascontiguousarray(lattice, dtype=np.float64)
+        self.call('nio_j3', _pd(lat), same, diff)
+        return dict(same=[same[0], same[1]], diff=[diff[0], diff[1]])
+
+    def j3_functor(self, rcut, params):
+        f = capi.J3Functor()
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        assert p.size == capi.J3_PARAMS
+        self.call('j3_functor_setup', rcut, _pd(p), C.byref(f))
+        return f
+
     def ws_radius(self, lattice):
         ws = C.c_double()
         lat = np.ascontiguousarray(lattice, dtype=np.float64)
@@ -174,6 +189,14 @@ class SystemSpec:
             d.j1[g] = js['j1'][g]
         d.j2_uu = js['j2_uu']
         d.j2_ud = js['j2_ud']
+        if components & capi.WF_J3:
+            # buildJeeI's tables (species 0 and 1; a third or fourth species
+            # reuses species 1's functors)
+            j3 = lib.nio_j3(ions['lattice'])
+            for g in range(ions['n_groups']):
+                d.j3_same[g] = j3['same'][min(g, 1)]
+                d.j3_diff[g] = j3['diff'][min(g, 1)]
+            js = dict(js, j3=j3)
         self.desc = d
         self.jastrows = js
 
@@ -333,7 +356,7 @@ class Walkers:
         return n, ws, r
 
     def components(self):
-        c = np.zeros((self.W, 6))
+        c = np.zeros((self.W, 7))
         self.lib.call('wf_components', self.h, _pd(c))
         return c
 

@@ -9,13 +9,14 @@ import ctypes as C
 QMC_OK = 0
 STATUS = {0: 'QMC_OK', 1: 'QMC_ERR_ARG', 2: 'QMC_ERR_CUDA', 3: 'QMC_ERR_OOM', 4: 'QMC_ERR_SINGULAR',
           5: 'QMC_ERR_NONFINITE', 6: 'QMC_ERR_TIMEOUT', 7: 'QMC_ERR_STATE', 8: 'QMC_ERR_NODEVICE',
-          9: 'QMC_ERR_ADMISSION'}
+          9: 'QMC_ERR_ADMISSION', 10: 'QMC_ERR_CAPACITY'}
 PREC_FP64, PREC_MIXED = 0, 1
 NLPP_SPHERE, NLPP_DRIVER = 0, 1
 NOALLOC_MAX_N = 768  # largest n of qmc_invert_transpose_noalloc
 FILL_USER, FILL_REFERENCE, FILL_UNIFORM = 0, 1, 2
 LAP_HXX, LAP_TRACE = 0, 1
-WF_DET, WF_J1, WF_J2, WF_ALL = 1, 2, 4, 7
+WF_DET, WF_J1, WF_J2, WF_ALL, WF_J3 = 1, 2, 4, 7, 8
+J3_PARAMS = 26
 RNG_DEVICE, RNG_HOST = 0, 1
 NIO_REF32, NIO_PRIM4 = 0, 1
 NIO_QUIRK_UNIT_IONS, NIO_QUIRK_ONE_GROUP = 1, 2
@@ -28,6 +29,10 @@ class Functor(C.Structure):
                 ('coefs', C.c_double * MAX_FUNCTOR_COEFS)]
 
 
+class J3Functor(C.Structure):
+    _fields_ = [('cutoff', C.c_double), ('gamma', C.c_double * 64)]
+
+
 class SystemDesc(C.Structure):
     _fields_ = [('lattice', C.c_double * 9), ('n_ions', C.c_int), ('n_ion_groups', C.c_int),
                 ('ion_pos', C.POINTER(C.c_double)), ('ion_group', C.POINTER(C.c_int)),
@@ -35,7 +40,8 @@ class SystemDesc(C.Structure):
                 ('grid', C.c_int * 3), ('n_orb', C.c_int), ('spo_fill', C.c_int),
                 ('spo_seed', C.c_uint64), ('spo_user_coefs', C.POINTER(C.c_double)),
                 ('lap_mode', C.c_int), ('components', C.c_int),
-                ('j1', Functor * MAX_ION_GROUPS), ('j2_uu', Functor), ('j2_ud', Functor)]
+                ('j1', Functor * MAX_ION_GROUPS), ('j2_uu', Functor), ('j2_ud', Functor),
+                ('j3_same', J3Functor * MAX_ION_GROUPS), ('j3_diff', J3Functor * MAX_ION_GROUPS)]
 
 
 class SweepOpts(C.Structure):
@@ -70,6 +76,8 @@ SIGNATURES = {
     'nio_build': (I, [I, I, I, I, I, PD, PD, PI, PI, PD]),
     'nio_jastrows': (I, [PD, C.POINTER(Functor), C.POINTER(Functor), C.POINTER(Functor), C.POINTER(Functor)]),
     'functor_setup': (I, [I, D, D, PD, C.POINTER(Functor)]),
+    'nio_j3': (I, [PD, C.POINTER(J3Functor), C.POINTER(J3Functor)]),
+    'j3_functor_setup': (I, [D, PD, C.POINTER(J3Functor)]),
     'lattice_ws_radius': (I, [PD, PD]),
     'system_create': (I, [C.POINTER(SystemDesc), I, C.POINTER(P)]),
     'system_destroy': (I, [P]),

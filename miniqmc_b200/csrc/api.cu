@@ -63,6 +63,9 @@ int device_status(qmc_walkers* w)
       return fail(QMC_ERR_TIMEOUT, "a bounded wait on the tensor-core pipeline gave up");
     if (st & DEV_ERR_STATE)
       return fail(QMC_ERR_STATE, "move protocol violated (no proposed move for this electron)");
+    if (st & DEV_ERR_CAPACITY)
+      return fail(QMC_ERR_CAPACITY, "a J3 electron list of an ion, the ions near one position or the "
+                                    "pairs of one move exceeded its fixed capacity");
     return fail(QMC_ERR_CUDA, "device error bits set");
   }
   return QMC_OK;
@@ -84,6 +87,7 @@ const char* qmc_status_string(int s)
   case QMC_ERR_STATE: return "QMC_ERR_STATE";
   case QMC_ERR_NODEVICE: return "QMC_ERR_NODEVICE";
   case QMC_ERR_ADMISSION: return "QMC_ERR_ADMISSION";
+  case QMC_ERR_CAPACITY: return "QMC_ERR_CAPACITY";
   default: return "QMC_ERR_UNKNOWN";
   }
 }
@@ -160,6 +164,47 @@ int qmc_nio_jastrows(const double* lattice, qmc_functor* j1_O, qmc_functor* j1_N
   return QMC_OK;
 }
 
+int qmc_j3_functor_setup(double rcut, const double* params, qmc_j3_functor* out)
+{
+  int st = qmc_host::j3_functor_setup(rcut, params, out);
+  return st ? fail(st, "bad three-body functor parameters") : QMC_OK;
+}
+// buildJeeI (nio.hpp:171-245): the four PolynomialFunctor3D parameter sets
+// of the reference's NiO input, in the order it adds them
+int qmc_nio_j3(const double* lattice, qmc_j3_functor* same, qmc_j3_functor* diff)
+{
+  if (!lattice || !same || !diff)
+    return fail(QMC_ERR_ARG, "null pointer");
+  static const double Y[4][QMC_J3_PARAMS] = {
+      {-0.003356164484, 0.002412623253, 0.01653623839, 0.0008341346169, -0.002808360734, 0.000710697475,
+       0.01076942152, 0.0009228283355, 0.01576022161, -0.003585259096, 0.003323106938, -0.02282975998,
+       -0.002246144403, -0.007196992871, -0.00404316239, 0.001465337212, 0.02026982926, -0.03528735393,
+       0.04594087928, -0.008776410679, -0.001552528476, -0.005554407743, 0.001858594451, 0.002001634408,
+       0.0009302256139, -0.0006304447229},
+      {-0.006861627197, 0.003278047306, 0.03324006545, 0.003097361067, -0.004710623571, 9.652180317e-06,
+       0.02212708787, -0.003718893286, 0.03390124932, -0.00710566395, 0.008807743592, -0.04281661568,
+       -0.008463011294, -0.01269994613, -0.002005229447, 0.002186590944, 0.03350196472, -0.05677253817,
+       0.07810604648, -0.009629896208, -0.006372643712, -0.01056861605, 0.002485188615, 0.008392442289,
+       1.073423014e-05, -0.0004812466328},
+      {-0.003775082438, -0.00169971229, 0.02162925441, 0.005674020544, -0.0008296047161, 0.00128057705,
+       0.005487203215, 0.001637322446, 0.02976838198, -0.0003207100945, 0.01143855436, -0.05336741304,
+       -0.00732359381, -0.01556942626, 0.0001149478453, 0.001838601199, 0.02570154203, -0.0675325214,
+       0.1080671614, -0.01258358969, 0.001839834045, -0.02422400426, 0.005154953014, 0.003510582598,
+       0.007464427016, -0.002454817757},
+      {-0.009590393593, 0.002498010871, 0.04225872633, 0.00460311261, -0.01071033503, 0.001253155062,
+       0.02934351285, -0.01823794726, 0.07224890393, -0.01020046849, 0.006310807929, -0.05655009412,
+       -0.0363775247, 0.002062411388, 0.02037856173, 0.003372676617, 0.03915277249, -0.02680556816,
+       0.08648136635, 0.01499088063, -0.02231984329, -0.02399792096, 0.001105720128, 0.02196005181,
+       0.003162638982, -0.00119645772}};
+  const double rcut = std::min(qmc_host::ws_radius(lattice), 4.8261684030);
+  for (int sp = 0; sp < 2; ++sp)
+  {
+    qmc_host::j3_functor_setup(rcut, Y[2 * sp], same + sp);
+    qmc_host::j3_functor_setup(rcut, Y[2 * sp + 1], diff + sp);
+  }
+  return QMC_OK;
+}
+
 // The synthetic Jastrows of the NiO workloads: n_params knot values per
 // functor, uniform in [-0.1, 0.1) from SplitMix64(seed, 64*f + i) with
 // f = 0 (uu), 1 (ud), 2.. (one per ion species); cutoff = half the
@@ -233,6 +278,11 @@ int qmc_system_create(const qmc_system_desc* d, int precision, qmc_system** out)
   for (int i = 1; i < d->n_ions; ++i)
     if (d->ion_group[i] < d->ion_group[i - 1])
       return fail(QMC_ERR_ARG, "ions must be grouped by species");
+  if (comp & QMC_WF_J3)
+    for (int g = 0; g < d->n_ion_groups; ++g)
+      if (!(d->j3_same[g].cutoff > 0) || d->j3_same[g].cutoff != d->j3_diff[g].cutoff)
+        // ThreeBodyJastrow::check_complete aborts on unequal radii
+        return fail(QMC_ERR_ARG, "J3 functors of an ion species need one positive cutoff");
   auto* s  = new qmc_system_s;
   s->fp32  = precision == QMC_PREC_MIXED;
   DevSystem& h = s->h;
@@ -363,6 +413,31 @@ int qmc_system_create(const qmc_system_desc* d, int precision, qmc_system** out)
     cudaMemcpy(p, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice);
     h.ion_soa = p;
   }
+  if (comp & QMC_WF_J3)
+  {
+    // gammas in the walker precision, [species][same, opposite][64]
+    std::vector<double> gm((size_t)QMC_MAX_ION_GROUPS * 2 * 64, 0.0);
+    for (int g = 0; g < d->n_ion_groups; ++g)
+    {
+      h.j3_icut[g] = 0.5 * d->j3_same[g].cutoff;
+      for (int q = 0; q < 64; ++q)
+      {
+        gm[(size_t)(2 * g) * 64 + q]     = d->j3_same[g].gamma[q];
+        gm[(size_t)(2 * g + 1) * 64 + q] = d->j3_diff[g].gamma[q];
+      }
+    }
+    void* p = nullptr;
+    if ((st = dalloc(s->allocs, s->bytes, reinterpret_cast<unsigned char**>(&p), gm.size() * (s->fp32 ? 4 : 8))))
+      return st;
+    if (s->fp32)
+    {
+      std::vector<float> f(gm.begin(), gm.end());
+      cudaMemcpy(p, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    else
+      cudaMemcpy(p, gm.data(), gm.size() * sizeof(double), cudaMemcpyHostToDevice);
+    h.j3_gamma = p;
+  }
   if ((st = dalloc(s->allocs, s->bytes, &s->d, 1)))
     return st;
   CK(cudaMemcpy(s->d, &h, sizeof(DevSystem), cudaMemcpyHostToDevice));
@@ -463,7 +538,19 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   st |= T(&d.j2_Uat, W * N);
   st |= T(&d.j2_d2Uat, W * N);
   st |= T(&d.j2_dUat, W * 3 * N);
-  st |= dalloc(L, B, &d.j_log, W * 2);
+  st |= dalloc(L, B, &d.j_log, W * 3);
+  d.j3_Uat = d.j3_d2Uat = d.j3_dUat = nullptr;
+  d.j3_cnt = d.j3_list = nullptr;
+  d.j3_cap = 0;
+  if (h.comp & QMC_WF_J3)
+  {
+    d.j3_cap = j3_list_capacity(h.n_elec, h.n_up);
+    st |= T(&d.j3_Uat, W * N);
+    st |= T(&d.j3_d2Uat, W * N);
+    st |= T(&d.j3_dUat, W * 3 * N);
+    st |= dalloc(L, B, &d.j3_cnt, W * 2 * (size_t)d.I);
+    st |= dalloc(L, B, &d.j3_list, W * 2 * (size_t)d.I * d.j3_cap);
+  }
   st |= dalloc(L, B, &d.mt, W * (size_t)(MT_N + 1));
   st |= dalloc(L, B, &d.words, W * (8 * N + 8));
   st |= dalloc(L, B, &d.ur, W * N);
@@ -491,6 +578,14 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
     return QMC_ERR_OOM;
   if (g_dry)
     return QMC_OK;
+  if (d.j3_cnt)
+  {
+    CK(cudaMemset(d.j3_cnt, 0, W * 2 * (size_t)d.I * sizeof(int)));
+    CK(cudaMemset(d.j3_Uat, 0, W * N * es));
+    CK(cudaMemset(d.j3_d2Uat, 0, W * N * es));
+    CK(cudaMemset(d.j3_dUat, 0, W * 3 * N * es));
+  }
+  CK(cudaMemset(d.j_log, 0, W * 3 * sizeof(double)));
   std::vector<MoveState> ms(W);
   for (auto& m : ms)
   {
@@ -889,6 +984,11 @@ int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi)
     CK(launch_jastrow_recompute(w->fp32, w->sys->d, w->dw, 256, w->stream));
     w->launches++;
   }
+  if (comp & QMC_WF_J3)
+  {
+    CK(launch_j3_recompute(w->fp32, w->sys->d, w->dw, 256, w->stream));
+    w->launches++;
+  }
   CK(launch_gl(w->fp32, w->sys->d, w->dw, w->threads, w->stream));
   w->launches++;
   std::vector<MoveState> ms(w->dw.W);
@@ -980,19 +1080,20 @@ int qmc_wf_components(qmc_walkers* w, double* comp)
   if (!w || !comp)
     return fail(QMC_ERR_ARG, "null pointer");
   const size_t W = w->dw.W;
-  std::vector<double> dl(2 * W), dp(2 * W), jl(2 * W);
+  std::vector<double> dl(2 * W), dp(2 * W), jl(3 * W);
   CK(cudaMemcpyAsync(dl.data(), w->dw.det_log, 2 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
   CK(cudaMemcpyAsync(dp.data(), w->dw.det_phase, 2 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
-  CK(cudaMemcpyAsync(jl.data(), w->dw.j_log, 2 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaMemcpyAsync(jl.data(), w->dw.j_log, 3 * W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
   CK(cudaStreamSynchronize(w->stream));
   for (size_t i = 0; i < W; ++i)
   {
-    comp[6 * i + 0] = dl[2 * i];
-    comp[6 * i + 1] = dl[2 * i + 1];
-    comp[6 * i + 2] = dp[2 * i];
-    comp[6 * i + 3] = dp[2 * i + 1];
-    comp[6 * i + 4] = jl[2 * i];
-    comp[6 * i + 5] = jl[2 * i + 1];
+    comp[7 * i + 0] = dl[2 * i];
+    comp[7 * i + 1] = dl[2 * i + 1];
+    comp[7 * i + 2] = dp[2 * i];
+    comp[7 * i + 3] = dp[2 * i + 1];
+    comp[7 * i + 4] = jl[3 * i];
+    comp[7 * i + 5] = jl[3 * i + 1];
+    comp[7 * i + 6] = jl[3 * i + 2];
   }
   return QMC_OK;
 }
@@ -1089,7 +1190,7 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
                          w->stream));
     }
     CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k, w->stream,
-                    w->use_tc));
+                    w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0));
     w->launches++;
     if (trace)
       CK(cudaMemcpyAsync(trace + (size_t)step * W * n_substeps * N * 8, w->d_trace,

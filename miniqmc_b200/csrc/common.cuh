@@ -1,6 +1,7 @@
 // common.cuh -- shared device/host helpers for the B200 VMC walker hot path.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -17,7 +18,8 @@ enum : unsigned
   DEV_ERR_NONFINITE = 2u,
   DEV_ERR_INDEX     = 4u,
   DEV_ERR_STATE     = 8u,
-  DEV_ERR_TIMEOUT   = 16u // a bounded wait on the tensor-core pipeline gave up
+  DEV_ERR_TIMEOUT   = 16u, // a bounded wait on the tensor-core pipeline gave up
+  DEV_ERR_CAPACITY  = 32u  // a fixed-size J3 list or pair buffer was full
 };
 
 constexpr double kPi = 3.14159265358979323846;

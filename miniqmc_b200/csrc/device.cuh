@@ -14,6 +14,7 @@
 //   radial functor            BsplineFunctor.h:222-339
 //   J1                        OneBodyJastrow.h:110-283
 //   J2                        TwoBodyJastrow.h:250-430
+//   J3                        ThreeBodyJastrow.h:30-677 (j3.cuh)
 //   determinant               DiracDeterminant.cpp:80-187
 //   delayed update            DelayedUpdate.h:95-231
 //   inverse + log|det|        DiracMatrix.h:25-38, 93-119 (Gauss-Jordan here)
@@ -39,6 +40,7 @@ template <typename T> struct SysSmem
   T rb[9], gb[9], cn[24];
   T mi_scale2;
   FunctorT<T> j1[QMC_MAX_ION_GROUPS], j2uu, j2ud;
+  T j3cut[QMC_MAX_ION_GROUPS]; // J3 ion cutoff per species
   int gfirst[QMC_MAX_ION_GROUPS], glast[QMC_MAX_ION_GROUPS];
   int n_groups, n_ions, n_elec, n_up, norb, npad, comp, lap_mode;
 };
@@ -52,7 +54,7 @@ template <typename T> struct SplineSmem
 struct MoveSmem
 {
   double red[32 * 16];
-  double sums[16];
+  double sums[24];
   double pos_old[3], pos_new[3];
   double p[MAXK + 1], wv[MAXK + 1], col[MAXK + 1];
   double ratio_det, curAt, curLap, curGrad[3], curUat, y;
@@ -102,7 +104,13 @@ template <typename T> struct WV
   T* Uat;
   T* d2Uat;
   T* dUat;
-  double* jlog;
+  T* j3Uat;
+  T* j3d2Uat;
+  T* j3dUat;
+  int* j3cnt;  // [2][I]
+  int* j3list; // [2][I][j3cap]
+  int j3cap;
+  double* jlog; // [3] J1, J2, J3
   uint32_t* mt;
   uint32_t* words;
   double* ur;
@@ -154,7 +162,13 @@ template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
   v.Uat       = (T*)d.j2_Uat + (size_t)w * d.N;
   v.d2Uat     = (T*)d.j2_d2Uat + (size_t)w * d.N;
   v.dUat      = (T*)d.j2_dUat + (size_t)w * 3 * d.N;
-  v.jlog      = d.j_log + (size_t)w * 2;
+  v.j3Uat     = d.j3_Uat ? (T*)d.j3_Uat + (size_t)w * d.N : nullptr;
+  v.j3d2Uat   = d.j3_d2Uat ? (T*)d.j3_d2Uat + (size_t)w * d.N : nullptr;
+  v.j3dUat    = d.j3_dUat ? (T*)d.j3_dUat + (size_t)w * 3 * d.N : nullptr;
+  v.j3cnt     = d.j3_cnt ? d.j3_cnt + (size_t)w * 2 * d.I : nullptr;
+  v.j3list    = d.j3_list ? d.j3_list + (size_t)w * 2 * d.I * d.j3_cap : nullptr;
+  v.j3cap     = d.j3_cap;
+  v.jlog      = d.j_log + (size_t)w * 3;
   v.mt        = d.mt + (size_t)w * (MT_N + 1);
   v.words     = d.words + (size_t)w * (8 * (size_t)d.N + 8);
   v.ur        = d.ur + (size_t)w * d.N;
@@ -205,6 +219,7 @@ template <typename T> __device__ void load_sys(const DevSystem* __restrict__ s, 
       ss.j1[g].dinv   = (T)s->j1[g].dinv;
       ss.gfirst[g]    = s->gfirst[g];
       ss.glast[g]     = s->glast[g];
+      ss.j3cut[g]     = (T)s->j3_icut[g];
     }
     ss.j2uu.n = s->j2uu.n, ss.j2uu.cutoff = (T)s->j2uu.cutoff, ss.j2uu.dinv = (T)s->j2uu.dinv;
     ss.j2ud.n = s->j2ud.n, ss.j2ud.cutoff = (T)s->j2ud.cutoff, ss.j2ud.dinv = (T)s->j2ud.dinv;
@@ -851,6 +866,12 @@ __device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, in
   __syncthreads();
 }
 
+} // namespace qmc
+
+#include "j3.cuh"
+
+namespace qmc
+{
 // ------------------------------------------------------- evaluateGL -----
 // WaveFunction::evaluateGL (WaveFunction.cpp:261-279): G, L per electron and
 // the log values; warp per electron for the determinant row dots.
@@ -858,6 +879,7 @@ template <typename T> __device__ void evaluate_gl(const SysSmem<T>& ss, const WV
 {
   const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
   const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const bool J3 = ss.comp & QMC_WF_J3;
   const int N = wv.N, npad = wv.npad;
   for (int i = wid; i < N; i += nw)
   {
@@ -897,25 +919,34 @@ template <typename T> __device__ void evaluate_gl(const SysSmem<T>& ss, const WV
           g[c] += (double)wv.dUat[c * N + i];
         l += (double)wv.d2Uat[i];
       }
+      if (J3)
+      {
+        for (int c = 0; c < 3; ++c)
+          g[c] += (double)wv.j3dUat[c * N + i];
+        l += (double)wv.j3d2Uat[i];
+      }
       for (int c = 0; c < 3; ++c)
         wv.G[3 * i + c] = g[c];
       wv.L[i] = l;
     }
   }
-  double part[2] = {0.0, 0.0};
+  double part[3] = {0.0, 0.0, 0.0};
   for (int i = tid; i < N; i += NT)
   {
     if (J1)
       part[0] += (double)wv.Vat[i];
     if (J2)
       part[1] += (double)wv.Uat[i];
+    if (J3)
+      part[2] += (double)wv.j3Uat[i];
   }
-  block_sum<2>(part, m.red, m.sums);
+  block_sum<3>(part, m.red, m.sums);
   if (tid == 0)
   {
     wv.jlog[0] = J1 ? -m.sums[0] : 0.0;
     wv.jlog[1] = J2 ? -0.5 * m.sums[1] : 0.0;
-    const double lp = (DET ? wv.det_log[0] + wv.det_log[1] : 0.0) + wv.jlog[0] + wv.jlog[1];
+    wv.jlog[2] = J3 ? -0.5 * m.sums[2] : 0.0;
+    const double lp = (DET ? wv.det_log[0] + wv.det_log[1] : 0.0) + wv.jlog[0] + wv.jlog[1] + wv.jlog[2];
     if (logpsi)
       *logpsi = lp;
   }
@@ -1011,7 +1042,9 @@ template <typename T> __device__ void rng_substep(const WV<T>& wv, int N)
 // --------------------------------------------------------- one move -----
 // evalGrad, makeMove, ratioGrad and the threshold accept of electron iel
 // (miniqmc.cpp:426-458).  Block-wide.
-template <typename T>
+// HAS_J3 = false compiles the three-body Jastrow out (launches without it
+// keep the smaller register footprint)
+template <typename T, bool HAS_J3 = true>
 __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys, const WV<T>& wv, MoveSmem& m,
                         SplineSmem<T>& sp, const T* __restrict__ ions, int iel, double accept_thr, double ur,
                         const double* dlt, double* trace, T* smem, bool has_next)
@@ -1020,6 +1053,7 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
   constexpr int VW = Vec16<T>::width;
   const int tid = threadIdx.x, NT = blockDim.x;
   const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const bool J3 = HAS_J3 && (ss.comp & QMC_WF_J3);
   const int s = iel < ss.n_up ? 0 : 1, r = iel - (s ? ss.n_up : 0);
   const int npad = wv.npad, nvec = npad / VW;
   if (tid == 0)
@@ -1067,6 +1101,15 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
       else
         prefetch_l2(wv.dpsi(s2) + (size_t)r2 * 3 * npad, (unsigned)(3 * npad * sizeof(T)));
     }
+  }
+  if (J3)
+  {
+    // J3 ratio and gradient sums of the proposed position, reduced on their
+    // own into sums[16..19] so that the triple code's registers are not live
+    // together with the determinant partials
+    double jp[4] = {0.0, 0.0, 0.0, 0.0};
+    j3_partials(ss, sys, wv, ions, *reinterpret_cast<J3Smem<T>*>(smem), iel, m.pos_new, jp);
+    block_sum<4>(jp, m.red, m.sums + 16);
   }
   // per-thread partial sums cover a few terms each: accumulate in the walker
   // precision, widen to FP64 for the block reduction
@@ -1165,6 +1208,15 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
       }
       ratio *= exp((double)wv.Uat[iel] - m.curUat);
     }
+    if (J3)
+    {
+      for (int c = 0; c < 3; ++c)
+      {
+        gn[c] += S[17 + c];
+        g0[c] += (double)wv.j3dUat[c * wv.N + iel];
+      }
+      ratio *= exp((double)wv.j3Uat[iel] - S[16]);
+    }
     if (!isfinite(ratio))
       atomicOr(wv.status, DEV_ERR_NONFINITE);
     if (trace)
@@ -1192,6 +1244,8 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
     }
     if (J2)
       j2_accept(ss, wv, m, iel);
+    if (J3)
+      j3_accept(ss, sys, wv, m, *reinterpret_cast<J3Smem<T>*>(smem), ions, iel);
     __syncthreads();
     phase_mark(m, PH_J2_ACCEPT);
     if (tid == 0)

@@ -314,4 +314,103 @@ inline int functor_setup(int n, double rcut, double cusp, const double* params, 
   return QMC_OK;
 }
 
+// PolynomialFunctor3D::reset_gamma (PolynomialFunctor3D.h:113-250) for
+// N_eI = N_ee = 3, C = 3.  The 40 distinct gammas (gamma(l,m,n) =
+// gamma(m,l,n)) obey 14 linear constraints: for every total e-I power k the
+// e-e cusp sum over l + m = k of gamma(l,m,1) vanishes, and for every power
+// k' the e-I no-cusp combination C gamma(l,0,n) - L gamma(l,1,n) over
+// l + n = k' vanishes.  Reduced row echelon form (largest pivot in the
+// column, columns whose remaining entries are all below 1e-6 skipped) splits
+// the columns into 14 pivot columns and 26 free ones; the free ones take the
+// parameters in column order and each pivot column follows from its row.
+inline int j3_functor_setup(double rcut, const double* params, qmc_j3_functor* out)
+{
+  constexpr int NEI = 3, NEE = 3, CEXP = 3;
+  constexpr int NG = (NEI + 1) * (NEI + 2) / 2 * (NEE + 1);
+  constexpr int NC = 2 * NEI + 1 + NEI + NEE + 1;
+  if (!params || !out || !(rcut > 0))
+    return QMC_ERR_ARG;
+  const double L = 0.5 * rcut;
+  // column of gamma(l, m, n): m outer, then l >= m, then n
+  int colof[NEI + 1][NEI + 1][NEE + 1];
+  int nc = 0;
+  for (int m = 0; m <= NEI; m++)
+    for (int l = m; l <= NEI; l++)
+      for (int n = 0; n <= NEE; n++)
+        colof[l][m][n] = colof[m][l][n] = nc++;
+  double A[NC][NG] = {};
+  for (int k = 0; k <= 2 * NEI; k++)
+    for (int m = 0; m <= k && m <= NEI; m++)
+    {
+      const int l = k - m;
+      if (l <= NEI)
+        A[k][colof[l][m][1]] = l > m ? 2.0 : (l == m ? 1.0 : A[k][colof[l][m][1]]);
+    }
+  for (int kp = 0; kp <= NEI + NEE; kp++)
+  {
+    double* row = A[2 * NEI + 1 + kp];
+    for (int l = 0; l <= std::min(kp, NEI); l++)
+    {
+      const int n = kp - l;
+      if (n > NEE)
+        continue;
+      row[colof[l][0][n]] = (double)CEXP;
+      row[colof[l][1][n]] = -L;
+    }
+  }
+  int pivot_col[NC];
+  bool is_free[NG];
+  for (int c = 0; c < NG; ++c)
+    is_free[c] = true;
+  int col = 0;
+  for (int r = 0; r < NC; ++r)
+  {
+    int best = -1;
+    for (; col < NG; ++col)
+    {
+      best      = r;
+      double mx = std::fabs(A[r][col]);
+      for (int q = r + 1; q < NC; ++q)
+        if (std::fabs(A[q][col]) > mx)
+          mx = std::fabs(A[q][col]), best = q;
+      if (mx >= 1.0e-6)
+        break;
+    }
+    if (col == NG)
+      return QMC_ERR_ARG;
+    for (int c = 0; c < NG; ++c)
+      std::swap(A[r][c], A[best][c]);
+    const double inv = 1.0 / A[r][col];
+    for (int c = 0; c < NG; ++c)
+      A[r][c] *= inv;
+    for (int q = 0; q < NC; ++q)
+      if (q != r)
+      {
+        const double f = A[q][col];
+        for (int c = 0; c < NG; ++c)
+          A[q][c] -= f * A[r][c];
+      }
+    pivot_col[r] = col;
+    is_free[col] = false;
+    ++col;
+  }
+  double g[NG] = {};
+  for (int c = 0, p = 0; c < NG; ++c)
+    if (is_free[c])
+      g[c] = params[p++];
+  for (int r = 0; r < NC; ++r)
+  {
+    const int pc = pivot_col[r];
+    for (int c = 0; c < NG; ++c)
+      if (c != pc)
+        g[pc] -= A[r][c] * g[c];
+  }
+  out->cutoff = rcut;
+  for (int l = 0; l <= NEI; l++)
+    for (int m = 0; m <= NEI; m++)
+      for (int n = 0; n <= NEE; n++)
+        out->gamma[16 * l + 4 * m + n] = g[colof[l][m][n]];
+  return QMC_OK;
+}
+
 } // namespace qmc_host

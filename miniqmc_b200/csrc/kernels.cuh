@@ -48,9 +48,10 @@ struct LaunchCfg
 // fused sweep: one MC step (n_substeps x N moves + completeUpdates, then
 // evaluateGL) for every walker of every task
 // tc: FP32 Woodbury flushes on the tensor cores (every task has dw.tci,
-// k <= 32, threads >= 128)
+// k <= 32, threads >= 128); j3: some task's wavefunction has the three-body
+// Jastrow (its shared-memory scratch is added to the launch)
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
-                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc);
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3);
 
 // evaluateLog pieces
 cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu,
@@ -60,6 +61,17 @@ cudaError_t launch_gj_inverse(bool fp32, const DevSystem* sys, const DevWalkers&
 cudaError_t launch_jastrow_recompute(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads,
                                      cudaStream_t st);
 cudaError_t launch_gl(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads, cudaStream_t st);
+// ThreeBodyJastrow::recompute: the per-ion electron lists and Uat, dUat, d2Uat
+cudaError_t launch_j3_recompute(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads,
+                                cudaStream_t st);
+
+// capacity of one J3 electron list (ThreeBodyJastrow::elecs_inside of one
+// ion and spin): the electrons of that spin, at most 128
+inline int j3_list_capacity(int n_elec, int n_up)
+{
+  const int m = n_up > n_elec - n_up ? n_up : n_elec - n_up;
+  return m < 128 ? m : 128;
+}
 cudaError_t launch_sync_rs(bool fp32, const DevWalkers& dw, cudaStream_t st);
 
 // drop-in verbs (all walkers of a batch, same electron)

@@ -11,6 +11,9 @@
 //   U, V     T      [W][2][k][npad]  delayed rows (DelayedUpdate::U, V)
 //   Binv     double [W][2][k][k]     k x k Woodbury block, FP64 in both forms
 //   J1 Vat/Lap T [W][N], Grad T [W][3][N]; J2 Uat/d2Uat T [W][N], dUat T [W][3][N]
+//   J3 Uat/d2Uat T [W][N], dUat T [W][3][N]; j3_cnt int [W][2][I] and
+//            j3_list int [W][2][I][cap]: the electrons of each spin within
+//            the J3 cutoff of each ion (ThreeBodyJastrow::elecs_inside)
 //   mt       uint32 [W][625]         per-walker mt19937 state + index
 // The spline table is shared by every walker of the system:
 //   coefs    T [(nx+3)][(ny+3)][(nz+3)][npad]  orbital-fastest (einspline
@@ -56,6 +59,11 @@ struct DevSystem
   int n_elec, n_up;
   int lap_mode, comp;
   DevFunctor j1[QMC_MAX_ION_GROUPS], j2uu, j2ud;
+  // three-body Jastrow: per ion species the ion cutoff (half the functor
+  // cutoff, also the L of its polynomial) and the gammas, in the walker
+  // precision, [species][0 same spin, 1 opposite spin][64]
+  double j3_icut[QMC_MAX_ION_GROUPS];
+  const void* j3_gamma;
 };
 
 // scalars of the move in progress, per walker (drop-in verb API)
@@ -70,6 +78,7 @@ struct MoveState
   double cur_ratio[2];
   double j1_curAt, j1_curLap, j1_curGrad[3];
   double j2_curUat;
+  double j3_curUat, j3_curGrad[3];
 };
 
 struct DevWalkers
@@ -93,7 +102,13 @@ struct DevWalkers
   void* j2_Uat;
   void* j2_d2Uat;
   void* j2_dUat;
-  double* j_log; // [W][2] J1, J2
+  void* j3_Uat;   // [W][N]      (null without J3)
+  void* j3_d2Uat; // [W][N]
+  void* j3_dUat;  // [W][3][N]
+  int* j3_cnt;    // [W][2][I]
+  int* j3_list;   // [W][2][I][j3_cap]
+  int j3_cap;
+  double* j_log; // [W][3] J1, J2, J3
   uint32_t* mt;  // [W][625]
   uint32_t* words; // [W][8N+4]
   double* ur;      // [W][N]

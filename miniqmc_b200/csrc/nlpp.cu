@@ -295,6 +295,8 @@ int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, 
 {
   if (!w || rmax <= 0 || (form != QMC_NLPP_SPHERE && form != QMC_NLPP_DRIVER) || (ratios && max_ratios < 0))
     return fail(QMC_ERR_ARG, "bad NLPP arguments");
+  if (w->sys->h.comp & QMC_WF_J3)
+    return fail(QMC_ERR_ARG, "NLPP ratios with the three-body Jastrow are not implemented");
   const size_t W = w->dw.W;
   NlppArgs a{};
   nlpp_sphere((int)w->nlpp_calls, a.rot);

@@ -23,6 +23,8 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
   const WV<T> wv = make_wv<T>(dw, w);
   MoveState* ms  = wv.ms;
   const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const bool J3 = ss.comp & QMC_WF_J3;
+  J3Smem<T>& J  = *reinterpret_cast<J3Smem<T>*>(dyn);
   const int iat = a.iat;
   const int s = iat < ss.n_up ? 0 : 1, r = iat - (s ? ss.n_up : 0);
   const int npad = wv.npad, nvec = npad / VW, N = wv.N;
@@ -87,6 +89,8 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
           g += (double)wv.Grad[c * N + iat];
         if (J2)
           g += (double)wv.dUat[c * N + iat];
+        if (J3)
+          g += (double)wv.j3dUat[c * N + iat];
         dw.out_grad[3 * w + c] = g;
       }
     }
@@ -158,6 +162,12 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
     }
     if (J2)
       j2_partials(ss, wv.Rs, wv.Npad, iat, m.pos_new, part + 12, grads);
+    if (J3)
+    {
+      double jp[4] = {0.0, 0.0, 0.0, 0.0};
+      j3_partials(ss, sys, wv, ions, J, iat, m.pos_new, jp);
+      block_sum<4>(jp, m.red, m.sums + 16);
+    }
     block_sum<16>(part, m.red, m.sums);
     if (tid == 0)
     {
@@ -195,6 +205,17 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
           for (int c = 0; c < 3; ++c)
             gn[c] += S[13 + c];
         ratio *= exp((double)wv.Uat[iat] - S[12]);
+      }
+      if (J3)
+      {
+        ms->j3_curUat = S[16];
+        for (int c = 0; c < 3; ++c)
+        {
+          ms->j3_curGrad[c] = S[17 + c];
+          if (grads)
+            gn[c] += S[17 + c];
+        }
+        ratio *= exp((double)wv.j3Uat[iat] - S[16]);
       }
       if (!isfinite(ratio))
         atomicOr(wv.status, DEV_ERR_NONFINITE);
@@ -253,6 +274,8 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
       __syncthreads();
       j2_accept(ss, wv, m, iat);
     }
+    if (J3)
+      j3_accept(ss, sys, wv, m, J, ions, iat);
     break;
   }
   case VERB_PSET_ACCEPT:
@@ -799,6 +822,132 @@ __global__ void __launch_bounds__(256) jastrow_recompute_kernel(const DevSystem*
   }
 }
 
+// ThreeBodyJastrow::recompute (ThreeBodyJastrow.h:222-243, 391-427): the
+// per-ion electron lists in ascending electron order (build_compact_list),
+// then for every electron the sums over all its triples.  The reference
+// walks the triangle k < j and adds the k-side terms back; the functor is
+// symmetric in its two electrons (gamma(l,m,n) = gamma(m,l,n)), so the full
+// sums per electron are the same quantities.  Warp per list, then warp per
+// electron.
+constexpr int J3R_WARPS = 8;
+template <typename T>
+__global__ void __launch_bounds__(256) j3_recompute_kernel(const DevSystem* __restrict__ sys, DevWalkers dw)
+{
+  __shared__ SysSmem<T> ss;
+  __shared__ int s_ion[J3R_WARPS][J3_NEAR];
+  __shared__ T s_r[J3R_WARPS][J3_NEAR], s_d[J3R_WARPS][3][J3_NEAR];
+  __shared__ int s_seg[J3R_WARPS][2 * J3_NEAR + 1];
+  load_sys(sys, ss);
+  const int w = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const WV<T> wv     = make_wv<T>(dw, w);
+  const int N = wv.N, I = ss.n_ions, Np = wv.Npad, cap = wv.j3cap;
+  const T* ions      = (const T*)sys->ion_soa;
+  const T* gam       = (const T*)sys->j3_gamma;
+  const unsigned below = (1u << lane) - 1u;
+  for (int li = wid; li < 2 * I; li += nw)
+  {
+    const int kg = li / I, ion = li % I;
+    const T cut  = ss.j3cut[ion_group(ss, ion)];
+    const int e0 = kg ? ss.n_up : 0, e1 = kg ? N : ss.n_up;
+    int* lst     = wv.j3list + (size_t)li * cap;
+    int c        = 0;
+    for (int j0 = e0; j0 < e1; j0 += 32)
+    {
+      const int j = j0 + lane;
+      bool in     = false;
+      if (j < e1)
+      {
+        T dx, dy, dz;
+        in = j3_ion_dist(ss, ions, ion, wv.Rs[j], wv.Rs[Np + j], wv.Rs[2 * Np + j], cut, dx, dy, dz) < cut;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, in);
+      const int at     = c + __popc(b & below);
+      if (in)
+      {
+        if (at < cap)
+          lst[at] = j;
+        else
+          atomicOr(wv.status, DEV_ERR_CAPACITY);
+      }
+      c += __popc(b);
+    }
+    if (lane == 0)
+      wv.j3cnt[li] = c < cap ? c : cap;
+  }
+  __syncthreads();
+  for (int j = wid; j < N; j += nw)
+  {
+    const T px = wv.Rs[j], py = wv.Rs[Np + j], pz = wv.Rs[2 * Np + j];
+    int nn     = 0;
+    for (int c0 = 0; c0 < I; c0 += 32)
+    {
+      const int c = c0 + lane;
+      bool in     = false;
+      T dx = 0, dy = 0, dz = 0, r = 0;
+      if (c < I)
+      {
+        const T cut = ss.j3cut[ion_group(ss, c)];
+        r           = j3_ion_dist(ss, ions, c, px, py, pz, cut, dx, dy, dz);
+        in          = r < cut;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, in);
+      const int at     = nn + __popc(b & below);
+      if (in)
+      {
+        if (at < J3_NEAR)
+        {
+          s_ion[wid][at]  = c;
+          s_r[wid][at]    = r;
+          s_d[wid][0][at] = dx;
+          s_d[wid][1][at] = dy;
+          s_d[wid][2][at] = dz;
+        }
+        else
+          atomicOr(wv.status, DEV_ERR_CAPACITY);
+      }
+      nn += __popc(b);
+    }
+    nn           = nn < J3_NEAR ? nn : J3_NEAR;
+    const int ns = 2 * nn;
+    __syncwarp();
+    for (int s = lane; s < ns; s += 32)
+      s_seg[wid][s + 1] = wv.j3cnt[(s / nn) * I + s_ion[wid][s % nn]];
+    __syncwarp();
+    if (lane == 0)
+    {
+      s_seg[wid][0] = 0;
+      for (int s = 1; s <= ns; ++s)
+        s_seg[wid][s] += s_seg[wid][s - 1];
+    }
+    __syncwarp();
+    const J3Near<T> nv{nn, s_seg[wid], s_ion[wid], s_r[wid], s_d[wid][0], s_d[wid][1], s_d[wid][2]};
+    const int P = s_seg[wid][ns];
+    double u = 0, g0 = 0, g1 = 0, g2 = 0, l = 0;
+    for (int p = lane; p < P; p += 32)
+    {
+      J3Terms<T> o;
+      if (j3_triple(ss, gam, wv, ions, nv, p, j, px, py, pz, o))
+      {
+        u += (double)o.uj;
+        g0 += (double)o.gj[0];
+        g1 += (double)o.gj[1];
+        g2 += (double)o.gj[2];
+        l += (double)o.lj;
+      }
+    }
+    u = warp_sum(u), g0 = warp_sum(g0), g1 = warp_sum(g1), g2 = warp_sum(g2), l = warp_sum(l);
+    if (lane == 0)
+    {
+      wv.j3Uat[j]          = (T)u;
+      wv.j3dUat[j]         = (T)g0;
+      wv.j3dUat[N + j]     = (T)g1;
+      wv.j3dUat[2 * N + j] = (T)g2;
+      wv.j3d2Uat[j]        = (T)l;
+    }
+    __syncwarp(); // the warp's near-ion arrays are rewritten for its next electron
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) gl_kernel(const DevSystem* __restrict__ sys, DevWalkers dw)
 {
@@ -911,15 +1060,18 @@ cudaError_t launch_verb(bool fp32, const DevSystem* sys, const DevWalkers& dw, c
 {
   if (max_k > MAXK)
     return cudaErrorInvalidValue;
+  // dynamic shared memory: the flush scratch, or the J3 move scratch
+  const size_t b32 = std::max(flush_smem_bytes<float>(), sizeof(J3Smem<float>));
+  const size_t b64 = std::max(flush_smem_bytes<double>(), sizeof(J3Smem<double>));
   if (fp32)
   {
-    allow_smem(verb_kernel<float>, flush_smem_bytes<float>());
-    verb_kernel<float><<<dw.W, threads, flush_smem_bytes<float>(), st>>>(sys, dw, a);
+    allow_smem(verb_kernel<float>, b32);
+    verb_kernel<float><<<dw.W, threads, b32, st>>>(sys, dw, a);
   }
   else
   {
-    allow_smem(verb_kernel<double>, flush_smem_bytes<double>());
-    verb_kernel<double><<<dw.W, threads, flush_smem_bytes<double>(), st>>>(sys, dw, a);
+    allow_smem(verb_kernel<double>, b64);
+    verb_kernel<double><<<dw.W, threads, b64, st>>>(sys, dw, a);
   }
   return cudaGetLastError();
 }
@@ -977,6 +1129,17 @@ cudaError_t launch_jastrow_recompute(bool fp32, const DevSystem* sys, const DevW
     jastrow_recompute_kernel<float><<<dw.W, threads, 0, st>>>(sys, dw);
   else
     jastrow_recompute_kernel<double><<<dw.W, threads, 0, st>>>(sys, dw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_j3_recompute(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads,
+                                cudaStream_t st)
+{
+  (void)threads; // one warp per list / electron, J3R_WARPS warps
+  if (fp32)
+    j3_recompute_kernel<float><<<dw.W, 32 * J3R_WARPS, 0, st>>>(sys, dw);
+  else
+    j3_recompute_kernel<double><<<dw.W, 32 * J3R_WARPS, 0, st>>>(sys, dw);
   return cudaGetLastError();
 }
 

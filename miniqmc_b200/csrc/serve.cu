@@ -34,7 +34,7 @@ struct TaskList
 {
   SweepTask* d = nullptr;
   int cap = 0, n = 0, blocks = 0, threads = 64, max_npad = 0, max_k = 0;
-  bool fp32 = true, tc = false;
+  bool fp32 = true, tc = false, j3 = false;
 
   ~TaskList() { cudaFree(d); }
 
@@ -51,7 +51,7 @@ struct TaskList
       cap = n;
     }
     std::vector<SweepTask> h;
-    blocks = 0, max_npad = 0, max_k = 0, tc = false;
+    blocks = 0, max_npad = 0, max_k = 0, tc = false, j3 = false;
     threads = launch_threads;
     double inflight = 0;
     for (auto* w : batches)
@@ -64,6 +64,7 @@ struct TaskList
       max_k    = std::max(max_k, w->dw.k);
       inflight += (double)w->dw.W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8);
       fp32 = w->fp32;
+      j3   = j3 || (w->sys->h.comp & QMC_WF_J3) != 0;
       h.push_back(t);
     }
     // the next-move L2 prefetch only while all walkers' stencils fit well
@@ -76,7 +77,7 @@ struct TaskList
 
   cudaError_t launch(int n_substeps, double accept, cudaStream_t st) const
   {
-    return launch_sweep(fp32, d, n, blocks, n_substeps, accept, threads, max_npad, max_k, st, tc);
+    return launch_sweep(fp32, d, n, blocks, n_substeps, accept, threads, max_npad, max_k, st, tc, j3);
   }
 };
 

@@ -44,15 +44,25 @@ std::vector<Field> state_fields(qmc_walkers* w)
 {
   const DevWalkers& d = w->dw;
   const size_t W = d.W, N = d.N, Np = d.Npad, n = d.n, np = d.npad, k = d.k, es = w->fp32 ? 4 : 8;
-  return {{d.R, W * N * 3 * 8},         {d.Rs, W * 3 * Np * es},        {d.Ainv, W * 2 * n * np * es},
+  std::vector<Field> f = {{d.R, W * N * 3 * 8},         {d.Rs, W * 3 * Np * es},        {d.Ainv, W * 2 * n * np * es},
           {d.dpsiM, W * 6 * n * np * es}, {d.d2psiM, W * 2 * n * np * es}, {d.U, W * 2 * k * np * es},
           {d.V, W * 2 * k * np * es},    {d.Binv, W * 2 * k * k * 8},    {d.delay_list, W * 2 * k * 4},
           {d.delay_count, W * 2 * 4},    {d.det_log, W * 2 * 8},         {d.det_phase, W * 2 * 8},
           {d.j1_Vat, W * N * es},        {d.j1_Lap, W * N * es},         {d.j1_Grad, W * 3 * N * es},
           {d.j2_Uat, W * N * es},        {d.j2_d2Uat, W * N * es},       {d.j2_dUat, W * 3 * N * es},
-          {d.j_log, W * 2 * 8},          {d.mt, W * (MT_N + 1) * 4},     {d.ms, W * sizeof(MoveState)},
+          {d.j_log, W * 3 * 8},          {d.mt, W * (MT_N + 1) * 4},     {d.ms, W * sizeof(MoveState)},
           {d.G, W * N * 3 * 8},          {d.L, W * N * 8},               {d.logpsi, W * 8},
           {d.accepted, W * 8}};
+  if (d.j3_cnt)
+  {
+    const size_t I = d.I;
+    f.push_back({d.j3_Uat, W * N * es});
+    f.push_back({d.j3_d2Uat, W * N * es});
+    f.push_back({d.j3_dUat, W * 3 * N * es});
+    f.push_back({d.j3_cnt, W * 2 * I * 4});
+    f.push_back({d.j3_list, W * 2 * I * d.j3_cap * 4});
+  }
+  return f;
 }
 
 struct Header
@@ -67,7 +77,7 @@ Header make_header(qmc_walkers* w)
 {
   Header h{};
   std::memcpy(h.magic, "QMCWALK", 8);
-  h.version = 1, h.W = w->dw.W, h.N = w->dw.N, h.n = w->dw.n, h.npad = w->dw.npad, h.k = w->dw.k;
+  h.version = 2, h.W = w->dw.W, h.N = w->dw.N, h.n = w->dw.n, h.npad = w->dw.npad, h.k = w->dw.k;
   h.fp32 = w->fp32 ? 1 : 0;
   h.steps_done = w->steps_done, h.nlpp_calls = w->nlpp_calls;
   h.payload = 0;
@@ -129,7 +139,7 @@ int qmc_walkers_restore(qmc_walkers* w, const void* buffer, size_t bytes)
   Header h;
   std::memcpy(&h, buffer, sizeof(h));
   const Header mine = make_header(w);
-  if (std::memcmp(h.magic, "QMCWALK", 8) || h.version != 1 || h.W != mine.W || h.N != mine.N || h.n != mine.n ||
+  if (std::memcmp(h.magic, "QMCWALK", 8) || h.version != 2 || h.W != mine.W || h.N != mine.N || h.n != mine.n ||
       h.npad != mine.npad || h.k != mine.k || h.fp32 != mine.fp32 || h.payload != mine.payload ||
       bytes < sizeof(Header) + h.payload)
     return fail(QMC_ERR_ARG, "checkpoint does not match this batch (system, walkers, delay rank, precision)");

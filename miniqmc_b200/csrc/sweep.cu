@@ -12,7 +12,7 @@
 
 namespace qmc
 {
-template <typename T>
+template <typename T, bool HAS_J3>
 __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restrict__ tasks, int n_tasks, int n_substeps,
                                                     double accept_thr, int tc)
 {
@@ -34,7 +34,8 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   const T* ions = (const T*)sys->ion_soa;
   long long acc = 0;
   const bool DET = ss.comp & QMC_WF_DET;
-  // dynamic shared memory: [Binv of the active spin (k x k FP64)][flush scratch]
+  // dynamic shared memory: [Binv of the active spin (k x k FP64)][flush
+  // scratch, or the J3 move scratch between flushes]
   const int k = wv.k;
   T* smem     = reinterpret_cast<T*>(dyn + bsm_bytes(k));
   auto load_binv = [&](int spin) {
@@ -86,8 +87,8 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
         load_binv(1);
       }
       double* tr = task.trace ? task.trace + (((size_t)w * n_substeps + l) * N + iel) * 8 : nullptr;
-      do_move(ss, sys, wv, m, sp, ions, iel, accept_thr, urp[iel], dp + 3 * iel, tr, smem,
-              task.prefetch && iel + 1 < N);
+      do_move<T, HAS_J3>(ss, sys, wv, m, sp, ions, iel, accept_thr, urp[iel], dp + 3 * iel, tr, smem,
+                         task.prefetch && iel + 1 < N);
       acc += m.accept ? 1 : 0;
       __syncthreads(); // m.accept is rewritten by the next move
       if (m.tc_abort)
@@ -115,18 +116,33 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   }
 }
 
-template <typename T> static void set_smem_attr(size_t bytes)
+template <typename T, bool HAS_J3> static void set_smem_attr(size_t bytes)
 {
   static size_t done = 0;
   if (bytes > done)
   {
-    cudaFuncSetAttribute(sweep_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sweep_kernel<T, HAS_J3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     done = bytes;
+  }
+}
+template <typename T>
+static void launch_sweep_t(bool j3, size_t bytes, const SweepTask* d_tasks, int n_tasks, int total_blocks,
+                           int n_substeps, double accept, int threads, cudaStream_t st, int tc)
+{
+  if (j3)
+  {
+    set_smem_attr<T, true>(bytes);
+    sweep_kernel<T, true><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
+  }
+  else
+  {
+    set_smem_attr<T, false>(bytes);
+    sweep_kernel<T, false><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
   }
 }
 
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
-                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc)
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3)
 {
   (void)max_npad;
   if (max_k > MAXK || (tc && (!fp32 || threads < 128))) // a task flushes on the tensor cores only if its k <= 32
@@ -136,14 +152,16 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
     size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<float>(threads, max_k);
     if (tc && tc_flush_smem_bytes() > bytes)
       bytes = tc_flush_smem_bytes(); // the tiles overlay the cached Binv
-    set_smem_attr<float>(bytes);
-    sweep_kernel<float><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc ? 1 : 0);
+    if (j3)
+      bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<float>));
+    launch_sweep_t<float>(j3, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, tc ? 1 : 0);
   }
   else
   {
-    const size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<double>(threads, max_k);
-    set_smem_attr<double>(bytes);
-    sweep_kernel<double><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, 0);
+    size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<double>(threads, max_k);
+    if (j3)
+      bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<double>));
+    launch_sweep_t<double>(j3, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, 0);
   }
   return cudaGetLastError();
 }

@@ -151,6 +151,70 @@ int oracle_nio_jastrows(const double* lattice, qmc_functor* j1_O, qmc_functor* j
   return 0;
 }
 
+// PolynomialFunctor3D::reset_gamma (PolynomialFunctor3D.h:113-250)
+int oracle_j3_functor_setup(double rcut, const double* params, qmc_j3_functor* out)
+{
+  J3Func f;
+  f.setup(rcut, params);
+  out->cutoff = f.cutoff_radius;
+  for (int l = 0; l < 4; ++l)
+    for (int m = 0; m < 4; ++m)
+      for (int n = 0; n < 4; ++n)
+        out->gamma[16 * l + 4 * m + n] = f.gamma[l][m][n];
+  return 0;
+}
+static J3Func to_j3(const qmc_j3_functor& q)
+{
+  J3Func f;
+  f.cutoff_radius = q.cutoff;
+  for (int l = 0; l < 4; ++l)
+    for (int m = 0; m < 4; ++m)
+      for (int n = 0; n < 4; ++n)
+        f.gamma[l][m][n] = q.gamma[16 * l + 4 * m + n];
+  return f;
+}
+// PolynomialFunctor3D::evaluate(r12, r1I, r2I, grad, hess): out = value,
+// grad[3], hess 00 01 02 11 12 22
+int oracle_j3_functor_eval(const qmc_j3_functor* q, double r12, double r1I, double r2I, double* out10)
+{
+  const J3Func f = to_j3(*q);
+  out10[0]       = f.eval(r12, r1I, r2I, out10 + 1, out10 + 4);
+  return 0;
+}
+// buildJeeI (nio.hpp:171-245)
+int oracle_nio_j3(const double* lattice, qmc_j3_functor* same, qmc_j3_functor* diff)
+{
+  Lattice L(lattice);
+  const double rcut = std::min(L.WignerSeitzRadius, 4.8261684030);
+  static const double Y[4][QMC_J3_PARAMS] = {
+      {-0.003356164484, 0.002412623253, 0.01653623839, 0.0008341346169, -0.002808360734, 0.000710697475,
+       0.01076942152, 0.0009228283355, 0.01576022161, -0.003585259096, 0.003323106938, -0.02282975998,
+       -0.002246144403, -0.007196992871, -0.00404316239, 0.001465337212, 0.02026982926, -0.03528735393,
+       0.04594087928, -0.008776410679, -0.001552528476, -0.005554407743, 0.001858594451, 0.002001634408,
+       0.0009302256139, -0.0006304447229},
+      {-0.006861627197, 0.003278047306, 0.03324006545, 0.003097361067, -0.004710623571, 9.652180317e-06,
+       0.02212708787, -0.003718893286, 0.03390124932, -0.00710566395, 0.008807743592, -0.04281661568,
+       -0.008463011294, -0.01269994613, -0.002005229447, 0.002186590944, 0.03350196472, -0.05677253817,
+       0.07810604648, -0.009629896208, -0.006372643712, -0.01056861605, 0.002485188615, 0.008392442289,
+       1.073423014e-05, -0.0004812466328},
+      {-0.003775082438, -0.00169971229, 0.02162925441, 0.005674020544, -0.0008296047161, 0.00128057705,
+       0.005487203215, 0.001637322446, 0.02976838198, -0.0003207100945, 0.01143855436, -0.05336741304,
+       -0.00732359381, -0.01556942626, 0.0001149478453, 0.001838601199, 0.02570154203, -0.0675325214,
+       0.1080671614, -0.01258358969, 0.001839834045, -0.02422400426, 0.005154953014, 0.003510582598,
+       0.007464427016, -0.002454817757},
+      {-0.009590393593, 0.002498010871, 0.04225872633, 0.00460311261, -0.01071033503, 0.001253155062,
+       0.02934351285, -0.01823794726, 0.07224890393, -0.01020046849, 0.006310807929, -0.05655009412,
+       -0.0363775247, 0.002062411388, 0.02037856173, 0.003372676617, 0.03915277249, -0.02680556816,
+       0.08648136635, 0.01499088063, -0.02231984329, -0.02399792096, 0.001105720128, 0.02196005181,
+       0.003162638982, -0.00119645772}};
+  for (int s = 0; s < 2; ++s)
+  {
+    oracle_j3_functor_setup(rcut, Y[2 * s], same + s);
+    oracle_j3_functor_setup(rcut, Y[2 * s + 1], diff + s);
+  }
+  return 0;
+}
+
 // -------------------------------------------------------------- system --
 int oracle_system_create(const qmc_system_desc* d, int precision, oracle_system** out)
 {
@@ -198,6 +262,13 @@ int oracle_system_create(const qmc_system_desc* d, int precision, oracle_system*
   s.use_det  = (comp & QMC_WF_DET) != 0;
   s.use_j1   = (comp & QMC_WF_J1) != 0;
   s.use_j2   = (comp & QMC_WF_J2) != 0;
+  s.use_j3   = (comp & QMC_WF_J3) != 0;
+  if (s.use_j3)
+    for (int g = 0; g < s.n_groups; ++g)
+    {
+      s.j3_same.push_back(to_j3(d->j3_same[g]));
+      s.j3_diff.push_back(to_j3(d->j3_diff[g]));
+    }
   for (int g = 0; g < s.n_groups; ++g)
     s.j1.push_back(to_functor(d->j1[g]));
   s.j2_uu = to_functor(d->j2_uu);
@@ -409,12 +480,13 @@ int oracle_wf_components(oracle_walkers* o, double* comp)
   for (int i = 0; i < o->W; ++i)
   {
     const Walker& w = o->w[i];
-    comp[6 * i + 0] = w.det[0].LogValue;
-    comp[6 * i + 1] = w.det[1].LogValue;
-    comp[6 * i + 2] = w.det[0].PhaseValue;
-    comp[6 * i + 3] = w.det[1].PhaseValue;
-    comp[6 * i + 4] = w.j1_LogValue;
-    comp[6 * i + 5] = w.j2_LogValue;
+    comp[7 * i + 0] = w.det[0].LogValue;
+    comp[7 * i + 1] = w.det[1].LogValue;
+    comp[7 * i + 2] = w.det[0].PhaseValue;
+    comp[7 * i + 3] = w.det[1].PhaseValue;
+    comp[7 * i + 4] = w.j1_LogValue;
+    comp[7 * i + 5] = w.j2_LogValue;
+    comp[7 * i + 6] = w.j3_LogValue;
   }
   return 0;
 }

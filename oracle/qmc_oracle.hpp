@@ -969,6 +969,186 @@ struct DelayedUpdate
   }
 };
 
+// -------------------------------------------------- PolynomialFunctor3D --
+// The eeI functor of the three-body Jastrow (PolynomialFunctor3D.h:38-560)
+// with N_eI = N_ee = 3 and C = 3: the gamma(l, m, n) coefficients follow
+// from the free parameters through the e-e and e-I no-cusp constraints
+// (resize: the constraint matrix and its row reduction; reset_gamma).
+struct J3Func
+{
+  static constexpr int NeI = 3, Nee = 3, C = 3;
+  double cutoff_radius = 0.0;
+  double gamma[NeI + 1][NeI + 1][Nee + 1] = {};
+
+  void setup(double rcut, const double* params)
+  {
+    cutoff_radius   = rcut;
+    const double L  = 0.5 * rcut;
+    const int NumGamma = (NeI + 1) * (NeI + 2) / 2 * (Nee + 1);
+    const int NumC     = (2 * NeI + 1) + (NeI + Nee + 1);
+    int index[NeI + 1][NeI + 1][Nee + 1];
+    int num = 0;
+    for (int m = 0; m <= NeI; m++)
+      for (int l = m; l <= NeI; l++)
+        for (int n = 0; n <= Nee; n++)
+          index[l][m][n] = index[m][l][n] = num++;
+    std::vector<double> A((size_t)NumC * NumGamma, 0.0);
+    auto a = [&](int r, int c) -> double& { return A[(size_t)r * NumGamma + c]; };
+    int k;
+    for (k = 0; k <= 2 * NeI; k++)
+      for (int m = 0; m <= k; m++)
+      {
+        const int l = k - m;
+        if (l <= NeI && m <= NeI)
+        {
+          const int i = index[l][m][1];
+          if (l > m)
+            a(k, i) = 2.0;
+          else if (l == m)
+            a(k, i) = 1.0;
+        }
+      }
+    for (int kp = 0; kp <= NeI + Nee; kp++)
+    {
+      if (kp <= Nee)
+      {
+        a(k + kp, index[0][0][kp]) = (double)C;
+        a(k + kp, index[0][1][kp]) = -L;
+      }
+      for (int l = 1; l <= kp; l++)
+      {
+        const int n = kp - l;
+        if (n >= 0 && n <= Nee && l <= NeI)
+        {
+          a(k + kp, index[l][0][n]) = (double)C;
+          a(k + kp, index[l][1][n]) = -L;
+        }
+      }
+    }
+    // row reduction with the reference's column scan and row pivoting
+    std::vector<bool> indep(NumGamma, false);
+    int col = -1;
+    for (int row = 0; row < NumC; row++)
+    {
+      int max_loc;
+      double max_abs;
+      do
+      {
+        col++;
+        max_loc = row;
+        max_abs = std::abs(a(row, col));
+        for (int ri = row + 1; ri < NumC; ri++)
+          if (std::abs(a(ri, col)) > max_abs)
+          {
+            max_loc = ri;
+            max_abs = std::abs(a(ri, col));
+          }
+        if (max_abs < 1.0e-6)
+          indep[col] = true;
+      } while (max_abs < 1.0e-6);
+      for (int c = 0; c < NumGamma; c++)
+        std::swap(a(row, c), a(max_loc, c));
+      const double lead_inv = 1.0 / a(row, col);
+      for (int c = 0; c < NumGamma; c++)
+        a(row, c) *= lead_inv;
+      for (int ri = 0; ri < NumC; ri++)
+        if (ri != row)
+        {
+          const double val = a(ri, col);
+          for (int c = 0; c < NumGamma; c++)
+            a(ri, c) -= val * a(row, c);
+        }
+    }
+    for (int c = col + 1; c < NumGamma; c++)
+      indep[c] = true;
+    std::vector<double> g(NumGamma, 0.0);
+    int var = 0;
+    for (int i = 0; i < NumGamma; i++)
+      if (indep[i])
+        g[i] = params[var++];
+    var = 0;
+    for (int i = 0; i < NumGamma; i++)
+      if (!indep[i])
+      {
+        for (int j = 0; j < NumGamma; j++)
+          if (i != j)
+            g[i] -= a(var, j) * g[j];
+        var++;
+      }
+    num = 0;
+    for (int m = 0; m <= NeI; m++)
+      for (int l = m; l <= NeI; l++)
+        for (int n = 0; n <= Nee; n++)
+          gamma[m][l][n] = gamma[l][m][n] = g[num++];
+  }
+  // value, grad (d/dr_12, d/dr_1I, d/dr_2I) and the Hessian entries (00, 01,
+  // 02, 11, 12, 22) (PolynomialFunctor3D::evaluate with derivatives)
+  double eval(double r12, double r1I, double r2I, double* gr, double* h) const
+  {
+    const double L = 0.5 * cutoff_radius;
+    for (int i = 0; i < 3; ++i)
+      gr[i] = 0.0;
+    for (int i = 0; i < 6; ++i)
+      h[i] = 0.0;
+    if (r1I >= L || r2I >= L)
+      return 0.0;
+    double val = 0.0, g0 = 0, g1 = 0, g2 = 0, h00 = 0, h01 = 0, h02 = 0, h11 = 0, h12 = 0, h22 = 0;
+    double r2l = 1, r2l_1 = 0, r2l_2 = 0, lf = 0;
+    for (int l = 0; l <= NeI; l++)
+    {
+      double r2m = 1, r2m_1 = 0, r2m_2 = 0, mf = 0;
+      for (int m = 0; m <= NeI; m++)
+      {
+        double r2n = 1, r2n_1 = 0, r2n_2 = 0, nf = 0;
+        for (int n = 0; n <= Nee; n++)
+        {
+          const double gg = gamma[l][m][n];
+          const double g00x = gg * r2l * r2m, g10x = gg * r2l_1 * r2m, g01x = gg * r2l * r2m_1, gxx0 = gg * r2n;
+          val += g00x * r2n;
+          g0 += g00x * r2n_1;
+          g1 += g10x * r2n;
+          g2 += g01x * r2n;
+          h00 += g00x * r2n_2;
+          h01 += g10x * r2n_1;
+          h02 += g01x * r2n_1;
+          h11 += gxx0 * r2l_2 * r2m;
+          h12 += gxx0 * r2l_1 * r2m_1;
+          h22 += gxx0 * r2l * r2m_2;
+          nf += 1;
+          r2n_2 = r2n_1 * nf;
+          r2n_1 = r2n * nf;
+          r2n *= r12;
+        }
+        mf += 1;
+        r2m_2 = r2m_1 * mf;
+        r2m_1 = r2m * mf;
+        r2m *= r2I;
+      }
+      lf += 1;
+      r2l_2 = r2l_1 * lf;
+      r2l_1 = r2l * lf;
+      r2l *= r1I;
+    }
+    const double a2 = r2I - L, a1 = r1I - L, b = a2 * a1;
+    for (int i = 0; i < C; i++)
+    {
+      h00 = b * h00;
+      h01 = b * h01 + a2 * g0;
+      h02 = b * h02 + a1 * g0;
+      h11 = b * h11 + 2.0 * a2 * g1;
+      h12 = b * h12 + a1 * g1 + a2 * g2 + val;
+      h22 = b * h22 + 2.0 * a1 * g2;
+      g0  = b * g0;
+      g1  = b * g1 + a2 * val;
+      g2  = b * g2 + a1 * val;
+      val *= b;
+    }
+    gr[0] = g0, gr[1] = g1, gr[2] = g2;
+    h[0] = h00, h[1] = h01, h[2] = h02, h[3] = h11, h[4] = h12, h[5] = h22;
+    return val;
+  }
+};
+
 // ------------------------------------------------------------ System ---
 struct System
 {
@@ -980,9 +1160,10 @@ struct System
   std::vector<int> group_first, group_last;
   Spline spline;
   int lap_mode = 0;
-  bool use_det = true, use_j1 = true, use_j2 = true;
+  bool use_det = true, use_j1 = true, use_j2 = true, use_j3 = false;
   std::vector<Functor> j1; // per ion group
   Functor j2_uu, j2_ud;
+  std::vector<J3Func> j3_same, j3_diff; // per ion group: same-spin and opposite-spin electron pairs
 };
 
 // NonLocalPP's 12-point sphere (NonLocalPP.hpp:61-80) rotated by
@@ -1100,6 +1281,8 @@ struct Walker
       v->assign(N, 0.0);
     G.assign((size_t)N * 3, 0.0);
     L.assign(N, 0.0);
+    if (s->use_j3)
+      j3_init();
   }
 
   // build_els (ParticleSet_builder.cpp:33-53): 3N uniforms in lattice units
@@ -1503,6 +1686,362 @@ struct Walker
     j2_LogValue = -0.5 * s;
   }
 
+  // ---- three-body Jastrow (ThreeBodyJastrow.h:30-677) ----
+  std::vector<double> j3_Uat, j3_dUat, j3_d2Uat;                         // dUat [N][3]
+  std::vector<double> j3_newUk, j3_newdUk, j3_newd2Uk, j3_oldUk, j3_olddUk, j3_oldd2Uk;
+  double j3_cur_Uat = 0, j3_cur_d2Uat = 0, j3_LogValue = 0;
+  Vec3 j3_cur_dUat{0, 0, 0};
+  bool j3_partial = false;
+  std::vector<double> j3_cut;                    // [I] half the functor cutoff
+  std::vector<std::vector<int>> j3_in;           // [eg * I + ion] elecs_inside
+  std::vector<std::vector<double>> j3_in_d;      // their e-I distances
+  std::vector<std::vector<Vec3>> j3_in_dx;       // their e-I displacements
+  std::vector<double> c_jk, c_jI, c_kI;          // compressed pair lists
+  std::vector<Vec3> c_djk, c_djI, c_dkI;
+  std::vector<int> c_idx;
+  std::vector<double> j3_r, j3_dx, j3_dy, j3_dz; // e-I row scratch
+
+  const J3Func& j3f(int ig, int jg, int kg) const { return jg == kg ? sys->j3_same[ig] : sys->j3_diff[ig]; }
+  void j3_init()
+  {
+    const int N = sys->n_elec, I = sys->n_ions;
+    for (auto* v : {&j3_Uat, &j3_d2Uat, &j3_newUk, &j3_newd2Uk, &j3_oldUk, &j3_oldd2Uk})
+      v->assign(N, 0.0);
+    for (auto* v : {&j3_dUat, &j3_newdUk, &j3_olddUk})
+      v->assign((size_t)N * 3, 0.0);
+    j3_cut.assign(I, 0.0);
+    for (int i = 0; i < I; ++i)
+      j3_cut[i] = 0.5 * sys->j3_same[sys->ion_group[i]].cutoff_radius;
+    j3_in.assign(2 * I, {});
+    j3_in_d.assign(2 * I, {});
+    j3_in_dx.assign(2 * I, {});
+    for (auto* v : {&c_jk, &c_jI, &c_kI})
+      v->assign(N, 0.0);
+    for (auto* v : {&c_djk, &c_djI, &c_dkI})
+      v->assign(N, Vec3{0, 0, 0});
+    c_idx.assign(N, 0);
+    for (auto* v : {&j3_r, &j3_dx, &j3_dy, &j3_dz})
+      v->assign(I, 0.0);
+  }
+  // build_compact_list (ThreeBodyJastrow.h:222-243)
+  void j3_build_lists()
+  {
+    const int N = sys->n_elec, I = sys->n_ions;
+    for (auto& v : j3_in)
+      v.clear();
+    for (auto& v : j3_in_d)
+      v.clear();
+    for (auto& v : j3_in_dx)
+      v.clear();
+    for (int jel = 0; jel < N; ++jel)
+    {
+      const int jg = egroup(jel);
+      ab_row(pos(jel), j3_r.data(), j3_dx.data(), j3_dy.data(), j3_dz.data());
+      for (int iat = 0; iat < I; ++iat)
+        if (j3_r[iat] < j3_cut[iat])
+        {
+          j3_in[jg * I + iat].push_back(jel);
+          j3_in_d[jg * I + iat].push_back(j3_r[iat]);
+          j3_in_dx[jg * I + iat].push_back(Vec3{j3_dx[iat], j3_dy[iat], j3_dz[iat]});
+        }
+    }
+  }
+  // computeU3_engine (ThreeBodyJastrow.h:484-580): evaluateVGL of the
+  // compressed pairs, then the contributions to jel and to every kel
+  void j3_engine(const J3Func& f, int cnt, double& Uj, Vec3& dUj, double& d2Uj, double* Uk, double* dUk, double* d2Uk)
+  {
+    std::vector<double> val(cnt), g0(cnt), g1(cnt), g2(cnt), h00(cnt), h11(cnt), h22(cnt), h01(cnt), h02(cnt);
+    for (int p = 0; p < cnt; ++p)
+    {
+      double gr[3], h[6];
+      val[p] = f.eval(c_jk[p], c_jI[p], c_kI[p], gr, h);
+      g0[p]  = gr[0] / c_jk[p];
+      g1[p]  = gr[1] / c_jI[p];
+      g2[p]  = gr[2] / c_kI[p];
+      h00[p] = h[0];
+      h11[p] = h[3];
+      h22[p] = h[5];
+      h01[p] = h[1] / (c_jk[p] * c_jI[p]);
+      h02[p] = h[2] / (c_jk[p] * c_kI[p]);
+    }
+    double s_g0 = 0, s_g1 = 0, s_h00 = 0, s_h11 = 0;
+    for (int p = 0; p < cnt; ++p)
+      Uj += val[p];
+    for (int p = 0; p < cnt; ++p)
+      s_g0 += g0[p];
+    for (int p = 0; p < cnt; ++p)
+      s_g1 += g1[p];
+    for (int p = 0; p < cnt; ++p)
+      s_h00 += h00[p];
+    for (int p = 0; p < cnt; ++p)
+      s_h11 += h11[p];
+    d2Uj -= s_h00 + s_h11 + 2.0 * (s_g0 + s_g1);
+    std::fill(h11.begin(), h11.end(), 0.0);
+    for (int d = 0; d < 3; ++d)
+    {
+      double dx = 0.0;
+      for (int p = 0; p < cnt; ++p)
+      {
+        h11[p] += c_dkI[p][d] * c_djk[p][d];
+        dx += g1[p] * c_djI[p][d];
+        const double temp = c_djk[p][d] * g0[p];
+        dx += temp;
+        c_djk[p][d] *= c_djI[p][d];
+        c_dkI[p][d] = c_dkI[p][d] * g2[p] - temp;
+      }
+      dUj[d] += dx;
+      if (d > 0)
+        for (int p = 0; p < cnt; ++p)
+          c_djk[p][0] += c_djk[p][d];
+      for (int p = 0; p < cnt; ++p)
+        dUk[3 * c_idx[p] + d] += c_dkI[p][d];
+    }
+    double sum = 0.0;
+    for (int p = 0; p < cnt; ++p)
+      sum += h01[p] * c_djk[p][0];
+    d2Uj -= 2.0 * sum;
+    for (int p = 0; p < cnt; ++p)
+      h00[p] = h00[p] + h22[p] + 2.0 * (g0[p] + g2[p]) - 2.0 * h02[p] * h11[p];
+    for (int p = 0; p < cnt; ++p)
+    {
+      Uk[c_idx[p]] += val[p];
+      d2Uk[c_idx[p]] -= h00[p];
+    }
+  }
+  // computeU3 (ThreeBodyJastrow.h:582-654)
+  void j3_computeU3(int jel, const double* rI, const double* dxI, const double* dyI, const double* dzI,
+                    const double* rk, const double* dxk, const double* dyk, const double* dzk, double& Uj, Vec3& dUj,
+                    double& d2Uj, double* Uk, double* dUk, double* d2Uk, bool triangle)
+  {
+    const int N = sys->n_elec, I = sys->n_ions;
+    Uj = 0.0, dUj = Vec3{0, 0, 0}, d2Uj = 0.0;
+    const int jg = egroup(jel), kelmax = triangle ? jel : N;
+    std::fill_n(Uk, kelmax, 0.0);
+    std::fill_n(d2Uk, kelmax, 0.0);
+    std::fill_n(dUk, 3 * (size_t)kelmax, 0.0);
+    std::vector<int> near;
+    for (int iat = 0; iat < I; ++iat)
+      if (rI[iat] < j3_cut[iat])
+        near.push_back(iat);
+    for (int kg = 0; kg < 2; ++kg)
+    {
+      int cnt = 0;
+      for (size_t ii = 0; ii < near.size(); ++ii)
+      {
+        const int iat = near[ii], ig = sys->ion_group[iat];
+        const Vec3 djI{dxI[iat], dyI[iat], dzI[iat]};
+        const auto& lst = j3_in[kg * I + iat];
+        for (size_t kk = 0; kk < lst.size(); ++kk)
+        {
+          const int kel = lst[kk];
+          if (kel < kelmax && kel != jel)
+          {
+            c_kI[cnt]  = j3_in_d[kg * I + iat][kk];
+            c_jI[cnt]  = rI[iat];
+            c_jk[cnt]  = rk[kel];
+            c_dkI[cnt] = j3_in_dx[kg * I + iat][kk];
+            c_djI[cnt] = djI;
+            c_djk[cnt] = Vec3{dxk[kel], dyk[kel], dzk[kel]};
+            c_idx[cnt] = kel;
+            if (++cnt == N)
+            {
+              j3_engine(j3f(ig, jg, kg), cnt, Uj, dUj, d2Uj, Uk, dUk, d2Uk);
+              cnt = 0;
+            }
+          }
+        }
+        if ((ii + 1 == near.size() || ig != sys->ion_group[near[ii + 1]]) && cnt > 0)
+        {
+          j3_engine(j3f(ig, jg, kg), cnt, Uj, dUj, d2Uj, Uk, dUk, d2Uk);
+          cnt = 0;
+        }
+      }
+    }
+  }
+  // computeU (ThreeBodyJastrow.h:429-482): the value only
+  double j3_computeU(int jel, const double* rI, const double* rk)
+  {
+    const int I = sys->n_ions, N = sys->n_elec, jg = egroup(jel);
+    std::vector<int> near;
+    for (int iat = 0; iat < I; ++iat)
+      if (rI[iat] < j3_cut[iat])
+        near.push_back(iat);
+    double Uj = 0.0;
+    auto evalV = [&](const J3Func& f, int cnt) {
+      const double L = 0.5 * f.cutoff_radius;
+      double tot     = 0.0;
+      for (int p = 0; p < cnt; ++p)
+      {
+        double val = 0.0, r2l = 1.0;
+        for (int l = 0; l <= J3Func::NeI; l++)
+        {
+          double r2m = r2l;
+          for (int m = 0; m <= J3Func::NeI; m++)
+          {
+            double r2n = r2m;
+            for (int n = 0; n <= J3Func::Nee; n++)
+            {
+              val += f.gamma[l][m][n] * r2n;
+              r2n *= c_jk[p];
+            }
+            r2m *= c_kI[p];
+          }
+          r2l *= c_jI[p];
+        }
+        const double b = (c_kI[p] - L) * (c_jI[p] - L);
+        for (int i = 0; i < J3Func::C; i++)
+          val *= b;
+        tot += val;
+      }
+      return tot;
+    };
+    for (int kg = 0; kg < 2; ++kg)
+    {
+      int cnt = 0;
+      for (size_t ii = 0; ii < near.size(); ++ii)
+      {
+        const int iat = near[ii], ig = sys->ion_group[iat];
+        const auto& lst = j3_in[kg * I + iat];
+        for (size_t kk = 0; kk < lst.size(); ++kk)
+        {
+          const int kel = lst[kk];
+          if (kel != jel)
+          {
+            c_kI[cnt] = j3_in_d[kg * I + iat][kk];
+            c_jk[cnt] = rk[kel];
+            c_jI[cnt] = rI[iat];
+            if (++cnt == N)
+            {
+              Uj += evalV(j3f(ig, jg, kg), cnt);
+              cnt = 0;
+            }
+          }
+        }
+        if ((ii + 1 == near.size() || ig != sys->ion_group[near[ii + 1]]) && cnt > 0)
+        {
+          Uj += evalV(j3f(ig, jg, kg), cnt);
+          cnt = 0;
+        }
+      }
+    }
+    return Uj;
+  }
+  // recompute (ThreeBodyJastrow.h:391-427)
+  void j3_recompute()
+  {
+    const int N = sys->n_elec;
+    j3_build_lists();
+    for (int jel = 0; jel < N; ++jel)
+    {
+      ab_row(pos(jel), j3_r.data(), j3_dx.data(), j3_dy.data(), j3_dz.data());
+      aa_row_current(jel);
+      Vec3 dU;
+      j3_computeU3(jel, j3_r.data(), j3_dx.data(), j3_dy.data(), j3_dz.data(), row_r.data(), row_dx.data(),
+                   row_dy.data(), row_dz.data(), j3_Uat[jel], dU, j3_d2Uat[jel], j3_newUk.data(), j3_newdUk.data(),
+                   j3_newd2Uk.data(), true);
+      for (int c = 0; c < 3; ++c)
+        j3_dUat[3 * jel + c] = dU[c];
+      for (int kel = 0; kel < jel; kel++)
+      {
+        j3_Uat[kel] += j3_newUk[kel];
+        j3_d2Uat[kel] += j3_newd2Uk[kel];
+      }
+      for (int c = 0; c < 3; ++c)
+        for (int kel = 0; kel < jel; kel++)
+          j3_dUat[3 * kel + c] += j3_newdUk[3 * kel + c];
+    }
+  }
+  void j3_GL()
+  {
+    const int N = sys->n_elec;
+    double s    = 0.0;
+    for (int i = 0; i < N; ++i)
+    {
+      s += j3_Uat[i];
+      for (int c = 0; c < 3; ++c)
+        G[3 * i + c] += j3_dUat[3 * i + c];
+      L[i] += j3_d2Uat[i];
+    }
+    j3_LogValue = -0.5 * s;
+  }
+  double j3_ratioGrad(int iat, Vec3& grad)
+  {
+    j3_partial = true;
+    j3_computeU3(iat, ab_r.data(), ab_dx.data(), ab_dy.data(), ab_dz.data(), aa_r.data(), aa_dx.data(), aa_dy.data(),
+                 aa_dz.data(), j3_cur_Uat, j3_cur_dUat, j3_cur_d2Uat, j3_newUk.data(), j3_newdUk.data(),
+                 j3_newd2Uk.data(), false);
+    for (int c = 0; c < 3; ++c)
+      grad[c] += j3_cur_dUat[c];
+    return std::exp(j3_Uat[iat] - j3_cur_Uat);
+  }
+  double j3_ratio(int iat)
+  {
+    j3_partial = false;
+    j3_cur_Uat = j3_computeU(iat, ab_r.data(), aa_r.data());
+    return std::exp(j3_Uat[iat] - j3_cur_Uat);
+  }
+  // acceptMove (ThreeBodyJastrow.h:300-389)
+  void j3_accept(int iat)
+  {
+    const int N = sys->n_elec, I = sys->n_ions;
+    ab_row(pos(iat), j3_r.data(), j3_dx.data(), j3_dy.data(), j3_dz.data());
+    aa_row_current(iat);
+    Vec3 dtemp;
+    j3_computeU3(iat, j3_r.data(), j3_dx.data(), j3_dy.data(), j3_dz.data(), row_r.data(), row_dx.data(),
+                 row_dy.data(), row_dz.data(), j3_Uat[iat], dtemp, j3_d2Uat[iat], j3_oldUk.data(), j3_olddUk.data(),
+                 j3_oldd2Uk.data(), false);
+    if (!j3_partial)
+      j3_computeU3(iat, ab_r.data(), ab_dx.data(), ab_dy.data(), ab_dz.data(), aa_r.data(), aa_dx.data(),
+                   aa_dy.data(), aa_dz.data(), j3_cur_Uat, j3_cur_dUat, j3_cur_d2Uat, j3_newUk.data(),
+                   j3_newdUk.data(), j3_newd2Uk.data(), false);
+    for (int jel = 0; jel < N; jel++)
+    {
+      j3_Uat[jel] += j3_newUk[jel] - j3_oldUk[jel];
+      j3_d2Uat[jel] += j3_newd2Uk[jel] - j3_oldd2Uk[jel];
+    }
+    for (int c = 0; c < 3; ++c)
+      for (int jel = 0; jel < N; jel++)
+        j3_dUat[3 * jel + c] += j3_newdUk[3 * jel + c] - j3_olddUk[3 * jel + c];
+    j3_LogValue += j3_Uat[iat] - j3_cur_Uat;
+    j3_Uat[iat] = j3_cur_Uat;
+    for (int c = 0; c < 3; ++c)
+      j3_dUat[3 * iat + c] = j3_cur_dUat[c];
+    j3_d2Uat[iat] = j3_cur_d2Uat;
+    const int ig = egroup(iat);
+    for (int jat = 0; jat < I; jat++)
+    {
+      auto& lst      = j3_in[ig * I + jat];
+      auto& ld       = j3_in_d[ig * I + jat];
+      auto& lx       = j3_in_dx[ig * I + jat];
+      const bool in  = ab_r[jat] < j3_cut[jat];
+      const auto it  = std::find(lst.begin(), lst.end(), iat);
+      const size_t k = it - lst.begin();
+      if (in)
+      {
+        if (it == lst.end())
+        {
+          lst.push_back(iat);
+          ld.push_back(ab_r[jat]);
+          lx.push_back(Vec3{ab_dx[jat], ab_dy[jat], ab_dz[jat]});
+        }
+        else
+        {
+          ld[k] = ab_r[jat];
+          lx[k] = Vec3{ab_dx[jat], ab_dy[jat], ab_dz[jat]};
+        }
+      }
+      else if (it != lst.end())
+      {
+        lst[k] = lst.back();
+        lst.pop_back();
+        ld[k] = ld.back();
+        ld.pop_back();
+        lx[k] = lx.back();
+        lx.pop_back();
+      }
+    }
+  }
+
   // ---- ParticleSet protocol (ParticleSet.cpp:280-378) ----
   void makeMove(int iat, const Vec3& displ)
   {
@@ -1584,6 +2123,12 @@ struct Walker
       j2_GL();
       LogValue += j2_LogValue;
     }
+    if (sys->use_j3)
+    {
+      j3_recompute();
+      j3_GL();
+      LogValue += j3_LogValue;
+    }
     return ok;
   }
   Vec3 evalGrad(int iat)
@@ -1596,6 +2141,9 @@ struct Walker
     if (sys->use_j2)
       for (int c = 0; c < 3; ++c)
         g[c] += j2_dUat[3 * iat + c];
+    if (sys->use_j3)
+      for (int c = 0; c < 3; ++c)
+        g[c] += j3_dUat[3 * iat + c];
     return g;
   }
   double ratioGrad(int iat, Vec3& grad)
@@ -1607,6 +2155,8 @@ struct Walker
       ratio *= j1_ratioGrad(iat, grad);
     if (sys->use_j2)
       ratio *= j2_ratioGrad(iat, grad);
+    if (sys->use_j3)
+      ratio *= j3_ratioGrad(iat, grad);
     return ratio;
   }
   double ratio(int iat)
@@ -1617,6 +2167,8 @@ struct Walker
       r *= j1_ratio(iat);
     if (sys->use_j2)
       r *= j2_ratio(iat);
+    if (sys->use_j3)
+      r *= j3_ratio(iat);
     return r;
   }
   void acceptMove(int iat)
@@ -1628,6 +2180,8 @@ struct Walker
       j1_accept(iat);
     if (sys->use_j2)
       j2_accept(iat);
+    if (sys->use_j3)
+      j3_accept(iat);
   }
   void completeUpdates()
   {
@@ -1655,6 +2209,11 @@ struct Walker
     {
       j2_GL();
       LogValue += j2_LogValue;
+    }
+    if (sys->use_j3)
+    {
+      j3_GL();
+      LogValue += j3_LogValue;
     }
   }
 };

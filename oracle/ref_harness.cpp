@@ -18,7 +18,10 @@
 #include <QMCWaveFunctions/Jastrow/BsplineFunctor.h>
 #include <QMCWaveFunctions/Jastrow/OneBodyJastrow.h>
 #include <QMCWaveFunctions/Jastrow/TwoBodyJastrow.h>
+#include <QMCWaveFunctions/Jastrow/PolynomialFunctor3D.h>
+#include <QMCWaveFunctions/Jastrow/ThreeBodyJastrow.h>
 #include <Drivers/NonLocalPP.hpp>
+#include <array>
 #include <cstdio>
 #include <random>
 #include <string>
@@ -276,6 +279,134 @@ int main(int argc, char** argv)
     arr("spo_v", v.data(), v.size());
     arr("spo_g", g.data(), g.size());
     arr("spo_h", h.data(), h.size());
+  }
+  // ---- the three-body (eeI) Jastrow, built as WaveFunction does with -j
+  // (WaveFunction.cpp:97-100, nio.hpp buildJeeI): variant "q" on the
+  // reference's own ions (every ion in group 0), variant "g" with the ions
+  // split into their species (0-15 group 0, 16-31 group 1)
+  for (int variant = 0; variant < 2; ++variant)
+  {
+    const char* tag = variant == 0 ? "q" : "g";
+    std::vector<int> saved(ions.GroupID.begin(), ions.GroupID.end());
+    if (variant == 1)
+      for (int i = 0; i < I; ++i)
+        ions.GroupID[i] = i < 16 ? 0 : 1;
+    RandomGenerator<RealType> rng3(myPrimes[1]);
+    ParticleSet e3;
+    build_els(e3, ions, rng3);
+    e3.addTable(e3, DT_SOA);
+    ThreeBodyJastrow<PolynomialFunctor3D> J3(ions, e3);
+    buildJeeI(J3, e3.Lattice.WignerSeitzRadius);
+    e3.update();
+    char key[64];
+    if (variant == 0)
+    {
+      // buildJeeI's functors, captured through its addFunc interface
+      struct Capture
+      {
+        using FuncType = PolynomialFunctor3D;
+        PolynomialFunctor3D* f[2][2][2] = {};
+        void addFunc(int i, int a, int b, PolynomialFunctor3D* p) { f[i][a][b] = p; }
+      } cap;
+      buildJeeI(cap, e3.Lattice.WignerSeitzRadius);
+      printf("\"j3_rcut\": %.17g,\n", cap.f[0][0][0]->cutoff_radius);
+      const char* names[4] = {"j3_gamma_uu0", "j3_gamma_ud0", "j3_gamma_uu1", "j3_gamma_ud1"};
+      for (int q = 0; q < 4; ++q)
+      {
+        const PolynomialFunctor3D* f = cap.f[q / 2][0][q % 2];
+        std::vector<double> gm;
+        for (int l = 0; l < 4; ++l)
+          for (int m = 0; m < 4; ++m)
+            for (int n = 0; n < 4; ++n)
+              gm.push_back(f->gamma(l, m, n));
+        arr(names[q], gm.data(), gm.size());
+      }
+      std::vector<double> ev;
+      for (auto pt : std::vector<std::array<double, 3>>{{1.1, 0.7, 1.3}, {0.4, 2.0, 0.9}, {2.5, 1.6, 1.7}})
+      {
+        TinyVector<RealType, 3> g;
+        Tensor<RealType, 3> h;
+        const double v = cap.f[0][0][1]->evaluate(pt[0], pt[1], pt[2], g, h);
+        ev.push_back(v);
+        for (int d = 0; d < 3; ++d)
+          ev.push_back(g[d]);
+        ev.push_back(h(0, 0)), ev.push_back(h(0, 1)), ev.push_back(h(0, 2));
+        ev.push_back(h(1, 1)), ev.push_back(h(1, 2)), ev.push_back(h(2, 2));
+      }
+      arr("j3_ud0_eval_val_grad3_hess6", ev.data(), ev.size());
+    }
+    auto p0 = flat(e3.R);
+    snprintf(key, sizeof(key), "j3%s_R0", tag);
+    arr(key, p0.data(), p0.size());
+    e3.G = 0.0;
+    e3.L = 0.0;
+    const double l3 = J3.evaluateLog(e3, e3.G, e3.L);
+    printf("\"j3%s_log\": %.17g,\n", tag, l3);
+    std::vector<double> g, l;
+    for (int i = 0; i < N; ++i)
+    {
+      for (int d = 0; d < 3; ++d)
+        g.push_back(e3.G[i][d]);
+      l.push_back(e3.L[i]);
+    }
+    snprintf(key, sizeof(key), "j3%s_G", tag);
+    arr(key, g.data(), g.size());
+    snprintf(key, sizeof(key), "j3%s_L", tag);
+    arr(key, l.data(), l.size());
+    // one substep of the move protocol with J3 only, continuing the stream
+    std::vector<double> ur(N);
+    ParticlePos_t delta(N);
+    rng3.generate_uniform(ur.data(), N);
+    rng3.generate_normal(&delta[0][0], 3 * N);
+    std::vector<double> ratios, gnew, gnow;
+    std::vector<int> acc;
+    for (int iel = 0; iel < N; ++iel)
+    {
+      e3.setActive(iel);
+      PosType g0 = J3.evalGrad(e3, iel);
+      e3.makeMove(iel, delta[iel]);
+      PosType gn(0.0);
+      ratios.push_back(J3.ratioGrad(e3, iel, gn));
+      for (int d = 0; d < 3; ++d)
+        gnew.push_back(gn[d]), gnow.push_back(g0[d]);
+      if (ur[iel] < 0.5)
+      {
+        J3.acceptMove(e3, iel);
+        e3.acceptMove(iel);
+        acc.push_back(1);
+      }
+      else
+      {
+        e3.rejectMove(iel);
+        acc.push_back(0);
+      }
+    }
+    e3.donePbyP();
+    e3.G = 0.0;
+    e3.L = 0.0;
+    J3.evaluateGL(e3, e3.G, e3.L);
+    snprintf(key, sizeof(key), "j3%s_sweep_ratio", tag);
+    arr(key, ratios.data(), ratios.size());
+    snprintf(key, sizeof(key), "j3%s_sweep_grad_new", tag);
+    arr(key, gnew.data(), gnew.size());
+    snprintf(key, sizeof(key), "j3%s_sweep_grad_now", tag);
+    arr(key, gnow.data(), gnow.size());
+    snprintf(key, sizeof(key), "j3%s_sweep_accept", tag);
+    arri(key, acc.data(), acc.size());
+    printf("\"j3%s_sweep_log\": %.17g,\n", tag, J3.LogValue);
+    g.clear(), l.clear();
+    for (int i = 0; i < N; ++i)
+    {
+      for (int d = 0; d < 3; ++d)
+        g.push_back(e3.G[i][d]);
+      l.push_back(e3.L[i]);
+    }
+    snprintf(key, sizeof(key), "j3%s_sweep_G", tag);
+    arr(key, g.data(), g.size());
+    snprintf(key, sizeof(key), "j3%s_sweep_L", tag);
+    arr(key, l.data(), l.size());
+    for (int i = 0; i < I; ++i)
+      ions.GroupID[i] = saved[i];
   }
   {
     // NonLocalPP's rotated quadrature spheres of its first three randomize

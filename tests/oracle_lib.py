@@ -38,6 +38,8 @@ def library():
             'splitmix_uniform': (C.c_double, [C.c_uint64, C.c_uint64]),
             'distance_row': (C.c_int, [capi.PD, capi.PD, capi.PD, C.c_int, C.c_int, capi.PD, capi.PD]),
             'functor_eval': (C.c_int, [C.POINTER(capi.Functor), C.c_double, capi.PD]),
+            'j3_functor_eval': (C.c_int, [C.POINTER(capi.J3Functor), C.c_double, C.c_double, C.c_double,
+                                          capi.PD]),
             'walkers_skip': (C.c_int, [C.c_void_p, C.c_int]),
             'num_threads': (C.c_int, []),
             'detengine_delay_count': (C.c_int, [C.c_void_p]),

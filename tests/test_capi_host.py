@@ -78,6 +78,27 @@ def test_functors_and_jastrows_match_oracle(prod):
         assert list(fa.coefs) == list(fb.coefs)
 
 
+def test_j3_functors_match_reference(prod):
+    """The product's PolynomialFunctor3D::reset_gamma restatement and its
+    buildJeeI tables against the gammas the reference printed, on two cells
+    (the reference's 32-atom cell and the 4x4x2 NiO-128 cell)."""
+    import json
+    gold = json.load(open(os.path.join(oracle_lib.GOLDEN, 'reference_dump.json')))
+    lat = prod.nio(capi.NIO_REF32, (1, 1, 1), 3)['lattice']
+    j3 = prod.nio_j3(lat)
+    assert j3['same'][0].cutoff == gold['j3_rcut']
+    for key, f in (('j3_gamma_uu0', j3['same'][0]), ('j3_gamma_ud0', j3['diff'][0]),
+                   ('j3_gamma_uu1', j3['same'][1]), ('j3_gamma_ud1', j3['diff'][1])):
+        np.testing.assert_allclose(list(f.gamma), gold[key], rtol=1e-12, atol=1e-15)
+    orc = oracle_lib.library()
+    lat = prod.nio(capi.NIO_PRIM4, (4, 4, 2), 0)['lattice']
+    ja, jb = prod.nio_j3(lat), orc.nio_j3(lat)
+    for s in range(2):
+        for kind in ('same', 'diff'):
+            assert ja[kind][s].cutoff == jb[kind][s].cutoff
+            np.testing.assert_allclose(list(ja[kind][s].gamma), list(jb[kind][s].gamma), rtol=1e-12, atol=1e-15)
+
+
 def test_synthetic_jastrows_c_equals_python(prod):
     lat = prod.nio(capi.NIO_PRIM4, (2, 2, 1))['lattice']
     py = api.synthetic_jastrows(prod, lat, 2, 13, 8)
