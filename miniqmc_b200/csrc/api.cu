@@ -991,6 +991,7 @@ int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi)
   }
   CK(launch_gl(w->fp32, w->sys->d, w->dw, w->threads, w->stream));
   w->launches++;
+  w->ratio_moves = false;
   std::vector<MoveState> ms(w->dw.W);
   for (auto& m : ms)
   {
@@ -1043,7 +1044,12 @@ int qmc_wf_ratio_grad(qmc_walkers* w, int iat, double* ratio, double* grad)
 {
   return ratio_verb(w, VERB_RATIO_GRAD, iat, ratio, grad);
 }
-int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio) { return ratio_verb(w, VERB_RATIO, iat, ratio, nullptr); }
+int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio)
+{
+  if (w)
+    w->ratio_moves = true;
+  return ratio_verb(w, VERB_RATIO, iat, ratio, nullptr);
+}
 
 int qmc_wf_complete_updates(qmc_walkers* w)
 {
@@ -1062,6 +1068,12 @@ int qmc_wf_evaluate_gl(qmc_walkers* w, double* G, double* L, double* logpsi)
 {
   if (!w)
     return fail(QMC_ERR_ARG, "null handle");
+  if (w->ratio_moves && (w->sys->h.comp & QMC_WF_DET))
+  {
+    // derivative rows of the determinants left in ratio-only mode
+    CK(launch_spo_matrix(w->fp32, w->sys->d, w->dw, false, w->stream, true));
+    w->launches++;
+  }
   CK(launch_gl(w->fp32, w->sys->d, w->dw, w->threads, w->stream));
   w->launches++;
   const size_t W = w->dw.W, N = w->dw.N;

@@ -43,6 +43,7 @@ struct qmc_walkers_s
   size_t bytes      = 0;
   int64_t launches  = 0;
   int64_t steps_done = 0; // MC steps swept by this batch over all calls
+  bool ratio_moves   = false; // a ratio-only verb ran since the last evaluateLog
   int64_t nlpp_calls = 0; // NonLocalPP sphere rotations drawn so far
   qmc::SweepTask* d_task = nullptr;
   double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;

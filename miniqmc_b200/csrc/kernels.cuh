@@ -54,8 +54,10 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
                          double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3);
 
 // evaluateLog pieces
+// ratio_mode_only: only the derivative rows of the determinants whose last
+// move was ratio-only (the evaluateGL re-evaluation)
 cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu,
-                              cudaStream_t st);
+                              cudaStream_t st, bool ratio_mode_only = false);
 cudaError_t launch_gj_inverse(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads, int n_spins,
                               cudaStream_t st);
 cudaError_t launch_jastrow_recompute(bool fp32, const DevSystem* sys, const DevWalkers& dw, int threads,

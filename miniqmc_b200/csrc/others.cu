@@ -347,13 +347,19 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
 // SPOSet::evaluate_notranspose for every electron of every walker: the
 // FP64 Slater matrices (for the inverse) and the derivative rows.
 template <typename T>
-__global__ void __launch_bounds__(256) spo_matrix_kernel(const DevSystem* __restrict__ sys, DevWalkers dw, int want_lu)
+__global__ void __launch_bounds__(256) spo_matrix_kernel(const DevSystem* __restrict__ sys, DevWalkers dw, int want_lu,
+                                                         int ratio_mode_only)
 {
   constexpr int VW = Vec16<T>::width;
   __shared__ SplineSmem<T> sp;
   __shared__ double pos[3];
   const int i = blockIdx.x, w = blockIdx.y;
   const WV<T> wv = make_wv<T>(dw, w);
+  // DiracDeterminant::evaluateGL (DiracDeterminant.cpp:163-168) re-evaluates
+  // the derivative rows only when the determinant's last move was a
+  // ratio-only one (UpdateMode ORB_PBYP_RATIO); the test is uniform per block
+  if (ratio_mode_only && wv.ms->partial[i < sys->n_up ? 0 : 1])
+    return;
   if (threadIdx.x == 0)
   {
     for (int c = 0; c < 3; ++c)
@@ -1076,15 +1082,16 @@ cudaError_t launch_verb(bool fp32, const DevSystem* sys, const DevWalkers& dw, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu, cudaStream_t st)
+cudaError_t launch_spo_matrix(bool fp32, const DevSystem* sys, const DevWalkers& dw, bool want_lu, cudaStream_t st,
+                              bool ratio_mode_only)
 {
   dim3 grid(dw.N, dw.W);
   const int vw      = fp32 ? 4 : 2;
   const int threads = min(256, round_up(dw.npad / vw, 32));
   if (fp32)
-    spo_matrix_kernel<float><<<grid, threads, 0, st>>>(sys, dw, want_lu ? 1 : 0);
+    spo_matrix_kernel<float><<<grid, threads, 0, st>>>(sys, dw, want_lu ? 1 : 0, ratio_mode_only ? 1 : 0);
   else
-    spo_matrix_kernel<double><<<grid, threads, 0, st>>>(sys, dw, want_lu ? 1 : 0);
+    spo_matrix_kernel<double><<<grid, threads, 0, st>>>(sys, dw, want_lu ? 1 : 0, ratio_mode_only ? 1 : 0);
   return cudaGetLastError();
 }
 

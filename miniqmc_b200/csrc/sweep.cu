@@ -109,6 +109,10 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   phase_mark(m, PH_GL);
   if (threadIdx.x == 0)
   {
+    // every move of the sweep was a ratioGrad one (DiracDeterminant's
+    // UpdateMode ORB_PBYP_PARTIAL)
+    wv.ms->partial[0] = wv.ms->partial[1] = 1;
+    wv.ms->j_partial                      = 1;
     task.dw.accepted[w] += acc;
     if (task.timers)
       for (int p = 0; p < NPHASE; ++p)

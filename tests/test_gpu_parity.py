@@ -209,6 +209,36 @@ def test_verbs(delay):
     assert rel_err(gw.components(), ow.components()) < RTOL64
 
 
+@pytest.mark.parametrize('last', ['ratio', 'ratio_grad'])
+def test_evaluate_gl_after_ratio_only_move(last):
+    """DiracDeterminant::evaluateGL re-evaluates the orbital derivative rows
+    of a determinant whose last move was ratio-only (the accept of such a
+    move leaves its dpsiM / d2psiM row stale); after a ratioGrad move it
+    does not, and the stale row stays.  Both outcomes match the oracle."""
+    gw, ow = H.make_pair(walkers=1, delay=2)
+    gw.evaluate_log()
+    ow.evaluate_log()
+    acc = np.ones(1, dtype=np.int32)
+    d = np.array([[0.3, -0.2, 0.4]])
+    for iel, kind in ((3, 'ratio'), (7, last)):
+        gw.make_move(iel, d)
+        ow.make_move(iel, d)
+        if kind == 'ratio':
+            check_ratios(gw.ratio(iel), ow.ratio(iel), RTOL64)
+        else:
+            gw.ratio_grad(iel)
+            ow.ratio_grad(iel)
+        gw.accept_restore(iel, acc)
+        ow.accept_restore(iel, acc)
+        gw.accept_reject(iel, acc)
+        ow.accept_reject(iel, acc)
+    gw.complete_updates()
+    ow.complete_updates()
+    Gg, Lg, _ = gw.evaluate_gl()
+    Go, Lo, _ = ow.evaluate_gl()
+    assert rel_err(Gg, Go) < 1e-9 and rel_err(Lg, Lo) < 1e-9
+
+
 @pytest.mark.parametrize('delay', [1, 4])
 def test_sweep_host_rng_fp64(delay):
     """Fused sweep vs oracle on identical random streams: bit-exact accept
