@@ -117,6 +117,29 @@ __device__ __forceinline__ J3Val<T> j3_vgl(const T* __restrict__ gam, T L, T r12
   return o;
 }
 
+// PolynomialFunctor3D::evaluateV for one triple inside both ion cutoffs:
+// the value only
+template <typename T> __device__ __forceinline__ T j3_v(const T* __restrict__ gam, T L, T r12, T r1I, T r2I)
+{
+  const T pl[4] = {T(1), r1I, r1I * r1I, r1I * r1I * r1I};
+  const T pm[4] = {T(1), r2I, r2I * r2I, r2I * r2I * r2I};
+  const T pn[4] = {T(1), r12, r12 * r12, r12 * r12 * r12};
+  T val = 0;
+#pragma unroll
+  for (int l = 0; l < 4; ++l)
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+    {
+      T s0 = 0;
+#pragma unroll
+      for (int n = 0; n < 4; ++n)
+        s0 += __ldg(gam + 16 * l + 4 * m + n) * pn[n];
+      val += pl[l] * pm[m] * s0;
+    }
+  const T ab = (r2I - L) * (r1I - L);
+  return val * ab * ab * ab;
+}
+
 // the minimum-image e-I distance of ion c from (px, py, pz) and the
 // displacement ion - electron (DistanceTableBA, every entry flipped), or a
 // value not below `cut` when every image is beyond it.  Every membership

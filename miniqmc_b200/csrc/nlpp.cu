@@ -12,15 +12,18 @@
 // DTD_BConds with every entry flipped, ParticleBConds.h:154-217).  The ratio
 // is WaveFunction::ratio (WaveFunction.cpp): the SPO values at r' dotted
 // with the electron's inverse row (DiracDeterminant::ratio; no delayed rows
-// are pending after completeUpdates), times exp(Vat - J1(r')) and
-// exp(Uat - J2(r')) (OneBodyJastrow / TwoBodyJastrow ratio).
+// are pending after completeUpdates), times exp(Vat - J1(r')),
+// exp(Uat - J2(r')) and exp(Uat3 - J3(r')) (OneBodyJastrow / TwoBodyJastrow
+// ratio, ThreeBodyJastrow::evaluateRatios through computeU).
 //
 // One CTA per walker.  Per electron the ions within rmax are gathered in
 // ascending order by a warp-ballot compaction; per ion the 12 knots are
 // evaluated together: every thread walks its 16-byte orbital vectors for all
 // 12 stencils (det partials in registers, warp-reduced), and the J1 / J2
 // pairs (ion or electron, knot) within the cutoff add into per-knot sums in
-// shared memory.
+// shared memory; the J3 value of each knot is one warp's: its ions within
+// the J3 cutoff by ballot, then the (ion, listed electron) triples over the
+// lanes.
 #include "device.cuh"
 #include "host_api.hpp"
 
@@ -51,14 +54,20 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
   __shared__ SysSmem<T> ss;
   __shared__ SplineSmem<T> sk[NLPP_K];
   __shared__ double vpos[NLPP_K][3];
-  __shared__ double sums[3 * NLPP_K];
+  __shared__ double sums[4 * NLPP_K];
   __shared__ int s_n, wcnt[8], in_iat[NLPP_MAXIN];
   __shared__ double in_d[NLPP_MAXIN], in_dx[NLPP_MAXIN][3];
+  __shared__ int j3_ion[8][J3_NEAR], j3_seg[8][2 * J3_NEAR + 1];
+  __shared__ T j3_r[8][J3_NEAR];
+  __shared__ int spin_used[2];
   const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
   load_sys(sys, ss);
   const int w    = blockIdx.x;
   const WV<T> wv = make_wv<T>(dw, w);
   const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const bool J3  = ss.comp & QMC_WF_J3;
+  if (tid < 2)
+    spin_used[tid] = 0;
   const int N = wv.N, I = ss.n_ions, npad = wv.npad, nvec = npad / VW;
   const T* ions  = (const T*)sys->ion_soa;
   const T* coefs = (const T*)sys->coefs;
@@ -136,7 +145,7 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
         if (DET)
           spline_locate(sys, vpos[k], sk[k]);
       }
-      if (tid < 3 * NLPP_K)
+      if (tid < 4 * NLPP_K)
         sums[tid] = 0.0;
       __syncthreads();
       // ---- determinant: SPO values at the 12 points . inverse row
@@ -202,10 +211,85 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
             atomicAdd(&sums[2 * NLPP_K + k], (double)functor_v(f, rr));
         }
       }
+      // ---- J3: warp per point
+      if (J3)
+      {
+        const unsigned below = (1u << lane) - 1u;
+        const T* gam         = (const T*)sys->j3_gamma;
+        const int jg         = jel < ss.n_up ? 0 : 1;
+        for (int k = wid; k < NLPP_K; k += nw)
+        {
+          const T px = (T)vpos[k][0], py = (T)vpos[k][1], pz = (T)vpos[k][2];
+          int nn     = 0;
+          for (int c0 = 0; c0 < I; c0 += 32)
+          {
+            const int c = c0 + lane;
+            bool in     = false;
+            T rr        = 0;
+            if (c < I)
+            {
+              const T cut = ss.j3cut[ion_group(ss, c)];
+              T dx, dy, dz;
+              rr = j3_ion_dist(ss, ions, c, px, py, pz, cut, dx, dy, dz);
+              in = rr < cut;
+            }
+            const unsigned b = __ballot_sync(0xffffffffu, in);
+            const int at     = nn + __popc(b & below);
+            if (in)
+            {
+              if (at < J3_NEAR)
+                j3_ion[wid][at] = c, j3_r[wid][at] = rr;
+              else
+                atomicOr(wv.status, DEV_ERR_CAPACITY);
+            }
+            nn += __popc(b);
+          }
+          nn           = nn < J3_NEAR ? nn : J3_NEAR;
+          const int ns = 2 * nn;
+          __syncwarp();
+          for (int q = lane; q < ns; q += 32)
+            j3_seg[wid][q + 1] = wv.j3cnt[(q / nn) * I + j3_ion[wid][q % nn]];
+          __syncwarp();
+          if (lane == 0)
+          {
+            j3_seg[wid][0] = 0;
+            for (int q = 1; q <= ns; ++q)
+              j3_seg[wid][q] += j3_seg[wid][q - 1];
+          }
+          __syncwarp();
+          const int P = j3_seg[wid][ns];
+          double u    = 0.0;
+          for (int p = lane; p < P; p += 32)
+          {
+            int q = 0;
+            while (j3_seg[wid][q + 1] <= p)
+              ++q;
+            const int kg = q / nn, slot = q % nn, ion = j3_ion[wid][slot];
+            const int k2 = wv.j3list[((size_t)kg * I + ion) * wv.j3cap + (p - j3_seg[wid][q])];
+            if (k2 == jel)
+              continue;
+            const T kx = wv.Rs[k2], ky = wv.Rs[wv.Npad + k2], kz = wv.Rs[2 * wv.Npad + k2];
+            T ix = (ions[ion] - kx) * T(-1), iy = (ions[I + ion] - ky) * T(-1), iz = (ions[2 * I + ion] - kz) * T(-1);
+            const T rkI  = min_image(ix, iy, iz, ss.rb, ss.gb, ss.cn);
+            const T flip = k2 < jel ? T(1) : T(-1);
+            T ex = (kx - px) * flip, ey = (ky - py) * flip, ez = (kz - pz) * flip;
+            const T rjk = min_image(ex, ey, ez, ss.rb, ss.gb, ss.cn);
+            const int ig = ion_group(ss, ion);
+            u += (double)j3_v(gam + (size_t)(2 * ig + (jg == kg ? 0 : 1)) * 64, ss.j3cut[ig], rjk,
+                              j3_r[wid][slot], rkI);
+          }
+          u = warp_sum(u);
+          if (lane == 0)
+            sums[3 * NLPP_K + k] = u;
+          __syncwarp(); // this warp's near-ion arrays are rewritten for its next point
+        }
+      }
       __syncthreads();
       if (tid == 0)
       {
+        spin_used[s] = 1;
         const double vat = J1 ? (double)wv.Vat[jel] : 0.0, uat = J2 ? (double)wv.Uat[jel] : 0.0;
+        const double u3  = J3 ? (double)wv.j3Uat[jel] : 0.0;
         for (int k = 0; k < NLPP_K; ++k)
         {
           double ratio = DET ? sums[k] : 1.0;
@@ -213,6 +297,8 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
             ratio *= exp(vat - sums[NLPP_K + k]);
           if (J2)
             ratio *= exp(uat - sums[2 * NLPP_K + k]);
+          if (J3)
+            ratio *= exp(u3 - sums[3 * NLPP_K + k]);
           wsum += wk * ratio;
           ++cnt;
           if (w == 0 && a.ratios && n_out < a.max_ratios)
@@ -226,6 +312,11 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
   {
     a.wsum[w]  = wsum;
     a.count[w] = cnt;
+    // DiracDeterminant::ratio leaves a determinant it evaluated in the
+    // ratio-only update mode (its next evaluateGL re-evaluates dpsiM)
+    for (int q = 0; q < 2; ++q)
+      if (DET && spin_used[q])
+        wv.ms->partial[q] = 0;
   }
 }
 
@@ -295,8 +386,6 @@ int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, 
 {
   if (!w || rmax <= 0 || (form != QMC_NLPP_SPHERE && form != QMC_NLPP_DRIVER) || (ratios && max_ratios < 0))
     return fail(QMC_ERR_ARG, "bad NLPP arguments");
-  if (w->sys->h.comp & QMC_WF_J3)
-    return fail(QMC_ERR_ARG, "NLPP ratios with the three-body Jastrow are not implemented");
   const size_t W = w->dw.W;
   NlppArgs a{};
   nlpp_sphere((int)w->nlpp_calls, a.rot);
@@ -313,6 +402,7 @@ int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, 
   CK(launch_nlpp(w->fp32, w->sys->d, w->dw, a, threads, w->stream));
   w->launches++;
   w->nlpp_calls++;
+  w->ratio_moves = true; // the determinants it evaluated are in ratio-only mode
   std::vector<double> hw(W);
   std::vector<long long> hc(W);
   CK(cudaMemcpyAsync(hw.data(), a.wsum, W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));

@@ -17,8 +17,10 @@
 // well-conditioned SplitMix64 fill (-F uniform, seed -s).  -P picks the
 // arithmetic form and -R the FP64 refresh interval of the inverses (0 = off).
 // -a (spline tiles) is accepted and ignored: the table is one tile per
-// walker CTA here.  -b (reference implementations) and -j (three-body
-// Jastrow) are not part of this library and stop the driver with a message.
+// walker CTA here.  -j adds the three-body Jastrow with buildJeeI's
+// functors (WaveFunction.cpp:97-100, nio.hpp:171-245).  -b (the reference
+// implementations) is not part of this library and stops the driver with a
+// message.
 // After the steps, the pseudopotential ratios of the reference's loop
 // (miniqmc.cpp:472-495) run once per step through qmc_nlpp_evaluate, with
 // -x as rmax and the driver's form of the virtual moves.
@@ -48,7 +50,7 @@ void print_help()
               "  -b  use reference implementations  (not available)\n"
               "  -g  set the 3D tiling.             default: 1 1 1\n"
               "  -h  print help and exit\n"
-              "  -j  enable three body Jastrow      (not available)\n"
+              "  -j  enable three body Jastrow      default: off\n"
               "  -m  meshfactor                     default: 1.0\n"
               "  -n  number of MC steps             default: 5\n"
               "  -N  number of MC substeps          default: 1\n"
@@ -107,7 +109,7 @@ int main(int argc, char** argv)
   int na = 1, nb = 1, nc = 1, nsteps = 5, nsubsteps = 1, iseed = 11, nmovers = 512, delay_rank = 32;
   int nx = 37, ny = 37, nz = 37, refresh = 8;
   double accept = 0.5, rmax = 1.7;
-  bool verbose = false, fill_reference = false, fp64 = false;
+  bool verbose = false, fill_reference = false, fp64 = false, enable_j3 = false;
   std::string timer_level = "fine";
   int opt;
   while (optind < argc)
@@ -121,9 +123,7 @@ int main(int argc, char** argv)
       case 'b':
         std::fprintf(stderr, "miniqmc: the reference implementations (-b) are not part of this library\n");
         return 1;
-      case 'j':
-        std::fprintf(stderr, "miniqmc: the three-body Jastrow (-j) is not built\n");
-        return 1;
+      case 'j': enable_j3 = true; break;
       case 'g':
         if (std::sscanf(optarg, "%d %d %d", &na, &nb, &nc) != 3)
         {
@@ -196,9 +196,17 @@ int main(int argc, char** argv)
   d.spo_fill   = fill_reference ? QMC_FILL_REFERENCE : QMC_FILL_UNIFORM;
   d.spo_seed   = (uint64_t)iseed;
   d.lap_mode   = QMC_LAP_HXX;
-  d.components = QMC_WF_ALL;
+  d.components = QMC_WF_ALL | (enable_j3 ? QMC_WF_J3 : 0);
   if (check(qmc_nio_jastrows(d.lattice, &d.j1[0], &d.j1[1], &d.j2_uu, &d.j2_ud), "qmc_nio_jastrows"))
     return 1;
+  if (enable_j3)
+  {
+    qmc_j3_functor same[2], diff[2];
+    if (check(qmc_nio_j3(d.lattice, same, diff), "qmc_nio_j3"))
+      return 1;
+    for (int g = 0; g < d.n_ion_groups; ++g)
+      d.j3_same[g] = same[g < 2 ? g : 1], d.j3_diff[g] = diff[g < 2 ? g : 1];
+  }
 
   const size_t coef_bytes = (size_t)norb * (nx + 3) * (ny + 3) * (nz + 3) * (fp64 ? 8 : 4);
   std::printf("Number of orbitals/splines = %d\nTile size = %d\nNumber of tiles = 1\nNumber of electrons = %d\n"

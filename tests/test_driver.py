@@ -33,7 +33,7 @@ def test_help_and_version_exit_1(exe):
     assert run(exe, '-V').returncode == 1
 
 
-@pytest.mark.parametrize('opt', ['-b', '-j'])
+@pytest.mark.parametrize('opt', ['-b'])
 def test_unavailable_options_stop_with_a_message(exe, opt):
     r = run(exe, opt)
     assert r.returncode == 1 and r.stderr.strip()
@@ -46,8 +46,9 @@ def test_bad_arguments(exe):
 
 
 @pytest.mark.gpu
-def test_driver_matches_the_api(exe):
-    r = run(exe, '-g', '1 1 1', '-m', '0.5', '-w', '6', '-n', '2', '-k', '8', '-v')
+@pytest.mark.parametrize('j3', [False, True])
+def test_driver_matches_the_api(exe, j3):
+    r = run(exe, '-g', '1 1 1', '-m', '0.5', '-w', '6', '-n', '2', '-k', '8', '-v', *(['-j'] if j3 else []))
     assert r.returncode == 0, r.stdout + r.stderr
     assert 'Diffusion throughput' in r.stdout and 'Number of electrons = 384' in r.stdout
     accepted = int(re.search(r'Accepted moves = (\d+)', r.stdout).group(1))
@@ -55,7 +56,8 @@ def test_driver_matches_the_api(exe):
     lib = api.Library()
     lib.call('init', 0)
     spec = api.SystemSpec(lib, cell=capi.NIO_REF32, tiling=(1, 1, 1), grid=(18, 18, 18), fill=capi.FILL_UNIFORM,
-                          spo_seed=11, jastrow='reference')
+                          spo_seed=11, jastrow='reference',
+                          components=capi.WF_ALL | (capi.WF_J3 if j3 else 0))
     system = api.System(lib, spec, capi.PREC_MIXED)
     w = api.Walkers(system, 6, 8)
     primes = [3, 5, 7, 11, 13, 17]  # PrimeNumberSet<uint32_t> from 3

@@ -201,9 +201,43 @@ def test_j3_checkpoint_roundtrip():
     assert np.array_equal(a['logpsi'], b['logpsi'])
 
 
-def test_j3_nlpp_not_implemented():
-    gw, _ = H.make_pair(walkers=1, components=ALL_J3)
+@pytest.mark.parametrize('form', [capi.NLPP_SPHERE, capi.NLPP_DRIVER])
+def test_j3_nlpp_fp64(form):
+    """NonLocalPP ratios with J3 (ThreeBodyJastrow::evaluateRatios through
+    computeU at each quadrature point) against the oracle: same points,
+    ratios within the determinant's bound on this cell."""
+    gw, ow = H.make_pair(walkers=2, delay=4, components=ALL_J3, **REF)
     gw.evaluate_log()
-    with pytest.raises(api.QMCError) as ei:
-        gw.nlpp()
-    assert ei.value.status == 1  # QMC_ERR_ARG
+    ow.evaluate_log()
+    ng, wg, rg = gw.nlpp(1.7, form, max_ratios=1 << 14)
+    no, wo, ro = ow.nlpp(1.7, form, max_ratios=1 << 14)
+    assert np.array_equal(ng, no) and ng[0] > 0
+    m = int(ng[0])
+    check_ratios(rg[:m], ro[:m], 2e-9)
+    assert elem_rel(wg, wo).max() < 1e-9
+
+
+def test_j3_nlpp_jastrow_only_exact():
+    """J1 * J2 * J3 alone: the quadrature-point ratios agree to rounding."""
+    gw, ow = H.make_pair(walkers=1, components=capi.WF_J1 | capi.WF_J2 | capi.WF_J3, **REF)
+    gw.evaluate_log()
+    ow.evaluate_log()
+    ng, wg, rg = gw.nlpp(1.7, capi.NLPP_SPHERE, max_ratios=1 << 14)
+    no, wo, ro = ow.nlpp(1.7, capi.NLPP_SPHERE, max_ratios=1 << 14)
+    assert np.array_equal(ng, no)
+    m = int(ng[0])
+    assert elem_rel(rg[:m], ro[:m]).max() < 1e-12
+    # the J3-only ratios are not trivially one
+    assert np.abs(np.log(np.abs(ro[:m]))).max() > 1e-2
+
+
+def test_j3_nlpp_mixed():
+    gw, ow = H.make_pair(precision=capi.PREC_MIXED, walkers=1, delay=4, components=ALL_J3, **REF)
+    gw.evaluate_log()
+    ow.evaluate_log()
+    ng, wg, rg = gw.nlpp(1.7, capi.NLPP_SPHERE, max_ratios=1 << 14)
+    no, wo, ro = ow.nlpp(1.7, capi.NLPP_SPHERE, max_ratios=1 << 14)
+    assert np.array_equal(ng, no)
+    m = int(ng[0])
+    e = elem_rel(rg[:m], ro[:m])
+    assert np.median(e) < 1e-4 and np.percentile(e, 99) < 1e-2, (np.median(e), np.percentile(e, 99))
