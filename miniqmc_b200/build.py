@@ -80,9 +80,10 @@ def build_drivers(force=False):
     """Command-line drivers over the C ABI (no CUDA headers needed)."""
     os.makedirs(BIN, exist_ok=True)
     include = os.path.join(HERE, '..', 'include')
-    for src in sorted(glob.glob(os.path.join(DRIVERS, '*.cpp'))):
+    for src in sorted(glob.glob(os.path.join(DRIVERS, '*.cpp'))):  # driver_common.hpp is a header
         exe = os.path.join(BIN, os.path.basename(src)[:-4])
-        if not force and not _stale(exe, [src, LIB, os.path.join(include, 'qmcgpu.h')]):
+        if not force and not _stale(exe, [src, LIB, os.path.join(include, 'qmcgpu.h'),
+                                          os.path.join(DRIVERS, 'driver_common.hpp')]):
             continue
         cmd = [CXX, '-O2', '-std=c++17', '-I', include, src, '-L', HERE, '-lqmcgpu',
                '-Wl,-rpath,$ORIGIN/..', '-o', exe]

@@ -24,7 +24,7 @@
 // After the steps, the pseudopotential ratios of the reference's loop
 // (miniqmc.cpp:472-495) run once per step through qmc_nlpp_evaluate, with
 // -x as rmax and the driver's form of the virtual moves.
-#include "qmcgpu.h"
+#include "driver_common.hpp"
 
 #include <chrono>
 #include <cmath>
@@ -34,6 +34,9 @@
 #include <string>
 #include <unistd.h>
 #include <vector>
+
+using drv::check;
+using drv::now_s;
 
 namespace
 {
@@ -67,41 +70,6 @@ void print_help()
               "  -R  FP64 refresh every R steps     default: 8\n");
 }
 
-// PrimeNumberSet<uint32_t> (PrimeNumberSet.h): the primes from 3 upwards
-std::vector<uint32_t> primes(int n)
-{
-  std::vector<uint32_t> p;
-  for (uint32_t c = 3; (int)p.size() < n; c += 2)
-  {
-    bool ok = true;
-    for (uint32_t q : p)
-    {
-      if (q * q > c)
-        break;
-      if (c % q == 0)
-      {
-        ok = false;
-        break;
-      }
-    }
-    if (ok)
-      p.push_back(c);
-  }
-  return p;
-}
-
-double now_s()
-{
-  using namespace std::chrono;
-  return duration<double>(steady_clock::now().time_since_epoch()).count();
-}
-
-int check(int st, const char* what)
-{
-  if (st != QMC_OK)
-    std::fprintf(stderr, "miniqmc: %s failed: %s (%s)\n", what, qmc_status_string(st), qmc_last_error());
-  return st;
-}
 } // namespace
 
 int main(int argc, char** argv)
@@ -175,38 +143,11 @@ int main(int argc, char** argv)
     return 1;
 
   // ---- ions and electrons (build_ions + count_electrons, nio.hpp)
-  int n_ions = 0;
-  if (check(qmc_nio_count(QMC_NIO_REF32, na, nb, nc, &n_ions), "qmc_nio_count"))
+  drv::NioSystem nio;
+  if (nio.build(na, nb, nc, nx, ny, nz, fill_reference, iseed, QMC_WF_ALL | (enable_j3 ? QMC_WF_J3 : 0)))
     return 1;
-  std::vector<double> ion_pos(3 * (size_t)n_ions);
-  std::vector<int> ion_group(n_ions);
-  qmc_system_desc d;
-  std::memset(&d, 0, sizeof(d));
-  if (check(qmc_nio_build(QMC_NIO_REF32, na, nb, nc, 0, d.lattice, ion_pos.data(), ion_group.data(),
-                          &d.n_ion_groups, d.spo_lattice),
-            "qmc_nio_build"))
-    return 1;
-  int nels = 0;
-  for (int g : ion_group)
-    nels += g == 0 ? 6 : 18; // valence electrons of O and Ni
-  const int norb = nels / 2;
-  d.n_ions = n_ions, d.ion_pos = ion_pos.data(), d.ion_group = ion_group.data();
-  d.n_elec = nels, d.n_up = norb, d.n_orb = norb;
-  d.grid[0] = nx, d.grid[1] = ny, d.grid[2] = nz;
-  d.spo_fill   = fill_reference ? QMC_FILL_REFERENCE : QMC_FILL_UNIFORM;
-  d.spo_seed   = (uint64_t)iseed;
-  d.lap_mode   = QMC_LAP_HXX;
-  d.components = QMC_WF_ALL | (enable_j3 ? QMC_WF_J3 : 0);
-  if (check(qmc_nio_jastrows(d.lattice, &d.j1[0], &d.j1[1], &d.j2_uu, &d.j2_ud), "qmc_nio_jastrows"))
-    return 1;
-  if (enable_j3)
-  {
-    qmc_j3_functor same[2], diff[2];
-    if (check(qmc_nio_j3(d.lattice, same, diff), "qmc_nio_j3"))
-      return 1;
-    for (int g = 0; g < d.n_ion_groups; ++g)
-      d.j3_same[g] = same[g < 2 ? g : 1], d.j3_diff[g] = diff[g < 2 ? g : 1];
-  }
+  const qmc_system_desc& d = nio.d;
+  const int nels = nio.nels, norb = nio.norb;
 
   const size_t coef_bytes = (size_t)norb * (nx + 3) * (ny + 3) * (nz + 3) * (fp64 ? 8 : 4);
   std::printf("Number of orbitals/splines = %d\nTile size = %d\nNumber of tiles = 1\nNumber of electrons = %d\n"
@@ -228,7 +169,7 @@ int main(int argc, char** argv)
   qmc_walkers* w  = nullptr;
   if (check(qmc_walkers_create(sys, nmovers, delay_rank, &w), "qmc_walkers_create"))
     return 1;
-  std::vector<uint32_t> seeds = primes(nmovers);
+  std::vector<uint32_t> seeds = drv::primes(nmovers);
   if (check(qmc_walkers_init_random(w, seeds.data()), "qmc_walkers_init_random"))
     return 1;
   int st = qmc_wf_evaluate_log(w, nullptr);
