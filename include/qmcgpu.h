@@ -314,6 +314,12 @@ int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable);
  * the default covers the padded orbitals with 16-byte vectors.  The kernels
  * stride over any block size; >= 128 is needed for the tensor-core flush. */
 int qmc_walkers_set_threads(qmc_walkers* w, int threads);
+/* L2 prefetch of the next move's 16 spline-stencil rows while the current
+ * move runs (no reference counterpart).  AUTO: on while the batch's
+ * stencils in flight (16 rows x 4 npad coefficients per walker) stay within
+ * 32 MB of the 126 MB L2. */
+enum { QMC_PREFETCH_AUTO = 0, QMC_PREFETCH_OFF = 1, QMC_PREFETCH_ON = 2 };
+int qmc_walkers_set_prefetch(qmc_walkers* w, int mode);
 int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* tensor_cores);
 
 /* Batch groups (no reference counterpart: the reference's flex_ batch,

@@ -18,6 +18,7 @@ LAP_HXX, LAP_TRACE = 0, 1
 WF_DET, WF_J1, WF_J2, WF_ALL, WF_J3 = 1, 2, 4, 7, 8
 J3_PARAMS = 26
 RNG_DEVICE, RNG_HOST = 0, 1
+PREFETCH_AUTO, PREFETCH_OFF, PREFETCH_ON = 0, 1, 2
 NIO_REF32, NIO_PRIM4 = 0, 1
 NIO_QUIRK_UNIT_IONS, NIO_QUIRK_ONE_GROUP = 1, 2
 MAX_FUNCTOR_COEFS = 32
@@ -127,6 +128,7 @@ PRODUCT_ONLY = {
     'detengine_set_tensor_cores': (I, [P, I]),
     'walkers_set_tensor_cores': (I, [P, I]),
     'walkers_set_threads': (I, [P, I]),
+    'walkers_set_prefetch': (I, [P, I]),
     'local_kinetic': (I, [P, PD]),
     'walkers_checkpoint_bytes': (I, [P, C.POINTER(C.c_size_t)]),
     'walkers_checkpoint': (I, [P, P, C.c_size_t]),
@@ -156,7 +158,7 @@ PRODUCT_ONLY = {
     'walkers_phase_times': (I, [P, PD, PI]),
 }
 PHASES = ['random', 'getInvRow', 'spo+det dots', 'jastrow sums', 'reduce+ratio', 'acceptRow', 'woodbury flush',
-          'J2 accept', 'position', 'completeUpdates', 'evaluateGL']
+          'J2 accept', 'position', 'completeUpdates', 'evaluateGL', 'move setup']
 
 
 def bind(lib, prefix, extra=None):

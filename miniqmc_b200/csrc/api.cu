@@ -713,6 +713,14 @@ int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count)
   *count = w->launches;
   return QMC_OK;
 }
+int qmc_walkers_set_prefetch(qmc_walkers* w, int mode)
+{
+  if (!w || mode < QMC_PREFETCH_AUTO || mode > QMC_PREFETCH_ON)
+    return fail(QMC_ERR_ARG, "bad prefetch mode");
+  w->prefetch_mode = mode;
+  return QMC_OK;
+}
+
 int qmc_walkers_set_threads(qmc_walkers* w, int threads)
 {
   if (!w)
@@ -1238,7 +1246,8 @@ SweepTask sweep_task(qmc_walkers* w, int first_block)
   task.tc          = w->use_tc ? 1 : 0;
   // next-move L2 prefetch only while the batch's in-flight stencils (16 rows
   // of 4 npad coefficients per walker) stay well inside the 126 MB L2
-  task.prefetch = (double)w->dw.W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8) <= 32.0e6;
+  task.prefetch = w->prefetch_mode == QMC_PREFETCH_ON ||
+      (w->prefetch_mode == QMC_PREFETCH_AUTO && (double)w->dw.W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8) <= 32.0e6);
   return task;
 }
 

@@ -41,6 +41,11 @@ template <typename T> struct SysSmem
   T mi_scale2;
   FunctorT<T> j1[QMC_MAX_ION_GROUPS], j2uu, j2ud;
   T j3cut[QMC_MAX_ION_GROUPS]; // J3 ion cutoff per species
+  // orbital cell and spline grid, for locating a move's stencil without
+  // global loads
+  double spoG[9], sdinv[3];
+  long long sstride[3];
+  int sgrid[3];
   int gfirst[QMC_MAX_ION_GROUPS], glast[QMC_MAX_ION_GROUPS];
   int n_groups, n_ions, n_elec, n_up, norb, npad, comp, lap_mode;
 };
@@ -195,8 +200,15 @@ template <typename T> __device__ void load_sys(const DevSystem* __restrict__ s, 
   const int tid = threadIdx.x;
   if (tid < 9)
   {
-    ss.rb[tid] = (T)s->rb[tid];
-    ss.gb[tid] = (T)s->gb[tid];
+    ss.rb[tid]   = (T)s->rb[tid];
+    ss.gb[tid]   = (T)s->gb[tid];
+    ss.spoG[tid] = s->spoG[tid];
+  }
+  if (tid < 3)
+  {
+    ss.sdinv[tid]   = s->dinv[tid];
+    ss.sgrid[tid]   = s->grid[tid];
+    ss.sstride[tid] = tid == 0 ? s->xs : (tid == 1 ? s->ys : s->zs);
   }
   if (tid < 24)
     ss.cn[tid] = (T)s->corners[tid];
@@ -313,79 +325,66 @@ template <typename T> __device__ __forceinline__ T functor_v(const FunctorT<T>& 
 }
 
 // --------------------------------------------------------- B-spline SPO --
-// computeLocationAndFractional + compute_prefactors for a Cartesian point
-// (one thread).  Fractional coordinates are formed in FP64 in both forms.
-template <typename T> __device__ void spline_locate(const DevSystem* __restrict__ s, const double* pos, SplineSmem<T>& sp)
+// One dimension of computeLocationAndFractional + compute_prefactors: u is
+// the Cartesian point's fractional coordinate before wrapping (r . spoG
+// column d), formed in FP64 in both forms; returns the stencil corner's
+// offset along d and, when a is given, the weights a, da, d2a.
+template <typename T>
+__device__ __forceinline__ long long spline_dim(double u, double dinv, int grid, long long stride, T* a, T* da,
+                                                T* d2a)
 {
-  double u[3];
-  for (int d = 0; d < 3; ++d)
+  if (-DBL_EPSILON < u && u < 0)
+    u = 0.0;
+  else
+    u -= floor(u);
+  const double x = u * dinv;
+  int ind;
+  double t;
+  if (x < 0)
   {
-    u[d] = pos[0] * s->spoG[d] + pos[1] * s->spoG[3 + d] + pos[2] * s->spoG[6 + d];
-    if (-DBL_EPSILON < u[d] && u[d] < 0)
-      u[d] = 0.0;
-    else
-      u[d] -= floor(u[d]);
+    ind = 0;
+    t   = 0.0;
   }
-  long long base = 0;
-  const long long strides[3] = {s->xs, s->ys, s->zs};
-  for (int d = 0; d < 3; ++d)
+  else
   {
-    const double x = u[d] * s->dinv[d];
-    int ind;
-    double t;
-    if (x < 0)
+    const double ip = floor(x);
+    t               = x - ip;
+    ind             = (int)ip;
+    if (ind > grid - 1)
     {
-      ind = 0;
-      t   = 0.0;
+      ind = grid - 1;
+      t   = 1.0 - DBL_EPSILON;
     }
-    else
-    {
-      const double ip = floor(x);
-      t               = x - ip;
-      ind             = (int)ip;
-      if (ind > s->grid[d] - 1)
-      {
-        ind = s->grid[d] - 1;
-        t   = 1.0 - DBL_EPSILON;
-      }
-    }
-    base += (long long)ind * strides[d];
-    sp.a[d][0]   = (T)(((-1.0 / 6.0 * t + 3.0 / 6.0) * t + -3.0 / 6.0) * t + 1.0 / 6.0);
-    sp.a[d][1]   = (T)(((3.0 / 6.0 * t + -6.0 / 6.0) * t + 0.0 / 6.0) * t + 4.0 / 6.0);
-    sp.a[d][2]   = (T)(((-3.0 / 6.0 * t + 3.0 / 6.0) * t + 3.0 / 6.0) * t + 1.0 / 6.0);
-    sp.a[d][3]   = (T)(((1.0 / 6.0 * t + 0.0 / 6.0) * t + 0.0 / 6.0) * t + 0.0 / 6.0);
-    sp.da[d][0]  = (T)((-0.5 * t + 1.0) * t + -0.5);
-    sp.da[d][1]  = (T)((1.5 * t + -2.0) * t + 0.0);
-    sp.da[d][2]  = (T)((-1.5 * t + 1.0) * t + 0.5);
-    sp.da[d][3]  = (T)((0.5 * t + 0.0) * t + 0.0);
-    sp.d2a[d][0] = (T)(-1.0 * t + 1.0);
-    sp.d2a[d][1] = (T)(3.0 * t + -2.0);
-    sp.d2a[d][2] = (T)(-3.0 * t + 1.0);
-    sp.d2a[d][3] = (T)(1.0 * t + 0.0);
   }
-  sp.base = base;
+  if (a)
+  {
+    a[0]   = (T)(((-1.0 / 6.0 * t + 3.0 / 6.0) * t + -3.0 / 6.0) * t + 1.0 / 6.0);
+    a[1]   = (T)(((3.0 / 6.0 * t + -6.0 / 6.0) * t + 0.0 / 6.0) * t + 4.0 / 6.0);
+    a[2]   = (T)(((-3.0 / 6.0 * t + 3.0 / 6.0) * t + 3.0 / 6.0) * t + 1.0 / 6.0);
+    a[3]   = (T)(((1.0 / 6.0 * t + 0.0 / 6.0) * t + 0.0 / 6.0) * t + 0.0 / 6.0);
+    da[0]  = (T)((-0.5 * t + 1.0) * t + -0.5);
+    da[1]  = (T)((1.5 * t + -2.0) * t + 0.0);
+    da[2]  = (T)((-1.5 * t + 1.0) * t + 0.5);
+    da[3]  = (T)((0.5 * t + 0.0) * t + 0.0);
+    d2a[0] = (T)(-1.0 * t + 1.0);
+    d2a[1] = (T)(3.0 * t + -2.0);
+    d2a[2] = (T)(-3.0 * t + 1.0);
+    d2a[3] = (T)(1.0 * t + 0.0);
+  }
+  return (long long)ind * stride;
 }
 
-// element offset of the stencil corner for a Cartesian point (the index part
-// of spline_locate, used to prefetch the next move's coefficients)
-__device__ inline long long spline_base(const DevSystem* __restrict__ s, const double* pos)
+// the whole stencil location of a Cartesian point (one thread)
+template <typename T> __device__ void spline_locate(const DevSystem* __restrict__ s, const double* pos, SplineSmem<T>& sp)
 {
-  long long base             = 0;
   const long long strides[3] = {s->xs, s->ys, s->zs};
+  long long base             = 0;
   for (int d = 0; d < 3; ++d)
   {
-    double u = pos[0] * s->spoG[d] + pos[1] * s->spoG[3 + d] + pos[2] * s->spoG[6 + d];
-    if (-DBL_EPSILON < u && u < 0)
-      u = 0.0;
-    else
-      u -= floor(u);
-    const double x = u * s->dinv[d];
-    int ind        = x < 0 ? 0 : (int)floor(x);
-    if (ind > s->grid[d] - 1)
-      ind = s->grid[d] - 1;
-    base += (long long)ind * strides[d];
+    const double u = pos[0] * s->spoG[d] + pos[1] * s->spoG[3 + d] + pos[2] * s->spoG[6 + d];
+    base += spline_dim<T>(u, s->dinv[d], s->grid[d], strides[d], sp.a[d], sp.da[d], sp.d2a[d]);
   }
-  return base;
+  sp.base = base;
 }
 
 // L2 prefetch of `bytes` (multiple of 16) at a 16-byte aligned address,
@@ -1046,8 +1045,8 @@ template <typename T> __device__ void rng_substep(const WV<T>& wv, int N)
 // keep the smaller register footprint)
 template <typename T, bool HAS_J3 = true>
 __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys, const WV<T>& wv, MoveSmem& m,
-                        SplineSmem<T>& sp, const T* __restrict__ ions, int iel, double accept_thr, double ur,
-                        const double* dlt, double* trace, T* smem, bool has_next)
+                        SplineSmem<T>& sp, const T* __restrict__ ions, int iel, double accept_thr, const double* urp,
+                        const double* dlt, double* trace, T* smem, bool prefetch_next)
 {
   using Vt         = typename Vec16<T>::type;
   constexpr int VW = Vec16<T>::width;
@@ -1056,37 +1055,59 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
   const bool J3 = HAS_J3 && (ss.comp & QMC_WF_J3);
   const int s = iel < ss.n_up ? 0 : 1, r = iel - (s ? ss.n_up : 0);
   const int npad = wv.npad, nvec = npad / VW;
-  if (tid == 0)
+  if (tid < 32)
   {
-    for (int c = 0; c < 3; ++c)
+    // warp 0 sets the move up: lanes 0-2 take the three dimensions of this
+    // move's proposed position and stencil, lanes 3-5 those of the next
+    // electron's when its stencil is prefetched (its current position does
+    // not change during this move); one round trip for the positions, the
+    // cell constants from shared memory
+    const int lane = tid, d = lane % 3;
+    const bool cur = lane < 3, nxt = lane >= 3 && lane < 6 && prefetch_next;
+    double r = 0.0, pn = 0.0, urv = 0.0;
+    if (cur || nxt)
     {
-      m.pos_old[c] = wv.R[3 * iel + c];
-      m.pos_new[c] = m.pos_old[c] + dlt[c];
+      r  = wv.R[3 * (cur ? iel : iel + 1) + d];
+      pn = r + dlt[(cur ? 0 : 3) + d];
     }
-    m.accept = ur < accept_thr;
-    m.dc     = DET ? wv.dcount[s] : 0;
-    if (DET)
+    if (lane == 0)
+      urv = urp[0];
+    const int g0    = lane < 3 ? 0 : 3;
+    const double p0 = __shfl_sync(0xffffffffu, pn, g0), p1 = __shfl_sync(0xffffffffu, pn, g0 + 1),
+                 p2 = __shfl_sync(0xffffffffu, pn, g0 + 2);
+    const double u  = p0 * ss.spoG[d] + p1 * ss.spoG[3 + d] + p2 * ss.spoG[6 + d];
+    long long b     = 0;
+    if (DET && (cur || nxt))
+      b = spline_dim<T>(u, ss.sdinv[d], ss.sgrid[d], ss.sstride[d], cur ? sp.a[d] : nullptr,
+                        cur ? sp.da[d] : nullptr, cur ? sp.d2a[d] : nullptr);
+    const long long bc = __shfl_sync(0xffffffffu, b, 0) + __shfl_sync(0xffffffffu, b, 1) + __shfl_sync(0xffffffffu, b, 2);
+    const long long bn = __shfl_sync(0xffffffffu, b, 3) + __shfl_sync(0xffffffffu, b, 4) + __shfl_sync(0xffffffffu, b, 5);
+    if (cur)
     {
-      spline_locate(sys, m.pos_new, sp);
-      if (has_next)
+      m.pos_old[d] = r;
+      m.pos_new[d] = pn;
+    }
+    if (lane == 0)
+    {
+      m.accept = urv < accept_thr;
+      m.dc     = DET ? wv.dcount[s] : 0;
+      if (DET)
       {
-        // the next electron's current position does not change during this
-        // move, so its proposed position and stencil are known now
-        double pn[3];
-        for (int c = 0; c < 3; ++c)
-          pn[c] = wv.R[3 * (iel + 1) + c] + dlt[3 + c];
-        m.next_base = spline_base(sys, pn);
+        sp.base = bc;
+        if (prefetch_next)
+          m.next_base = bn;
       }
     }
   }
   __syncthreads();
+  phase_mark(m, PH_SETUP);
   // this move's 16 stencil rows start towards L2 now, so that their HBM
   // latency overlaps getInvRow (they may already be there when the next
   // move was prefetched during the previous one)
   if (DET && tid >= 32 && tid < 48)
     prefetch_l2((const T*)sys->coefs + sp.base + ((tid - 32) >> 2) * sys->xs + ((tid - 32) & 3) * sys->ys,
                 (unsigned)(4 * sys->zs * sizeof(T)));
-  if (DET && has_next && tid < 18)
+  if (DET && prefetch_next && tid < 18)
   {
     // warm L2 with the next move's 16 stencil rows and its inverse and
     // gradient rows while this move runs

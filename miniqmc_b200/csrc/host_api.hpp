@@ -44,6 +44,7 @@ struct qmc_walkers_s
   int64_t launches  = 0;
   int64_t steps_done = 0; // MC steps swept by this batch over all calls
   bool ratio_moves   = false; // a ratio-only verb ran since the last evaluateLog
+  int prefetch_mode  = QMC_PREFETCH_AUTO;
   int64_t nlpp_calls = 0; // NonLocalPP sphere rotations drawn so far
   qmc::SweepTask* d_task = nullptr;
   double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;

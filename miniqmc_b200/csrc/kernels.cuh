@@ -20,6 +20,7 @@ enum Phase
   PH_POSITION,      // ParticleSet::acceptMove
   PH_COMPLETE,      // completeUpdates ("Complete Updates")
   PH_GL,            // evaluateGL ("Kinetic Energy")
+  PH_SETUP,         // a move's serial set-up: positions, stencil location
   NPHASE
 };
 

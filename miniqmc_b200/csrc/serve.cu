@@ -68,8 +68,11 @@ struct TaskList
       h.push_back(t);
     }
     // the next-move L2 prefetch only while all walkers' stencils fit well
-    for (auto& t : h)
-      t.prefetch = inflight <= 32.0e6;
+    for (size_t i = 0; i < h.size(); ++i)
+    {
+      const int mode = batches[i]->prefetch_mode;
+      h[i].prefetch  = mode == QMC_PREFETCH_ON || (mode == QMC_PREFETCH_AUTO && inflight <= 32.0e6);
+    }
     if (n)
       CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(SweepTask), cudaMemcpyHostToDevice, st));
     return QMC_OK;

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
         load_binv(1);
       }
       double* tr = task.trace ? task.trace + (((size_t)w * n_substeps + l) * N + iel) * 8 : nullptr;
-      do_move<T, HAS_J3>(ss, sys, wv, m, sp, ions, iel, accept_thr, urp[iel], dp + 3 * iel, tr, smem,
+      do_move<T, HAS_J3>(ss, sys, wv, m, sp, ions, iel, accept_thr, urp + iel, dp + 3 * iel, tr, smem,
                          task.prefetch && iel + 1 < N);
       acc += m.accept ? 1 : 0;
       __syncthreads(); // m.accept is rewritten by the next move
