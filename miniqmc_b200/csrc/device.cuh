@@ -718,38 +718,55 @@ __device__ void j1_value(const SysSmem<T>& ss, const T* __restrict__ ions, const
   }
 }
 
+// J2 pair lists: each warp scans its electrons with the exact cutoff test
+// (beyond_cutoff) and compacts the candidates into its slice of `wlist`
+// (J2_SCAN chunks of 32 electrons per round), then all lanes work through
+// the list.  Only a few per cent of the pairs are within the cutoff in the
+// NiO cells, so this replaces a divergent branch on most warp steps with one
+// dense pass.
+constexpr int J2_SCAN = 8;
+// shared-memory bytes of the per-warp candidate lists (up to 8 warps)
+__host__ __device__ constexpr size_t j2_list_bytes() { return (size_t)8 * 32 * J2_SCAN * sizeof(int); }
+
 // partial J2 sums over the electrons for electron iel moved to pos:
 // sum u, sum du*dr (TwoBodyJastrow::ratioGrad with the move row, flip = iel)
 template <typename T, typename A>
 __device__ void j2_partials(const SysSmem<T>& ss, const T* __restrict__ Rs, int Npad, int iel, const double* pos,
-                            A* part, bool grads)
+                            A* part, bool grads, int* wlist)
 {
   const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];
   const int gi = iel < ss.n_up ? 0 : 1;
-  const int N = ss.n_elec, NT = blockDim.x;
-  for (int j0 = threadIdx.x; j0 < N; j0 += 4 * NT)
+  const int N = ss.n_elec, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  int* lst             = wlist + wid * 32 * J2_SCAN;
+  const int nchunks    = (N + 31) >> 5;
+  for (int c0 = wid; c0 < nchunks; c0 += nw * J2_SCAN)
   {
-    T rx[4], ry[4], rz[4];
+    int cnt = 0;
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int r = 0; r < J2_SCAN; ++r)
     {
-      const int j   = j0 + u * NT;
-      const bool ok = j < N;
-      rx[u]         = ok ? Rs[j] : T(0);
-      ry[u]         = ok ? Rs[Npad + j] : T(0);
-      rz[u]         = ok ? Rs[2 * Npad + j] : T(0);
+      const int j = ((c0 + r * nw) << 5) + lane;
+      bool in     = false;
+      if (j < N && j != iel)
+      {
+        const T flip = j < iel ? T(1) : T(-1);
+        const T dx = (Rs[j] - px) * flip, dy = (Rs[Npad + j] - py) * flip, dz = (Rs[2 * Npad + j] - pz) * flip;
+        const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+        in = !beyond_cutoff(dx, dy, dz, ss.gb, ss.mi_scale2, f.cutoff * f.cutoff);
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, in);
+      if (in)
+        lst[cnt + __popc(b & below)] = j;
+      cnt += __popc(b);
     }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
+    __syncwarp();
+    for (int q = lane; q < cnt; q += 32)
     {
-      const int j = j0 + u * NT;
-      if (j >= N || j == iel)
-        continue;
+      const int j  = lst[q];
       const T flip = j < iel ? T(1) : T(-1);
-      T dx = (rx[u] - px) * flip, dy = (ry[u] - py) * flip, dz = (rz[u] - pz) * flip;
+      T dx = (Rs[j] - px) * flip, dy = (Rs[Npad + j] - py) * flip, dz = (Rs[2 * Npad + j] - pz) * flip;
       const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
-      if (beyond_cutoff(dx, dy, dz, ss.gb, ss.mi_scale2, f.cutoff * f.cutoff))
-        continue;
       const T r = min_image(dx, dy, dz, ss.rb, ss.gb, ss.cn);
       if (r < f.cutoff)
       {
@@ -767,87 +784,84 @@ __device__ void j2_partials(const SysSmem<T>& ss, const T* __restrict__ Rs, int 
           part[0] += (A)functor_v(f, r);
       }
     }
+    __syncwarp(); // the list is rewritten by the next round
   }
 }
 
 // TwoBodyJastrow::acceptMove: update every electron's Uat, dUat, d2Uat with
-// the old (setActive) and new (move) rows of electron iel.  Block-wide.
+// the old (setActive) and new (move) rows of electron iel.  A pair beyond
+// the cutoff at both the old and the new position adds exact zeros to Uat,
+// dUat and d2Uat (TwoBodyJastrow.h:307-353 updates every entry with
+// new - old), so the scan keeps the pairs within the cutoff at either
+// position and only those entries are read and written.  Block-wide.
 template <typename T>
-__device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, int iel)
+__device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, int iel, int* wlist)
 {
   const T ox = (T)m.pos_old[0], oy = (T)m.pos_old[1], oz = (T)m.pos_old[2];
   const T nx = (T)m.pos_new[0], ny = (T)m.pos_new[1], nz = (T)m.pos_new[2];
   const int gi = iel < ss.n_up ? 0 : 1;
   const int Npad = wv.Npad, N = wv.N;
   const T* Rs = wv.Rs;
-  const int NT = blockDim.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  int* lst             = wlist + wid * 32 * J2_SCAN;
+  const int nchunks    = (N + 31) >> 5;
   T part[4] = {T(0), T(0), T(0), T(0)};
-  // a pair beyond the cutoff at both the old and the new position adds
-  // exact zeros to Uat, dUat and d2Uat (TwoBodyJastrow.h:307-353 updates
-  // every entry with new - old), so only pairs within the cutoff at either
-  // position are written back (about 3 % of the electrons in NiO cells);
-  // the loads are still issued up front so that one memory round trip
-  // covers the whole batch
-  for (int j0 = threadIdx.x; j0 < N; j0 += 2 * NT)
+  for (int c0 = wid; c0 < nchunks; c0 += nw * J2_SCAN)
   {
-    T rx[2], ry[2], rz[2], ua[2], la[2], g0[2], g1[2], g2[2];
+    int cnt = 0;
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
+    for (int r = 0; r < J2_SCAN; ++r)
     {
-      const int j   = j0 + u * NT;
-      const bool ok = j < N;
-      rx[u]         = ok ? Rs[j] : T(0);
-      ry[u]         = ok ? Rs[Npad + j] : T(0);
-      rz[u]         = ok ? Rs[2 * Npad + j] : T(0);
-      ua[u]         = ok ? wv.Uat[j] : T(0);
-      la[u]         = ok ? wv.d2Uat[j] : T(0);
-      g0[u]         = ok ? wv.dUat[j] : T(0);
-      g1[u]         = ok ? wv.dUat[N + j] : T(0);
-      g2[u]         = ok ? wv.dUat[2 * N + j] : T(0);
+      const int j = ((c0 + r * nw) << 5) + lane;
+      bool in     = false;
+      if (j < N && j != iel)
+      {
+        const T flip = j < iel ? T(1) : T(-1);
+        const T rx = Rs[j], ry = Rs[Npad + j], rz = Rs[2 * Npad + j];
+        const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
+        const T rc2 = f.cutoff * f.cutoff;
+        in = !beyond_cutoff((rx - ox) * flip, (ry - oy) * flip, (rz - oz) * flip, ss.gb, ss.mi_scale2, rc2) ||
+            !beyond_cutoff((rx - nx) * flip, (ry - ny) * flip, (rz - nz) * flip, ss.gb, ss.mi_scale2, rc2);
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, in);
+      if (in)
+        lst[cnt + __popc(b & below)] = j;
+      cnt += __popc(b);
     }
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
+    __syncwarp();
+    for (int q = lane; q < cnt; q += 32)
     {
-      const int j = j0 + u * NT;
-      if (j >= N || j == iel)
-        continue;
+      const int j  = lst[q];
       const T flip = j < iel ? T(1) : T(-1);
+      const T rx = Rs[j], ry = Rs[Npad + j], rz = Rs[2 * Npad + j];
+      const T ua = wv.Uat[j], la = wv.d2Uat[j], g0 = wv.dUat[j], g1 = wv.dUat[N + j], g2 = wv.dUat[2 * N + j];
       const FunctorT<T>& f = (gi == (j < ss.n_up ? 0 : 1)) ? ss.j2uu : ss.j2ud;
-      const T rc2 = f.cutoff * f.cutoff;
-      T odx = (rx[u] - ox) * flip, ody = (ry[u] - oy) * flip, odz = (rz[u] - oz) * flip;
-      T ndx = (rx[u] - nx) * flip, ndy = (ry[u] - ny) * flip, ndz = (rz[u] - nz) * flip;
-      const bool o_in = !beyond_cutoff(odx, ody, odz, ss.gb, ss.mi_scale2, rc2);
-      const bool n_in = !beyond_cutoff(ndx, ndy, ndz, ss.gb, ss.mi_scale2, rc2);
-      if (!o_in && !n_in)
-        continue;
+      T odx = (rx - ox) * flip, ody = (ry - oy) * flip, odz = (rz - oz) * flip;
+      T ndx = (rx - nx) * flip, ndy = (ry - ny) * flip, ndz = (rz - nz) * flip;
       T uo = 0, duo = 0, d2uo = 0, un = 0, dun = 0, d2un = 0;
-      if (o_in)
-      {
-        const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
-        if (ro < f.cutoff)
-          functor_vgl(f, ro, uo, duo, d2uo);
-      }
+      const T ro = min_image(odx, ody, odz, ss.rb, ss.gb, ss.cn);
+      if (ro < f.cutoff)
+        functor_vgl(f, ro, uo, duo, d2uo);
       odx *= flip, ody *= flip, odz *= flip;
-      if (n_in)
-      {
-        const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
-        if (rn < f.cutoff)
-          functor_vgl(f, rn, un, dun, d2un);
-      }
+      const T rn = min_image(ndx, ndy, ndz, ss.rb, ss.gb, ss.cn);
+      if (rn < f.cutoff)
+        functor_vgl(f, rn, un, dun, d2un);
       ndx *= flip, ndy *= flip, ndz *= flip;
       const T newl = d2un + T(2) * dun;
       const T dl   = d2uo + T(2) * duo - newl;
-      wv.Uat[j]   = ua[u] + (un - uo);
-      wv.d2Uat[j] = la[u] + dl;
+      wv.Uat[j]   = ua + (un - uo);
+      wv.d2Uat[j] = la + dl;
       part[0] -= newl;
       const T ng0 = dun * ndx, ng1 = dun * ndy, ng2 = dun * ndz;
-      wv.dUat[j]         = g0[u] - (ng0 - duo * odx);
-      wv.dUat[N + j]     = g1[u] - (ng1 - duo * ody);
-      wv.dUat[2 * N + j] = g2[u] - (ng2 - duo * odz);
+      wv.dUat[j]         = g0 - (ng0 - duo * odx);
+      wv.dUat[N + j]     = g1 - (ng1 - duo * ody);
+      wv.dUat[2 * N + j] = g2 - (ng2 - duo * odz);
       part[1] += ng0;
       part[2] += ng1;
       part[3] += ng2;
     }
+    __syncwarp();
   }
   {
     double dpart[4] = {(double)part[0], (double)part[1], (double)part[2], (double)part[3]};
@@ -856,11 +870,11 @@ __device__ void j2_accept(const SysSmem<T>& ss, const WV<T>& wv, MoveSmem& m, in
   if (threadIdx.x == 0)
   {
     wv.jlog[1] += (double)wv.Uat[iel] - m.curUat;
-    wv.Uat[iel]        = (T)m.curUat;
-    wv.dUat[iel]       = (T)m.sums[1];
-    wv.dUat[N + iel]   = (T)m.sums[2];
+    wv.Uat[iel]          = (T)m.curUat;
+    wv.dUat[iel]         = (T)m.sums[1];
+    wv.dUat[N + iel]     = (T)m.sums[2];
     wv.dUat[2 * N + iel] = (T)m.sums[3];
-    wv.d2Uat[iel]      = (T)m.sums[0];
+    wv.d2Uat[iel]        = (T)m.sums[0];
   }
   __syncthreads();
 }
@@ -1186,7 +1200,7 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
   if (J1)
     j1_partials(ss, ions, m.pos_new, part + 7);
   if (J2)
-    j2_partials(ss, wv.Rs, wv.Npad, iel, m.pos_new, part + 12, true);
+    j2_partials(ss, wv.Rs, wv.Npad, iel, m.pos_new, part + 12, true, reinterpret_cast<int*>(smem));
   phase_mark(m, PH_JASTROW);
   {
     double dpart[16];
@@ -1264,7 +1278,7 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
       wv.Lap[iel] = (T)m.curLap;
     }
     if (J2)
-      j2_accept(ss, wv, m, iel);
+      j2_accept(ss, wv, m, iel, reinterpret_cast<int*>(smem));
     if (J3)
       j3_accept(ss, sys, wv, m, *reinterpret_cast<J3Smem<T>*>(smem), ions, iel);
     __syncthreads();

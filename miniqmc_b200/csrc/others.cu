@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
         j1_value(ss, ions, m.pos_new, part + 7);
     }
     if (J2)
-      j2_partials(ss, wv.Rs, wv.Npad, iat, m.pos_new, part + 12, grads);
+      j2_partials(ss, wv.Rs, wv.Npad, iat, m.pos_new, part + 12, grads, reinterpret_cast<int*>(dyn));
     if (J3)
     {
       double jp[4] = {0.0, 0.0, 0.0, 0.0};
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
       if (tid == 0)
         m.curUat = ms->j2_curUat;
       __syncthreads();
-      j2_accept(ss, wv, m, iat);
+      j2_accept(ss, wv, m, iat, reinterpret_cast<int*>(dyn));
     }
     if (J3)
       j3_accept(ss, sys, wv, m, J, ions, iat);

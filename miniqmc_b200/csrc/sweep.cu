@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   long long acc = 0;
   const bool DET = ss.comp & QMC_WF_DET;
   // dynamic shared memory: [Binv of the active spin (k x k FP64)][flush
-  // scratch, or the J3 move scratch between flushes]
+  // scratch, or between flushes the J2 candidate lists / the J3 move scratch]
   const int k = wv.k;
   T* smem     = reinterpret_cast<T*>(dyn + bsm_bytes(k));
   auto load_binv = [&](int spin) {
@@ -153,7 +153,7 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
     return cudaErrorInvalidValue;
   if (fp32)
   {
-    size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<float>(threads, max_k);
+    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<float>(threads, max_k), j2_list_bytes());
     if (tc && tc_flush_smem_bytes() > bytes)
       bytes = tc_flush_smem_bytes(); // the tiles overlay the cached Binv
     if (j3)
@@ -162,7 +162,7 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
   }
   else
   {
-    size_t bytes = bsm_bytes(max_k) + flush_smem_bytes_for<double>(threads, max_k);
+    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<double>(threads, max_k), j2_list_bytes());
     if (j3)
       bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<double>));
     launch_sweep_t<double>(j3, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, 0);
