@@ -537,6 +537,7 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
 // A^{-1}[a][b] = M[piv[a]][pinv[b]], so psiM[i][j] = M[piv[j]][pinv[i]];
 // the sign of det A is the pivots' sign times the parity of piv.
 constexpr int GJB_B = 32;      // panel width
+constexpr int GJB_U = 8;       // rows per warp and pass of the rank-32 update
 constexpr int GJB_FS = GJB_B + 1; // padded panel row (conflict-free row-per-thread access)
 __host__ __device__ constexpr size_t gjb_smem_bytes(int n)
 {
@@ -675,14 +676,14 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
 #pragma unroll
       for (int k = 0; k < GJB_B; ++k)
         r[k] = R[k * 32 + lane];
-      // warp per row, lane per column; 4 rows per pass so that their loads
-      // are in flight together
+      // warp per row, lane per column; GJB_U rows per pass so that their
+      // loads are in flight together and their FMA chains interleave
       if (lane < jw)
-        for (int i0 = wid; i0 < n; i0 += 4 * nw)
+        for (int i0 = wid; i0 < n; i0 += GJB_U * nw)
         {
-          double acc[4];
+          double acc[GJB_U];
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < GJB_U; ++u)
           {
             const int i = i0 + u * nw;
             const int c = i < n ? pinv[i] : c0;
@@ -691,13 +692,13 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
 #pragma unroll
           for (int k = 0; k < GJB_B; ++k)
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < GJB_U; ++u)
             {
               const int i = min(i0 + u * nw, n - 1);
               acc[u]      = fma(F[i * GJB_FS + k], r[k], acc[u]);
             }
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < GJB_U; ++u)
           {
             const int i = i0 + u * nw;
             if (i < n)
