@@ -283,6 +283,15 @@ typedef struct {
   double* logpsi;         /* optional [W] log|psi| after the last step         */
 } qmc_sweep_opts;
 int qmc_sweep(qmc_walkers* w, const qmc_sweep_opts* opts);
+/* One fused single-electron move of every walker of the batch, the body of
+ * the driver's loop (miniqmc.cpp:426-458): evalGrad, makeMove(iat,
+ * delta[w]), ratioGrad, the threshold accept ur[w] < accept, acceptMove or
+ * restore, the position update and the delayed-update bookkeeping (a
+ * Woodbury flush when the delay fills).  ur[W] and delta[W][3] are host
+ * arrays; accepted[W] (may be NULL) receives 1 or 0 per walker.  After the
+ * last electron of a substep call qmc_wf_complete_updates, and
+ * qmc_wf_evaluate_gl after the substeps, as the driver does. */
+int qmc_step(qmc_walkers* w, int iat, double accept, const double* ur, const double* delta, int* accepted);
 /* Asynchronous form for device-resident callers: no host copies, inputs
  * already on the device (QMC_RNG_DEVICE only); results stay on the device
  * until qmc_walkers_sync + qmc_sweep_results. */

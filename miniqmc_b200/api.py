@@ -321,6 +321,15 @@ class Walkers:
     def complete_updates(self):
         self.lib.call('wf_complete_updates', self.h)
 
+    def step(self, iat, accept, ur, delta):
+        """qmc_step: the fused move of electron iat for every walker; returns
+        the accept flags [W]."""
+        u = np.ascontiguousarray(ur, dtype=np.float64).reshape(self.W)
+        d = np.ascontiguousarray(delta, dtype=np.float64).reshape(self.W, 3)
+        acc = np.zeros(self.W, dtype=np.int32)
+        self.lib.call('step', self.h, iat, accept, _pd(u), _pd(d), _pi(acc))
+        return acc
+
     def evaluate_gl(self):
         G = np.zeros((self.W, self.N, 3))
         L = np.zeros((self.W, self.N))

@@ -151,6 +151,7 @@ PRODUCT_ONLY = {
     'server_stats': (I, [P, C.POINTER(C.c_size_t), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     'invert_transpose_noalloc': (I, [I, P, P, PD, PD, P]),
     'sweep_async': (I, [P, I, I, D, I]),
+    'step': (I, [P, I, D, PD, PD, PI]),
     'walkers_sync': (I, [P]),
     'sweep_results': (I, [P, C.POINTER(C.c_int64), PD]),
     'walkers_launch_count': (I, [P, C.POINTER(C.c_int64)]),

@@ -572,6 +572,7 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   st |= dalloc(L, B, &d.status, 1);
   st |= dalloc(L, B, &w->d_task, 1);
   st |= dalloc(L, B, &w->d_displ, W * 3);
+  st |= dalloc(L, B, &w->d_step, W * 4);
   st |= dalloc(L, B, &w->d_flags, W);
   d.lu = nullptr;
   if (st)
@@ -1057,6 +1058,31 @@ int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio)
   if (w)
     w->ratio_moves = true;
   return ratio_verb(w, VERB_RATIO, iat, ratio, nullptr);
+}
+
+int qmc_step(qmc_walkers* w, int iat, double accept, const double* ur, const double* delta, int* accepted)
+{
+  int st = check_iat(w, iat);
+  if (st)
+    return st;
+  if (!ur || !delta)
+    return fail(QMC_ERR_ARG, "null ur or delta");
+  const size_t W = w->dw.W;
+  std::vector<double> in(4 * W);
+  for (size_t i = 0; i < W; ++i)
+  {
+    in[4 * i] = ur[i];
+    for (int c = 0; c < 3; ++c)
+      in[4 * i + 1 + c] = delta[3 * i + c];
+  }
+  CK(cudaMemcpyAsync(w->d_step, in.data(), 4 * W * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  CK(launch_step(w->fp32, (w->sys->h.comp & QMC_WF_J3) != 0, w->sys->d, w->dw, iat, accept, w->d_step, w->d_flags,
+                 w->threads, w->stream));
+  w->launches++;
+  if (accepted)
+    CK(cudaMemcpyAsync(accepted, w->d_flags, W * sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
 }
 
 int qmc_wf_complete_updates(qmc_walkers* w)

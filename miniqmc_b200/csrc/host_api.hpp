@@ -50,6 +50,7 @@ struct qmc_walkers_s
   double* d_ur = nullptr, *d_delta = nullptr, *d_trace = nullptr;
   size_t cap_rng = 0, cap_trace = 0;
   double* d_displ = nullptr;
+  double* d_step  = nullptr; // [W][4] qmc_step inputs: ur, delta xyz
   int* d_flags    = nullptr;
   double* d_rows  = nullptr;
   size_t cap_rows = 0;

@@ -100,6 +100,10 @@ struct VerbArgs
   double* ab_r;
   double* ab_dr;
 };
+// one fused single-electron move of every walker (qmc_step): in = [W][4]
+// (ur, delta xyz) on the device, accepted flags into out [W]
+cudaError_t launch_step(bool fp32, bool j3, const DevSystem* sys, const DevWalkers& dw, int iel, double accept,
+                        const double* in, int* out, int threads, cudaStream_t st);
 cudaError_t launch_verb(bool fp32, const DevSystem* sys, const DevWalkers& dw, const VerbArgs& a, int threads,
                         int max_k, cudaStream_t st);
 

@@ -120,6 +120,69 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   }
 }
 
+// qmc_step: the fused move of one electron for every walker, with the same
+// device code as one iteration of the sweep (do_move).  The inverse's
+// delayed block stays in global memory between calls and flushes run on the
+// CUDA cores, as in the per-call verbs.
+template <typename T, bool HAS_J3>
+__global__ void __launch_bounds__(256, 3) step_kernel(const DevSystem* __restrict__ sys, DevWalkers dw, int iel,
+                                                   double accept_thr, const double* __restrict__ in,
+                                                   int* __restrict__ out)
+{
+  __shared__ SysSmem<T> ss;
+  __shared__ MoveSmem m;
+  __shared__ SplineSmem<T> sp;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  load_sys(sys, ss);
+  const int w       = blockIdx.x;
+  const WV<T> wv    = make_wv<T>(dw, w);
+  const T* ions     = (const T*)sys->ion_soa;
+  const double* inw = in + (size_t)4 * w;
+  if (threadIdx.x == 0)
+  {
+    m.tc_on    = 0;
+    m.tc_abort = 0;
+    m.timing   = 0;
+  }
+  do_move<T, HAS_J3>(ss, sys, wv, m, sp, ions, iel, accept_thr, inw, inw + 1, nullptr, reinterpret_cast<T*>(dyn),
+                     false);
+  if (threadIdx.x == 0)
+  {
+    out[w] = m.accept;
+    dw.accepted[w] += m.accept;
+  }
+}
+
+template <typename T> static void launch_step_t(bool j3, const DevSystem* sys, const DevWalkers& dw, int iel,
+                                                double accept, const double* in, int* out, int threads,
+                                                cudaStream_t st)
+{
+  const size_t bytes =
+      std::max(std::max(flush_smem_bytes<T>(), sizeof(J3Smem<T>)), j2_list_bytes() + sizeof(double));
+  if (j3)
+  {
+    cudaFuncSetAttribute(step_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    step_kernel<T, true><<<dw.W, threads, bytes, st>>>(sys, dw, iel, accept, in, out);
+  }
+  else
+  {
+    cudaFuncSetAttribute(step_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    step_kernel<T, false><<<dw.W, threads, bytes, st>>>(sys, dw, iel, accept, in, out);
+  }
+}
+
+cudaError_t launch_step(bool fp32, bool j3, const DevSystem* sys, const DevWalkers& dw, int iel, double accept,
+                        const double* in, int* out, int threads, cudaStream_t st)
+{
+  if (dw.k > MAXK)
+    return cudaErrorInvalidValue;
+  if (fp32)
+    launch_step_t<float>(j3, sys, dw, iel, accept, in, out, threads, st);
+  else
+    launch_step_t<double>(j3, sys, dw, iel, accept, in, out, threads, st);
+  return cudaGetLastError();
+}
+
 template <typename T, bool HAS_J3> static void set_smem_attr(size_t bytes)
 {
   static size_t done = 0;

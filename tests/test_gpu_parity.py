@@ -209,6 +209,33 @@ def test_verbs(delay):
     assert rel_err(gw.components(), ow.components()) < RTOL64
 
 
+@pytest.mark.parametrize('prec,tol', [(capi.PREC_FP64, 1e-10), (capi.PREC_MIXED, 1e-4)])
+def test_step_entry_point_matches_sweep(prec, tol):
+    """qmc_step, one fused single-electron move of the batch per call, over
+    every electron of a substep followed by completeUpdates and evaluateGL
+    gives the fused sweep's walkers on the same streams: the same accept
+    flags, log values within the form's bound (the sweep flushes the up
+    determinant at the spin boundary, the steps at completeUpdates)."""
+    W = 2
+    seeds = H.oracle_primes(W)
+    g1, _ = H.make_pair(precision=prec, walkers=W, delay=4, seeds=seeds)
+    g2, _ = H.make_pair(precision=prec, walkers=W, delay=4, seeds=seeds)
+    if prec == capi.PREC_MIXED:
+        H.product().call('walkers_set_tensor_cores', g1.h, 0)
+    g1.evaluate_log()
+    g2.evaluate_log()
+    ur, de = H.host_streams(seeds, g1.N, 1, 1)
+    r1 = g1.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    flags = np.zeros((W, g2.N), dtype=np.int32)
+    for iel in range(g2.N):
+        flags[:, iel] = g2.step(iel, 0.5, ur[0, :, 0, iel], de[0, :, 0, iel])
+    g2.complete_updates()
+    _, _, lp2 = g2.evaluate_gl()
+    assert np.array_equal(flags, r1['trace'][0, :, 0, :, 7].astype(np.int32))
+    assert elem_rel(lp2, r1['logpsi']).max() < tol
+    assert np.max(np.abs(g1.positions() - g2.positions())) == 0.0
+
+
 @pytest.mark.parametrize('last', ['ratio', 'ratio_grad'])
 def test_evaluate_gl_after_ratio_only_move(last):
     """DiracDeterminant::evaluateGL re-evaluates the orbital derivative rows
