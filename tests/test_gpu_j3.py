@@ -241,3 +241,22 @@ def test_j3_nlpp_mixed():
     m = int(ng[0])
     e = elem_rel(rg[:m], ro[:m])
     assert np.median(e) < 1e-4 and np.percentile(e, 99) < 1e-2, (np.median(e), np.percentile(e, 99))
+
+
+def test_j3_capacity_is_reported():
+    """A three-body cutoff of 30 bohr on the NiO-128 cell puts every electron
+    inside every ion's cutoff: more than the 128 a list holds, and more than
+    64 ions around a point.  evaluateLog reports QMC_ERR_CAPACITY; the lists
+    and the near-ion buffers are written only within their bounds."""
+    lib = H.product()
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=(4, 4, 2), grid=(6, 6, 6), components=capi.WF_J3,
+                          jastrow='synthetic')
+    big = lib.j3_functor(30.0, np.zeros(capi.J3_PARAMS))
+    for g in range(spec.ions['n_groups']):
+        spec.desc.j3_same[g] = big
+        spec.desc.j3_diff[g] = big
+    w = api.Walkers(api.System(lib, spec), 1, 1)
+    w.init_random(H.oracle_primes(1))
+    with pytest.raises(api.QMCError) as ei:
+        w.evaluate_log()
+    assert capi.STATUS[ei.value.status] == 'QMC_ERR_CAPACITY'
