@@ -60,6 +60,9 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
   __shared__ int j3_ion[8][J3_NEAR], j3_seg[8][2 * J3_NEAR + 1];
   __shared__ T j3_r[8][J3_NEAR];
   __shared__ int spin_used[2];
+  // per-warp J2 candidate lists: warp w's electrons (chunks of 32, w mod nw)
+  // that can be within the J2 cutoff of any of the 12 points
+  extern __shared__ int cand[];
   const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
   load_sys(sys, ss);
   const int w    = blockIdx.x;
@@ -191,15 +194,38 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
           if (rr < f.cutoff)
             atomicAdd(&sums[NLPP_K + k], (double)functor_v(f, rr));
         }
-      // ---- J2: the other electrons within the cutoff of each point (AA row, flip at jel)
+      // ---- J2: the other electrons within the cutoff of each point (AA row,
+      // flip at jel).  The 12 points lie at distance d from the centre C of
+      // their sphere, so an electron whose every image is at least rc + d
+      // from C (the exact cutoff test, widened) adds to no point: each warp
+      // lists its remaining electrons once, then all lanes work through
+      // (candidate, point) pairs.
       if (J2)
       {
         const int gi = jel < ss.n_up ? 0 : 1;
-        for (int idx = tid; idx < N * NLPP_K; idx += NT)
+        const double sg = a.form == 0 ? 1.0 : -1.0;
+        const T cx = (T)(ex + sg * in_dx[li][0]), cy = (T)(ey + sg * in_dx[li][1]), cz = (T)(ez + sg * in_dx[li][2]);
+        const T reach  = (T)in_d[li] + (ss.j2uu.cutoff > ss.j2ud.cutoff ? ss.j2uu.cutoff : ss.j2ud.cutoff);
+        const int per  = ((((N + 31) >> 5) + nw - 1) / nw) << 5;
+        int* lst       = cand + wid * per;
+        int cnt        = 0;
+        const unsigned below = (1u << lane) - 1u;
+        for (int c0 = wid; (c0 << 5) < N; c0 += nw)
         {
-          const int j = idx % N, k = idx / N;
-          if (j == jel)
-            continue;
+          const int j = (c0 << 5) + lane;
+          bool in     = false;
+          if (j < N && j != jel)
+            in = !beyond_cutoff(wv.Rs[j] - cx, wv.Rs[wv.Npad + j] - cy, wv.Rs[2 * wv.Npad + j] - cz, ss.gb,
+                                ss.mi_scale2, reach * reach);
+          const unsigned b = __ballot_sync(0xffffffffu, in);
+          if (in)
+            lst[cnt + __popc(b & below)] = j;
+          cnt += __popc(b);
+        }
+        __syncwarp();
+        for (int idx = lane; idx < cnt * NLPP_K; idx += 32)
+        {
+          const int j = lst[idx % cnt], k = idx / cnt;
           const T flip = j < jel ? T(1) : T(-1);
           T dx = (wv.Rs[j] - (T)vpos[k][0]) * flip, dy = (wv.Rs[wv.Npad + j] - (T)vpos[k][1]) * flip,
             dz = (wv.Rs[2 * wv.Npad + j] - (T)vpos[k][2]) * flip;
@@ -323,10 +349,20 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
 cudaError_t launch_nlpp(bool fp32, const DevSystem* sys, const DevWalkers& dw, const NlppArgs& a, int threads,
                         cudaStream_t st)
 {
+  // the per-warp J2 candidate lists: up to ceil(chunks / warps) chunks of 32
+  // electrons per warp
+  const int nw = threads / 32, per = ((((dw.N + 31) / 32) + nw - 1) / nw) * 32;
+  const size_t bytes = (size_t)nw * per * sizeof(int);
   if (fp32)
-    nlpp_kernel<float><<<dw.W, threads, 0, st>>>(sys, dw, a);
+  {
+    cudaFuncSetAttribute(nlpp_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    nlpp_kernel<float><<<dw.W, threads, bytes, st>>>(sys, dw, a);
+  }
   else
-    nlpp_kernel<double><<<dw.W, threads, 0, st>>>(sys, dw, a);
+  {
+    cudaFuncSetAttribute(nlpp_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    nlpp_kernel<double><<<dw.W, threads, bytes, st>>>(sys, dw, a);
+  }
   return cudaGetLastError();
 }
 
