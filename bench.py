@@ -53,9 +53,10 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-walkers', type=int, default=0)
-    ap.add_argument('--workload', default='nio128', choices=['nio128', 'uneven', 'serve'],
+    ap.add_argument('--workload', default='nio128', choices=['nio128', 'uneven', 'serve', 'nlpp'],
                     help='nio128: the headline batch; uneven: three NiO systems in one autotuned, graph-replayed '
-                         'launch; serve: Poisson-arrival request loop')
+                         'launch; serve: Poisson-arrival request loop; nlpp: the NonLocalPP ratios')
+    ap.add_argument('--nlpp-grid', default='148,148,148', help='nlpp: orbital grid of the NiO 2,2,1 cell')
     ap.add_argument('--jobs', type=int, default=200, help='serve: number of jobs (the full configuration is 2000)')
     ap.add_argument('--rate', type=float, default=20.0, help='serve: arrivals per second')
     ap.add_argument('--budget-gb', type=float, default=100.0, help='serve: device memory budget of the server')
@@ -250,9 +251,51 @@ def run_extra_workload(args):
     from miniqmc_b200 import api, capi
     lib = api.Library()
     lib.call('init', 0)
-    out = run_uneven(args, lib, api, capi, torch) if args.workload == 'uneven' else \
-        run_serve(args, lib, api, capi, torch)
+    run = {'uneven': run_uneven, 'serve': run_serve, 'nlpp': run_nlpp}[args.workload]
+    out = run(args, lib, api, capi, torch)
     print(json.dumps(out), flush=True)
+
+
+def run_nlpp(args, lib, api, capi, torch):
+    """NonLocalPP ratios (qmc_nlpp_evaluate, the driver's form) on the
+    reference's NiO-128 cell (its 32-atom cell tiled 2x2x1: 1536 e-, 128
+    ions), --walkers walkers, the orbital grid of --nlpp-grid, mixed form.
+    A step is one call over every walker: all electrons x ions within rmax
+    1.7 x 12 points.  The dominant bytes of a point are its value-only
+    stencil, 64 n coefficients."""
+    grid = tuple(int(x) for x in args.nlpp_grid.split(','))
+    spec = api.SystemSpec(lib, cell=capi.NIO_REF32, tiling=(2, 2, 1), grid=grid, fill=capi.FILL_UNIFORM,
+                          spo_seed=11, jastrow='reference')
+    system = api.System(lib, spec, capi.PREC_MIXED)
+    w = api.Walkers(system, args.walkers, args.delay)
+    w.init_random((np.arange(args.walkers, dtype=np.uint32) * 7919 + 1009).astype(np.uint32))
+    w.evaluate_log()
+    for _ in range(args.warmup):
+        w.nlpp(1.7, capi.NLPP_DRIVER)
+    points, times = 0, []
+    clocks = ClockSampler(0)
+    clocks.start()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        n, _, _ = w.nlpp(1.7, capi.NLPP_DRIVER)
+        times.append(time.perf_counter() - t0)
+        points += int(np.sum(n))
+    clk = clocks.stop()
+    total = sum(times)
+    bytes_per_point = 64.0 * spec.n_orb * 4
+    achieved = points * bytes_per_point / total / 1e9
+    pk, kind = peaks()
+    peak = pk['hbm_gbs']
+    return {'metric': 'NLPP quadrature-point ratios/s', 'value': points / total, 'unit': 'ratios/s', 'n_gpus': 1,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_call': 1e3 * total / args.steps,
+            'points_per_call': points / args.steps, 'higher_is_better': True, 'dtype': 'f32', 'data': 'synthetic',
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'algorithmic_bytes_per_point': bytes_per_point,
+                         'kernel': 'nlpp_kernel<float>', 'peak_kind': kind},
+            'clocks': clk,
+            'config': {'workload': 'NLPP ratios, NiO 2,2,1 of the 32-atom cell: 128 ions, 1536 e-, 768 orbitals/spin, '
+                                   'grid %s FP32 table, %d walkers, rmax 1.7, 12 points' % (args.nlpp_grid, args.walkers),
+                       'l2': 'inputs larger than L2'}}
 
 
 def run_uneven(args, lib, api, capi, torch):
