@@ -226,6 +226,14 @@ int qmc_walkers_set_stream(qmc_walkers* w, void* stream);
 int qmc_walkers_init_random(qmc_walkers* w, const uint32_t* seeds);
 int qmc_walkers_set_positions(qmc_walkers* w, const double* R /* [W][N][3] */);
 int qmc_walkers_get_positions(qmc_walkers* w, double* R /* [W][N][3] */);
+/* SPOSet::evaluate (einspline_spo.hpp:163-223) for electron iat of every
+ * walker of a batch, at ParticleSet::activeR(iat): the proposed position
+ * after qmc_pset_make_move(iat), else the current one.  The outputs are
+ * caller-owned DEVICE buffers, FP64, SoA per walker: v[W][n_orb],
+ * g[W][3][n_orb], h[W][6][n_orb] (xx xy xz yy yz zz).  With g and h NULL
+ * only the values are evaluated.  Asynchronous on the batch's stream
+ * (qmc_walkers_sync waits). */
+int qmc_spo_evaluate_batch(qmc_walkers* w, int iat, double* v_dev, double* g_dev, double* h_dev);
 
 /* ParticleSet verbs over all walkers of the batch (the flex_* forms of
  * ParticleSet.cpp:296-346; W == 1 is the single-walker API). */

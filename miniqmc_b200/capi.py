@@ -152,6 +152,7 @@ PRODUCT_ONLY = {
     'invert_transpose_noalloc': (I, [I, P, P, PD, PD, P]),
     'sweep_async': (I, [P, I, I, D, I]),
     'step': (I, [P, I, D, PD, PD, PI]),
+    'spo_evaluate_batch': (I, [P, I, P, P, P]),
     'walkers_sync': (I, [P]),
     'sweep_results': (I, [P, C.POINTER(C.c_int64), PD]),
     'walkers_launch_count': (I, [P, C.POINTER(C.c_int64)]),

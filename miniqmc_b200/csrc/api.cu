@@ -1060,6 +1060,20 @@ int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio)
   return ratio_verb(w, VERB_RATIO, iat, ratio, nullptr);
 }
 
+int qmc_spo_evaluate_batch(qmc_walkers* w, int iat, double* v_dev, double* g_dev, double* h_dev)
+{
+  int st = check_iat(w, iat);
+  if (st)
+    return st;
+  if (!v_dev && !g_dev && !h_dev)
+    return fail(QMC_ERR_ARG, "no output buffer");
+  // the positions go through the qmc_step scratch ([W][4] doubles, >= [W][3])
+  CK(launch_active_pos(w->dw, iat, w->d_step, w->stream));
+  CK(launch_spo_points(w->fp32, w->sys->d, w->dw.W, w->d_step, v_dev, g_dev, h_dev, !g_dev && !h_dev, w->stream));
+  w->launches += 2;
+  return QMC_OK;
+}
+
 int qmc_step(qmc_walkers* w, int iat, double accept, const double* ur, const double* delta, int* accepted)
 {
   int st = check_iat(w, iat);

@@ -107,6 +107,8 @@ cudaError_t launch_step(bool fp32, bool j3, const DevSystem* sys, const DevWalke
 cudaError_t launch_verb(bool fp32, const DevSystem* sys, const DevWalkers& dw, const VerbArgs& a, int threads,
                         int max_k, cudaStream_t st);
 
+// ParticleSet::activeR(iat) of every walker into pos[W][3] (device)
+cudaError_t launch_active_pos(const DevWalkers& dw, int iat, double* pos, cudaStream_t st);
 // standalone SPO evaluation at arbitrary points (check_spo)
 cudaError_t launch_spo_points(bool fp32, const DevSystem* sys, int n_pos, const double* pos, double* v,
                               double* g, double* h, bool values_only, cudaStream_t st);

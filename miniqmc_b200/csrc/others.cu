@@ -1169,6 +1169,24 @@ cudaError_t launch_sync_rs(bool fp32, const DevWalkers& dw, cudaStream_t st)
   return cudaGetLastError();
 }
 
+// activeR(iat) (ParticleSet.h:222): the proposed position while iat is the
+// active electron, else the current one
+__global__ void active_pos_kernel(DevWalkers dw, int iat, double* pos)
+{
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= dw.W)
+    return;
+  const MoveState& ms = dw.ms[w];
+  for (int c = 0; c < 3; ++c)
+    pos[3 * w + c] = ms.active == iat ? ms.pos[c] : dw.R[((size_t)w * dw.N + iat) * 3 + c];
+}
+
+cudaError_t launch_active_pos(const DevWalkers& dw, int iat, double* pos, cudaStream_t st)
+{
+  active_pos_kernel<<<(dw.W + 127) / 128, 128, 0, st>>>(dw, iat, pos);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spo_points(bool fp32, const DevSystem* sys, int n_pos, const double* pos, double* v, double* g,
                               double* h, bool values_only, cudaStream_t st)
 {

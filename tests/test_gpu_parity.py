@@ -209,6 +209,36 @@ def test_verbs(delay):
     assert rel_err(gw.components(), ow.components()) < RTOL64
 
 
+def test_spo_evaluate_batch_device_buffers():
+    """qmc_spo_evaluate_batch: the batch's SPO at activeR(iat) into device
+    buffers, against the oracle's SPO at the same points (FP64): the proposed
+    positions after makeMove, then the current ones once the move is
+    rejected (values only)."""
+    import torch
+    W, iat = 3, 7
+    gw, ow = H.make_pair(walkers=W, delay=2)
+    gw.evaluate_log()
+    d = np.random.default_rng(4).normal(size=(W, 3)) * 0.5
+    gw.make_move(iat, d)
+    pos = gw.positions()[:, iat] + d
+    n = gw.sys.spec.n_orb
+    v = torch.zeros((W, n), dtype=torch.float64, device='cuda')
+    g = torch.zeros((W, 3, n), dtype=torch.float64, device='cuda')
+    h = torch.zeros((W, 6, n), dtype=torch.float64, device='cuda')
+    lib = H.product()
+    lib.call('spo_evaluate_batch', gw.h, iat, v.data_ptr(), g.data_ptr(), h.data_ptr())
+    lib.call('walkers_sync', gw.h)
+    vo, go, ho = ow.sys.spo_vgh(pos)
+    assert rel_err(v.cpu().numpy(), vo) < RTOL64
+    assert rel_err(g.cpu().numpy(), go) < RTOL64
+    assert rel_err(h.cpu().numpy(), ho) < RTOL64
+    gw.accept_reject(iat, np.zeros(W, dtype=np.int32))
+    v.zero_()
+    lib.call('spo_evaluate_batch', gw.h, iat, v.data_ptr(), None, None)
+    lib.call('walkers_sync', gw.h)
+    assert rel_err(v.cpu().numpy(), ow.sys.spo_v(gw.positions()[:, iat])) < RTOL64
+
+
 @pytest.mark.parametrize('prec,tol', [(capi.PREC_FP64, 1e-10), (capi.PREC_MIXED, 1e-4)])
 def test_step_entry_point_matches_sweep(prec, tol):
     """qmc_step, one fused single-electron move of the batch per call, over
