@@ -125,3 +125,33 @@ def test_server_admission_follows_the_budget():
     with pytest.raises(api.QMCError) as ei:
         srv.submit(s, 64, 2, 8, 4)
     assert capi.STATUS[ei.value.status] == 'QMC_ERR_ADMISSION'
+
+
+def test_handles_are_reentrant_across_host_threads():
+    """One host thread per batch (each on its own stream): two batches of
+    different systems swept concurrently give the walkers each gives alone
+    (the thread-local error state and the per-handle streams keep the calls
+    independent; ctypes releases the GIL around them)."""
+    import threading
+    seeds = [H.oracle_primes(3), H.oracle_primes(5)[2:]]
+    kw = [dict(tiling=(1, 1, 1)), dict(tiling=(1, 1, 2))]
+
+    def run(i, out):
+        gw, _ = H.make_pair(walkers=3, delay=4, seeds=seeds[i], **kw[i])
+        gw.evaluate_log()
+        ur, de = H.host_streams(seeds[i], gw.N, 2, 1)
+        r = gw.sweep(2, 1, 0.5, ur=ur, delta=de)
+        out[i] = (r['logpsi'].copy(), r['accepted'].copy(), gw.positions().copy())
+
+    alone = {}
+    for i in range(2):
+        run(i, alone)
+    together = {}
+    threads = [threading.Thread(target=run, args=(i, together)) for i in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for i in range(2):
+        for a, b in zip(alone[i], together[i]):
+            assert np.array_equal(a, b)
