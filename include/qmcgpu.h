@@ -317,7 +317,10 @@ int qmc_walkers_launch_count(const qmc_walkers* w, int64_t* count);
  * [0] random streams, [1] getInvRow, [2] SPO VGH + determinant dots,
  * [3] J1/J2 sums, [4] reductions and ratio, [5] acceptRow bookkeeping,
  * [6] Woodbury flush, [7] J2 accept, [8] position update,
- * [9] completeUpdates, [10] evaluateGL.  n_phases receives 11. */
+ * [9] completeUpdates, [10] evaluateGL, [11] a move's set-up, and for the
+ * tensor-core flush [12] its U2 = Binv V image and [13] its first GEMM
+ * (Ainv U^T), [6] then holding its second GEMM and the Ainv update.
+ * ms needs room for n_phases values; n_phases receives 14. */
 int qmc_walkers_enable_timers(qmc_walkers* w, int enable);
 
 /* Woodbury flush on the tensor cores (tcgen05, 3xTF32 with FP32

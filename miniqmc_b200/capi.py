@@ -160,7 +160,8 @@ PRODUCT_ONLY = {
     'walkers_phase_times': (I, [P, PD, PI]),
 }
 PHASES = ['random', 'getInvRow', 'spo+det dots', 'jastrow sums', 'reduce+ratio', 'acceptRow', 'woodbury flush',
-          'J2 accept', 'position', 'completeUpdates', 'evaluateGL', 'move setup']
+          'J2 accept', 'position', 'completeUpdates', 'evaluateGL', 'move setup',
+          'flush U2 image', 'flush GEMM1']
 
 
 def bind(lib, prefix, extra=None):

@@ -108,8 +108,11 @@ __device__ __forceinline__ void tc_split_store(float* hi, float* lo, int off, fl
 }
 
 // `smem`: at least tc_flush_smem_bytes() of dynamic shared memory when the
-// walker view has no cached Binv (the tiles then start there)
-__device__ inline void flush_tc(const WV<float>& wv, MoveSmem& m, int s, float* smem)
+// walker view has no cached Binv (the tiles then start there).
+// Out of line: the sweep calls the flush from four places, and one shared
+// copy instead of four inlined ones leaves the move code fewer spills (the
+// sweep measured 187 ms instead of 201 at NiO-128, 512 walkers).
+static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, int s, float* smem)
 {
   __shared__ int dls[TC_KD];
   const int tid = threadIdx.x, NT = blockDim.x, warp = tid >> 5, lane = tid & 31;
@@ -165,6 +168,7 @@ __device__ inline void flush_tc(const WV<float>& wv, MoveSmem& m, int s, float* 
   // the tiles overlay the cached Binv: keep the other spin's copy if cached
   double* keep = (wv.bsm && wv.bsm_spin != s) ? wv.Binv + (size_t)wv.bsm_spin * k * k : nullptr;
   __syncthreads();
+  phase_mark(m, PH_FLUSH_U2);
   if (keep)
   {
     for (int i = tid; i < k * k; i += NT)
@@ -248,6 +252,7 @@ __device__ inline void flush_tc(const WV<float>& wv, MoveSmem& m, int s, float* 
     if (m.tc_abort)
       break;
     tc_fence_after();
+    phase_mark(m, PH_FLUSH_G1);
 
     // ------------------------- tm = TMEM - E, split into the GEMM2 A operand
     if (warp < 4)
@@ -342,6 +347,7 @@ __device__ inline void flush_tc(const WV<float>& wv, MoveSmem& m, int s, float* 
       tc_fence_before();
     }
     __syncthreads();
+    phase_mark(m, PH_FLUSH);
   }
   if (tid == 0)
   {

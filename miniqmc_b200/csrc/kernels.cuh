@@ -21,6 +21,8 @@ enum Phase
   PH_COMPLETE,      // completeUpdates ("Complete Updates")
   PH_GL,            // evaluateGL ("Kinetic Energy")
   PH_SETUP,         // a move's serial set-up: positions, stencil location
+  PH_FLUSH_U2,      // tensor-core flush: the U2 = Binv V image
+  PH_FLUSH_G1,      // tensor-core flush: GEMM1 (Ainv U^T); PH_FLUSH keeps GEMM2
   NPHASE
 };
 
