@@ -105,7 +105,16 @@ def test_sweep_nio128_tensor_core_flush():
     768 x 768 Slater matrices (the initial FP32 inverse already differs from
     the FP64 one by ~1e-5 of its largest entry; measured log-ratio median
     9e-4 with the CUDA-core flush); the 3xTF32 flush may add a few times
-    that (measured 1.6x)."""
+    that (measured 1.6x).
+
+    log psi after the step sums the log-ratios of the accepted moves, and the
+    threshold accept rule takes near-node moves (|ratio| << 1), whose errors
+    are O(1) at this conditioning.  Its error therefore depends on the
+    rounding of a few such moves: two summation orders of the same dots gave
+    9e-6 and 1.3e-4 with this flush (1.6e-5 and 6e-7 with the CUDA-core
+    one) at the same median log-ratio error.  The bound is set above that
+    spread; a wrong update gives O(1) errors or a different accept
+    sequence."""
     seeds = H.oracle_primes(1)
     g_tc, ow = _nio128_pair(capi.PREC_MIXED, True)
     g_simt, _ = _nio128_pair(capi.PREC_MIXED, False)
@@ -120,4 +129,4 @@ def test_sweep_nio128_tensor_core_flush():
     lt, ls = _logratio_err(r_tc, r_o), _logratio_err(r_simt, r_o)
     assert np.median(lt) < 1e-2, np.median(lt)
     assert np.median(lt) < 4 * max(np.median(ls), 1e-7), (np.median(lt), np.median(ls))
-    assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-4
+    assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-3
