@@ -537,38 +537,39 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
 // A^{-1}[a][b] = M[piv[a]][pinv[b]], so psiM[i][j] = M[piv[j]][pinv[i]];
 // the sign of det A is the pivots' sign times the parity of piv.
 constexpr int GJB_B = 32;      // panel width
-constexpr int GJB_U = 8;       // rows per warp and pass of the rank-32 update
 constexpr int GJB_FS = GJB_B + 1; // padded panel row (conflict-free row-per-thread access)
 __host__ __device__ constexpr size_t gjb_smem_bytes(int n)
 {
-  return (size_t)n * GJB_FS * sizeof(double) + (size_t)GJB_B * 32 * sizeof(double) + (size_t)2 * n * sizeof(int);
+  return (((size_t)n * GJB_FS + 1) & ~(size_t)1) * sizeof(double) + (size_t)2 * GJB_B * 32 * sizeof(double) +
+      (size_t)2 * n * sizeof(int);
 }
-constexpr size_t GJB_MAX_SMEM = 220 * 1024;
+constexpr size_t GJB_MAX_SMEM = 226 * 1024;
 
 template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kernel(DevWalkers dw)
 {
   extern __shared__ __align__(16) unsigned char dyn[];
   const int n = dw.n, npad = dw.npad;
   double* F = reinterpret_cast<double*>(dyn);   // [n][GJB_FS] panel
-  double* R = F + (size_t)n * GJB_FS;            // [GJB_B][32] pivot rows of one column chunk
-  int* piv  = reinterpret_cast<int*>(R + GJB_B * 32); // [n] pivot row of each column
+  double* R = F + (((size_t)n * GJB_FS + 1) & ~(size_t)1); // [2][GJB_B][32] pivot rows of a column chunk (16-byte aligned)
+  int* piv  = reinterpret_cast<int*>(R + 2 * GJB_B * 32); // [n] pivot row of each column
   int* pinv = piv + n;                                 // [n] column pivoted by each row, -1 while free
   __shared__ double s_val[32];
   __shared__ int s_idx[32];
   __shared__ double s_logdet, s_tiny;
-  __shared__ int s_neg, s_sing, s_p;
+  __shared__ int s_neg, s_sing;
   const int s = blockIdx.x, w = blockIdx.y, tid = threadIdx.x, NT = blockDim.x;
   const int lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
   const WV<T> wv = make_wv<T>(dw, w);
   double* M = wv.lu + (size_t)s * n * npad;
 
-  // threshold for a zero pivot: n eps max|A|
+  // threshold for a zero pivot: n eps max|A| (warp per row, lanes along it)
   double mx = 0.0;
   for (int i = tid; i < n; i += NT)
-  {
     pinv[i] = -1;
+  for (int i = wid; i < n; i += nw)
+  {
     const double* row = M + (size_t)i * npad;
-    for (int j = 0; j < n; ++j)
+    for (int j = lane; j < n; j += 32)
       mx = fmax(mx, fabs(row[j]));
   }
   for (int o = 16; o > 0; o >>= 1)
@@ -598,9 +599,19 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
       F[i * GJB_FS + kk] = kk < bw ? M[(size_t)i * npad + c0 + kk] : 0.0;
     }
     __syncthreads();
-    // ---- unblocked Gauss-Jordan on the panel
+    // ---- unblocked Gauss-Jordan on the panel, two barriers per pivot: every
+    // thread reduces the warps' candidates itself (same order, same pivot);
+    // the other rows are eliminated with the unscaled pivot row times 1/pv,
+    // and the pivot row is scaled at the start of the next step (it is no
+    // longer a candidate, and the next elimination reads it after the
+    // barrier)
+    int pp     = -1;  // pivot row of the previous step, still unscaled
+    double prp = 0.0; // its reciprocal pivot
+    int pk     = 0;   // its column
     for (int kk = 0; kk < bw; ++kk)
     {
+      if (pp >= 0 && tid < bw)
+        F[pp * GJB_FS + tid] = tid == pk ? prp : F[pp * GJB_FS + tid] * prp;
       double bv = -1.0;
       int bi    = n;
       for (int i = tid; i < n; i += NT)
@@ -620,19 +631,19 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
       if (lane == 0)
         s_val[wid] = bv, s_idx[wid] = bi;
       __syncthreads();
+      double v = s_val[0];
+      int p    = s_idx[0];
+      for (int q = 1; q < nw; ++q)
+        if (s_val[q] > v || (s_val[q] == v && s_idx[q] < p))
+          v = s_val[q], p = s_idx[q];
+      const double pv = F[p * GJB_FS + kk];
+      const bool ok   = fabs(pv) > tiny;
       if (tid == 0)
       {
-        double v = s_val[0];
-        int p    = s_idx[0];
-        for (int q = 1; q < nw; ++q)
-          if (s_val[q] > v || (s_val[q] == v && s_idx[q] < p))
-            v = s_val[q], p = s_idx[q];
-        const double pv = F[p * GJB_FS + kk];
-        piv[c0 + kk]    = p;
-        pinv[p]         = c0 + kk;
-        s_p             = p;
-        if (!(fabs(pv) > tiny))
-          s_sing = 1;
+        piv[c0 + kk] = p;
+        pinv[p]      = c0 + kk;
+        if (!ok)
+          s_sing = 1; // zero pivot: reported, column left as is
         else
         {
           s_logdet += log(fabs(pv));
@@ -640,72 +651,100 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
             s_neg ^= 1;
         }
       }
-      __syncthreads();
-      const int p     = s_p;
-      const double pv = F[p * GJB_FS + kk];
-      if (!(fabs(pv) > tiny))
-        continue; // zero pivot: reported, column left as is
-      const double rp = 1.0 / pv;
-      __syncthreads(); // every thread has read pv before the pivot row changes
-      if (tid < bw)
-        F[p * GJB_FS + tid] = tid == kk ? rp : F[p * GJB_FS + tid] * rp;
-      __syncthreads();
-      for (int i = tid; i < n; i += NT)
-        if (i != p)
-        {
-          double* fi     = F + i * GJB_FS;
-          const double f = fi[kk];
-          for (int q = 0; q < bw; ++q)
-            fi[q] = q == kk ? -f * rp : fi[q] - f * F[p * GJB_FS + q];
-        }
+      pp = -1;
+      if (ok)
+      {
+        const double rp = 1.0 / pv;
+        for (int i = tid; i < n; i += NT)
+          if (i != p)
+          {
+            double* fi     = F + i * GJB_FS;
+            const double g = fi[kk] * rp;
+            for (int q = 0; q < bw; ++q)
+              fi[q] = q == kk ? -g : fi[q] - g * F[p * GJB_FS + q];
+          }
+        pp = p, prp = rp, pk = kk;
+      }
       __syncthreads();
     }
+    if (pp >= 0 && tid < bw)
+      F[pp * GJB_FS + tid] = tid == pk ? prp : F[pp * GJB_FS + tid] * prp;
+    __syncthreads();
     // ---- the other columns, in chunks of 32: A[:, J] <- [i not in P] A[:, J] + F A[P, J]
+    // (the chunks' pivot rows alternate between two buffers: one barrier per
+    // chunk; a buffer is refilled only after every thread has passed the
+    // next chunk's barrier, i.e. finished with it)
+    int rbuf = 0;
     for (int j0 = 0; j0 < n; j0 += 32)
     {
       if (j0 == c0)
         continue;
       const int jw = min(32, n - j0);
+      double* Rb   = R + rbuf * GJB_B * 32;
+      rbuf ^= 1;
       for (int idx = tid; idx < GJB_B * 32; idx += NT)
       {
         const int k = idx >> 5, jj = idx & 31;
-        R[idx]      = (k < bw && jj < jw) ? M[(size_t)piv[c0 + k] * npad + j0 + jj] : 0.0;
+        Rb[idx]     = (k < bw && jj < jw) ? M[(size_t)piv[c0 + k] * npad + j0 + jj] : 0.0;
       }
       __syncthreads();
-      double r[GJB_B];
+      // each thread updates a 4-row x 4-column tile: columns j0 + 2 cg + {0, 1}
+      // and j0 + 16 + 2 cg + {0, 1} (cg = lane % 8: a row's 32 columns are
+      // two 128-byte runs over 8 lanes), rows ib..ib+3 (rg = lane / 8), so
+      // that one shared-memory load feeds several FMAs; each element's FMA
+      // chain over the panel runs in the same order as a row-by-row update
+      const int cg = lane & 7, rg = lane >> 3;
+      const int ja = 2 * cg, jb = 16 + 2 * cg;
+      const bool va = ja < jw, vb = jb < jw; // jw is even unless n is odd
+      for (int ib = wid * 16 + rg * 4; ib < n; ib += nw * 16)
+      {
+        double acc[4][4];
 #pragma unroll
-      for (int k = 0; k < GJB_B; ++k)
-        r[k] = R[k * 32 + lane];
-      // warp per row, lane per column; GJB_U rows per pass so that their
-      // loads are in flight together and their FMA chains interleave
-      if (lane < jw)
-        for (int i0 = wid; i0 < n; i0 += GJB_U * nw)
+        for (int u = 0; u < 4; ++u)
         {
-          double acc[GJB_U];
+          const int i     = ib + u;
+          const int c     = i < n ? pinv[i] : c0;
+          const bool zero = i >= n || (c >= c0 && c < c0 + bw);
+          const double* mi = M + (size_t)(i < n ? i : 0) * npad + j0;
 #pragma unroll
-          for (int u = 0; u < GJB_U; ++u)
+          for (int e = 0; e < 2; ++e)
           {
-            const int i = i0 + u * nw;
-            const int c = i < n ? pinv[i] : c0;
-            acc[u]      = (i >= n || (c >= c0 && c < c0 + bw)) ? 0.0 : M[(size_t)i * npad + j0 + lane];
-          }
-#pragma unroll
-          for (int k = 0; k < GJB_B; ++k)
-#pragma unroll
-            for (int u = 0; u < GJB_U; ++u)
-            {
-              const int i = min(i0 + u * nw, n - 1);
-              acc[u]      = fma(F[i * GJB_FS + k], r[k], acc[u]);
-            }
-#pragma unroll
-          for (int u = 0; u < GJB_U; ++u)
-          {
-            const int i = i0 + u * nw;
-            if (i < n)
-              M[(size_t)i * npad + j0 + lane] = acc[u];
+            acc[u][e]     = (zero || ja + e >= jw) ? 0.0 : mi[ja + e];
+            acc[u][2 + e] = (zero || jb + e >= jw) ? 0.0 : mi[jb + e];
           }
         }
-      __syncthreads(); // the next chunk's pivot rows are read from M
+#pragma unroll 4
+        for (int k = 0; k < GJB_B; ++k)
+        {
+          const double2 ra = *reinterpret_cast<const double2*>(Rb + k * 32 + ja);
+          const double2 rb = *reinterpret_cast<const double2*>(Rb + k * 32 + jb);
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+          {
+            const double f = F[min(ib + u, n - 1) * GJB_FS + k];
+            acc[u][0]      = fma(f, ra.x, acc[u][0]);
+            acc[u][1]      = fma(f, ra.y, acc[u][1]);
+            acc[u][2]      = fma(f, rb.x, acc[u][2]);
+            acc[u][3]      = fma(f, rb.y, acc[u][3]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+        {
+          const int i = ib + u;
+          if (i >= n)
+            continue;
+          double* mi = M + (size_t)i * npad + j0;
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+          {
+            if (va && ja + e < jw)
+              mi[ja + e] = acc[u][e];
+            if (vb && jb + e < jw)
+              mi[jb + e] = acc[u][2 + e];
+          }
+        }
+      }
     }
     for (int idx = tid; idx < n * bw; idx += NT)
     {
