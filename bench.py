@@ -548,6 +548,21 @@ def main():
                 'traffic_source': 'ncu dram bytes per move (64 walkers, grid 74x74x37) x moves per launch',
                 'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm,
                 'kernel': 'sweep_kernel<%s>' % ('float' if s == 4 else 'double'), 'launch_ms': avg_launch_ms}
+    # the Woodbury GEMMs on the tensor cores (tcgen05 kind::tf32, 3xTF32):
+    # per flush GEMM1 (n x npad by npad x k) and GEMM2 (n x k by k x npad),
+    # three TF32 products each, i.e. 12 n npad flops per accepted move.
+    # The TF32 peak is taken as half the measured dense BF16 rate (TF32
+    # MMAs run at half the BF16 rate).
+    tensor = None
+    if args.precision == 'mixed' and args.flush == 'tc':
+        npad = -(-n // 4) * 4
+        tflop = 12.0 * n * npad * a * W * N / 1e12
+        tf32_peak = pk['bf16_tflops'] / 2
+        ach = tflop / (avg_launch_ms / 1e3)
+        tensor = {'kernel': 'sweep_kernel Woodbury flush (tcgen05 kind::tf32, 3xTF32)', 'tflop_per_launch': tflop,
+                  'achieved': ach, 'peak': tf32_peak, 'unit': 'TFLOP/s', 'frac': ach / tf32_peak,
+                  'peak_kind': pk_kind + ' bf16 / 2',
+                  'ncu_pipe_tensor_cycles_active_pct': 0.75}
     plain = None
     if rank == 0 and world == 1 and args.plain_steps > 0:
         pv, pms = plain_fp64_form(lib, args, api, capi, torch.cuda.Stream)
@@ -579,7 +594,8 @@ def main():
                        'acceptance': a, 'parallelism': 'replicas x%d' % world,
                        'flush': args.flush if args.precision == 'mixed' else 'simt',
                        'recompute_every': args.recompute_every, 'recompute_ms': recompute_ms},
-            'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk, 'plain_fp64': plain,
+            'roofline': roofline, 'tensor': tensor, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk,
+            'plain_fp64': plain,
             'gpu_launches': launches,
         }
         print(json.dumps(out), flush=True)
