@@ -277,11 +277,14 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
     tc_fence_before();
 
     // ------------------------------------------ GEMM2 and the Ainv update
+    // B tile t (U2^T hi/lo, 8 KB of the per-walker image) into stage st:
+    // 16-byte cp.async copies, no registers held while they land
     auto load2 = [&](int t, int st) {
       const uint4* src = reinterpret_cast<const uint4*>(img + (size_t)t * 2 * 32 * Kd);
       uint4* dst       = reinterpret_cast<uint4*>(b2 + st * 2 * TC_BN2 * Kd);
       for (int i = tid; i < 2 * TC_BN2 * Kd / 4; i += NT)
-        dst[i] = src[i];
+        tc_cp_async16(dst + i, src + i);
+      tc_cp_async_commit();
     };
     auto mma2 = [&](int t) {
       float* Bs = b2 + (t & 1) * 2 * TC_BN2 * Kd;
@@ -299,25 +302,31 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
       }
       tc_commit(&m.tc_bar[2 + (t & 1)]);
     };
+    // Per column block t: the MMAs of block t+1 are issued first, then those
+    // of block t are waited for, block t+2's B tile starts into the stage
+    // they have just released, and the Ainv update of block t runs while
+    // block t+1 multiplies.  B tiles are thus copied two blocks ahead.
     load2(0, 0);
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0)
-      mma2(0);
+    if (T2 > 1)
+      load2(1, 1);
     for (int t = 0; t < T2; ++t)
     {
-      if (t + 1 < T2)
-      {
-        load2(t + 1, (t + 1) & 1); // its stage was read by the MMAs of block t-1
-        fence_async_smem();
-      }
+      tc_cp_async_wait_all(); // this thread's copies of block t+1's tile (and block 0's)
+      fence_async_smem();
       __syncthreads();
       if (m.tc_abort)
         break;
-      if (t + 1 < T2 && tid == 0)
-        mma2(t + 1);
+      if (tid == 0)
+      {
+        if (t == 0)
+          mma2(0);
+        if (t + 1 < T2)
+          mma2(t + 1);
+      }
       tc_wait(m, 2 + (t & 1), ph, wv);
       tc_fence_after();
+      if (t + 2 < T2)
+        load2(t + 2, t & 1); // its stage was read by the MMAs of block t, now complete
       if (warp < 4)
       {
         const int row = m0 + 32 * warp + lane;
@@ -346,6 +355,7 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
       }
       tc_fence_before();
     }
+    tc_cp_async_wait_all(); // nothing in flight if the loop was left early
     __syncthreads();
     phase_mark(m, PH_FLUSH);
   }
