@@ -130,3 +130,39 @@ def test_sweep_nio128_tensor_core_flush():
     assert np.median(lt) < 1e-2, np.median(lt)
     assert np.median(lt) < 4 * max(np.median(ls), 1e-7), (np.median(lt), np.median(ls))
     assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-3
+
+
+def _phase_times(gw):
+    import ctypes as C
+    ms = np.zeros(32)
+    n = C.c_int()
+    H.product().call('walkers_phase_times', gw.h, ms.ctypes.data_as(capi.PD), C.byref(n))
+    return n.value, ms[:n.value]
+
+
+@pytest.mark.parametrize('tensor_cores', [True, False])
+def test_phase_timers(tensor_cores):
+    """qmc_walkers_phase_times after one timed sweep of NiO-128: one value
+    per named phase, none negative; the tensor-core flush fills its three
+    sub-phases (U2 image, GEMM1, GEMM2), the CUDA-core flush only the
+    flush's own; the timers leave the results unchanged."""
+    seeds = H.oracle_primes(1)
+    ur, de = H.host_streams(seeds, 1536, 1, 1)
+    runs = []
+    for timed in (False, True):
+        gw, _ = _nio128_pair(capi.PREC_MIXED, tensor_cores)
+        gw.evaluate_log()
+        H.product().call('walkers_enable_timers', gw.h, 1 if timed else 0)
+        runs.append(gw.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True))
+    n, ms = _phase_times(gw)
+    assert n == len(capi.PHASES) == 14
+    assert np.all(ms >= 0) and ms.sum() > 0
+    ph = dict(zip(capi.PHASES, ms))
+    for name in ('getInvRow', 'spo+det dots', 'jastrow sums', 'woodbury flush'):
+        assert ph[name] > 0, name
+    if tensor_cores:
+        assert ph['flush U2 image'] > 0 and ph['flush GEMM1'] > 0
+    else:
+        assert ph['flush U2 image'] == 0 and ph['flush GEMM1'] == 0
+    assert np.array_equal(runs[0]['trace'], runs[1]['trace'])
+    assert np.array_equal(runs[0]['logpsi'], runs[1]['logpsi'])
