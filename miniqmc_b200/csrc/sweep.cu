@@ -19,6 +19,9 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   __shared__ SysSmem<T> ss;
   __shared__ MoveSmem m;
   __shared__ SplineSmem<T> sp;
+  // the walker's view (its arrays' device pointers) in shared memory rather
+  // than in registers: the move code reads each pointer when it needs it
+  __shared__ WV<T> wv;
   extern __shared__ __align__(16) unsigned char dyn[];
   int t = 0;
   while (t + 1 < n_tasks && (int)blockIdx.x >= tasks[t + 1].first_block)
@@ -28,8 +31,9 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
   if (w >= task.dw.W)
     return;
   const DevSystem* sys = task.sys;
-  load_sys(sys, ss);
-  WV<T> wv      = make_wv<T>(task.dw, w);
+  if (threadIdx.x == 0)
+    wv = make_wv<T>(task.dw, w);
+  load_sys(sys, ss); // ends with a barrier
   const int N   = wv.N;
   const T* ions = (const T*)sys->ion_soa;
   long long acc = 0;
@@ -43,8 +47,12 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
     double* b       = reinterpret_cast<double*>(dyn);
     for (int i = threadIdx.x; i < k * k; i += blockDim.x)
       b[i] = g[i];
-    wv.bsm      = b;
-    wv.bsm_spin = spin;
+    __syncthreads(); // every thread has read wv.bsm of the previous spin
+    if (threadIdx.x == 0)
+    {
+      wv.bsm      = b;
+      wv.bsm_spin = spin;
+    }
     __syncthreads();
   };
   if (threadIdx.x == 0)
@@ -99,7 +107,10 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
     {
       flush(wv, m, 0, smem);
       flush(wv, m, 1, smem);
-      wv.bsm = nullptr;
+      __syncthreads();
+      if (threadIdx.x == 0)
+        wv.bsm = nullptr;
+      __syncthreads();
     }
     phase_mark(m, PH_COMPLETE);
   }
