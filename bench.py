@@ -145,11 +145,11 @@ def build_workload(lib, args, capi, api, device_rng_seeds):
 
 
 # DRAM bytes per electron move of sweep_kernel<float> measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 24.856 + 5.242 GB over one
+# (dram__bytes_read.sum + dram__bytes_write.sum = 24.772 + 5.215 GB over one
 # launch of 64 walkers x 1536 moves, NiO 4x4x2, grid 74x74x37, k=32, mixed,
 # tensor-core flush); the bench's traffic figure scales it by the moves of
 # one launch
-MEASURED_TRAFFIC_PER_MOVE = (24.856e9 + 5.242e9) / (64 * 1536)
+MEASURED_TRAFFIC_PER_MOVE = (24.772e9 + 5.215e9) / (64 * 1536)
 
 
 def plain_fp64_form(lib, args, api, capi, stream_cls):
