@@ -17,10 +17,14 @@ __global__ void __launch_bounds__(256) verb_kernel(const DevSystem* __restrict__
   __shared__ SplineSmem<T> sp;
   __shared__ int s_invrow, s_partial, s_jpartial, s_active, s_flag;
   extern __shared__ __align__(16) unsigned char dyn[];
+  // the walker's view in shared memory rather than registers (as in the
+  // fused sweep)
+  __shared__ WV<T> wv;
   T* smem     = reinterpret_cast<T*>(dyn);
   const int w = blockIdx.x, tid = threadIdx.x, NT = blockDim.x;
-  load_sys(sys, ss);
-  const WV<T> wv = make_wv<T>(dw, w);
+  if (tid == 0)
+    wv = make_wv<T>(dw, w);
+  load_sys(sys, ss); // ends with a barrier
   MoveState* ms  = wv.ms;
   const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
   const bool J3 = ss.comp & QMC_WF_J3;

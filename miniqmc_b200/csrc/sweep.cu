@@ -143,10 +143,13 @@ __global__ void __launch_bounds__(256, 3) step_kernel(const DevSystem* __restric
   __shared__ SysSmem<T> ss;
   __shared__ MoveSmem m;
   __shared__ SplineSmem<T> sp;
+  // the walker's view in shared memory rather than registers, as in the sweep
+  __shared__ WV<T> wv;
   extern __shared__ __align__(16) unsigned char dyn[];
-  load_sys(sys, ss);
-  const int w       = blockIdx.x;
-  const WV<T> wv    = make_wv<T>(dw, w);
+  const int w = blockIdx.x;
+  if (threadIdx.x == 0)
+    wv = make_wv<T>(dw, w);
+  load_sys(sys, ss); // ends with a barrier
   const T* ions     = (const T*)sys->ion_soa;
   const double* inw = in + (size_t)4 * w;
   if (threadIdx.x == 0)
