@@ -65,8 +65,11 @@ enum {
                              field times cos(2 pi n / norb)
                              (einspline_spo.hpp:145-155,
                               BsplineAllocator.hpp:161-182)                */
-  QMC_FILL_UNIFORM = 2    /* every coefficient independent, uniform
+  QMC_FILL_UNIFORM = 2,   /* every coefficient independent, uniform
                              [-0.5, 0.5) from SplitMix64(seed, index)      */
+  QMC_FILL_UNIFORM_F32 = 3 /* QMC_FILL_UNIFORM rounded to FP32: in an FP64
+                             system, the mixed form's table held exactly,
+                             the FP64 form to measure the mixed one against */
 };
 
 /* what the determinant uses as the orbital "laplacian" */
@@ -252,9 +255,13 @@ int qmc_pset_get_temp_rows(qmc_walkers* w, double* aa_r, double* aa_dr, double* 
 /* evaluateLog from scratch: SPO VGH of all electrons, FP64 LU inverse and
  * log|det| per spin, J1/J2 recompute.  logpsi[W] may be NULL. */
 int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi);
+/* evalGrad: grad[W][3] = grad log psi at electron iat's current position.
+ * The output is assigned with the whole wavefunction's gradient, as
+ * WaveFunction::evalGrad returns it (WaveFunction.cpp:197-207). */
 int qmc_wf_eval_grad(qmc_walkers* w, int iat, double* grad /* [W][3] */);
 /* ratioGrad: ratio[W] = det * J1 * J2 ratio; grad[W][3] = grad log psi at
- * the proposed position. */
+ * the proposed position, assigned (WaveFunction::ratioGrad zeroes it before
+ * the components add their shares, WaveFunction.cpp:209-221). */
 int qmc_wf_ratio_grad(qmc_walkers* w, int iat, double* ratio, double* grad);
 /* ratio only (SPOSet values, no gradients). */
 int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio);
@@ -330,6 +337,15 @@ int qmc_walkers_enable_timers(qmc_walkers* w, int enable);
  * spin).  QMC_ERR_ARG when asked for where it does not apply.  Both compute
  * DelayedUpdate::updateInvMat (DelayedUpdate.h:184-191). */
 int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable);
+/* Limit, in SM cycles, of every bounded wait of the tensor-core flush on the
+ * MMAs it issued (no reference counterpart: the reference has no device
+ * waits).  Default 2e9 (about one second).  A wait that runs out sets the
+ * batch's error bit, the launch unwinds (the CTA drains its own MMAs before
+ * it frees its tensor memory) and the call that reads the status returns
+ * QMC_ERR_TIMEOUT.  The batch's inverses and delayed rows are then
+ * undefined: call qmc_wf_evaluate_log (which rebuilds them from the
+ * positions) or destroy the batch.  0 makes the first wait give up at once. */
+int qmc_walkers_set_wait_limit(qmc_walkers* w, long long cycles);
 /* Threads (one CTA) per walker: a multiple of 32 in [max(64, 2 delay), 256];
  * the default covers the padded orbitals with 16-byte vectors.  The kernels
  * stride over any block size; >= 128 is needed for the tensor-core flush. */
@@ -490,9 +506,10 @@ int qmc_nlpp_sphere(int n_calls, double* out);
  * device current, looks the array up (cudaGetSymbolAddress).  Make that
  * first call before any stream capture.  Calls on one device share the
  * array, so calls that overlap (other streams or host threads) race: the
- * caller must serialise them.  The call waits for `stream` (a cudaStream_t,
- * null for the default stream) to finish.  QMC_ERR_SINGULAR on a zero
- * pivot. */
+ * caller must serialise them.  Every call, not only the first, copies the
+ * log-det, phase and status to the host and waits for `stream` (a
+ * cudaStream_t, null for the default stream) to finish.  QMC_ERR_SINGULAR
+ * on a zero pivot. */
 #define QMC_NOALLOC_MAX_N 768
 int qmc_invert_transpose_noalloc(int n, const double* a, double* psim, double* logdet, double* phase,
                                  void* stream);

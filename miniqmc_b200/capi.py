@@ -13,7 +13,7 @@ STATUS = {0: 'QMC_OK', 1: 'QMC_ERR_ARG', 2: 'QMC_ERR_CUDA', 3: 'QMC_ERR_OOM', 4:
 PREC_FP64, PREC_MIXED = 0, 1
 NLPP_SPHERE, NLPP_DRIVER = 0, 1
 NOALLOC_MAX_N = 768  # largest n of qmc_invert_transpose_noalloc
-FILL_USER, FILL_REFERENCE, FILL_UNIFORM = 0, 1, 2
+FILL_USER, FILL_REFERENCE, FILL_UNIFORM, FILL_UNIFORM_F32 = 0, 1, 2, 3
 LAP_HXX, LAP_TRACE = 0, 1
 WF_DET, WF_J1, WF_J2, WF_ALL, WF_J3 = 1, 2, 4, 7, 8
 J3_PARAMS = 26
@@ -127,6 +127,7 @@ PRODUCT_ONLY = {
     'detengine_create_prec': (I, [I, I, I, C.POINTER(P)]),
     'detengine_set_tensor_cores': (I, [P, I]),
     'walkers_set_tensor_cores': (I, [P, I]),
+    'walkers_set_wait_limit': (I, [P, C.c_longlong]),
     'walkers_set_threads': (I, [P, I]),
     'walkers_set_prefetch': (I, [P, I]),
     'local_kinetic': (I, [P, PD]),

@@ -6,6 +6,7 @@
 // is no host fallback for any hot-path operation.
 #include "host_api.hpp"
 #include "host_lattice.hpp"
+#include "tc.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -250,6 +251,8 @@ __global__ void fill_table_kernel(T* coefs, size_t n_points, int norb, int npad,
     {
       if (mode == QMC_FILL_UNIFORM)
         v = splitmix_uniform(seed, g * norb + j) - 0.5;
+      else if (mode == QMC_FILL_UNIFORM_F32)
+        v = (double)(float)(splitmix_uniform(seed, g * norb + j) - 0.5);
       else if (mode == QMC_FILL_REFERENCE)
         v = field[g] * pref[j];
       else
@@ -273,6 +276,8 @@ int qmc_system_create(const qmc_system_desc* d, int precision, qmc_system** out)
     return fail(QMC_ERR_ARG, "bad system description");
   if ((comp & QMC_WF_DET) && (d->n_up != d->n_orb || d->n_elec - d->n_up != d->n_orb))
     return fail(QMC_ERR_ARG, "the determinants need n_up == n_elec - n_up == n_orb");
+  if (d->spo_fill < QMC_FILL_USER || d->spo_fill > QMC_FILL_UNIFORM_F32)
+    return fail(QMC_ERR_ARG, "unknown spline fill");
   if (d->spo_fill == QMC_FILL_USER && !d->spo_user_coefs)
     return fail(QMC_ERR_ARG, "QMC_FILL_USER needs spo_user_coefs");
   for (int i = 1; i < d->n_ions; ++i)
@@ -510,6 +515,7 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   const DevSystem& h = s->h;
   const size_t es = s->fp32 ? 4 : 8;
   d.W = W, d.N = h.n_elec, d.Npad = round_up(h.n_elec, 32), d.n = h.norb, d.npad = h.npad, d.I = h.n_ions, d.k = k;
+  d.wait_cycles = kTcWaitCycles;
   const size_t N = d.N, Np = d.Npad, n = d.n, np = d.npad, KK = k;
   std::vector<void*>& L = w->allocs;
   size_t& B             = w->bytes;
@@ -754,6 +760,16 @@ int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable)
     return fail(QMC_ERR_ARG, "tensor-core flush needs FP32 walkers, the determinant, delay rank <= 32 and >= 128 "
                              "threads per walker (480 or more orbitals per spin in FP32 give that)");
   w->use_tc = enable != 0;
+  return QMC_OK;
+}
+int qmc_walkers_set_wait_limit(qmc_walkers* w, long long cycles)
+{
+  if (!w || cycles < 0)
+    return fail(QMC_ERR_ARG, "null handle or negative wait limit");
+  cudaError_t e = cudaStreamSynchronize(w->stream); // no launch in flight reads the old value
+  if (e != cudaSuccess)
+    return fail(QMC_ERR_CUDA, cudaGetErrorString(e));
+  w->dw.wait_cycles = cycles;
   return QMC_OK;
 }
 int qmc_walkers_enable_timers(qmc_walkers* w, int enable)
@@ -1361,6 +1377,7 @@ int qmc_detengine_create_prec(int n, int delay, int precision, qmc_detengine_s**
   DevWalkers& d = w->dw;
   std::memset(&d, 0, sizeof(d));
   d.W = 1, d.N = n, d.Npad = round_up(n, 32), d.n = n, d.npad = round_up(n, 32), d.I = 0, d.k = delay;
+  d.wait_cycles    = kTcWaitCycles;
   w->fp32          = precision == QMC_PREC_MIXED;
   const size_t es  = w->fp32 ? 4 : 8;
   const size_t np  = d.npad, K = delay;

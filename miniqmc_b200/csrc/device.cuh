@@ -66,10 +66,12 @@ struct MoveSmem
   long long next_base;
   int accept, dc, ok;
   // tensor-core flush state: commit barriers (GEMM1 stages 0/1, GEMM2
-  // accumulators 0/1), their phase bits, the TMEM base, the abort flag
-  unsigned long long tc_bar[4];
+  // accumulators 0/1, and the drain barrier of an aborted CTA), their phase
+  // bits, the TMEM base, the abort flag and the limit of each bounded wait
+  unsigned long long tc_bar[5];
   unsigned tc_phase, tc_tmem;
   int tc_on, tc_abort;
+  long long tc_limit;
   // per-phase device timers (thread 0, clock64 at phase boundaries)
   int timing;
   long long tstamp;

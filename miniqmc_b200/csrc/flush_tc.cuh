@@ -48,14 +48,16 @@ __device__ __forceinline__ void tc_none(MoveSmem& m)
 }
 // set-up / tear-down of the CTA's tensor-core state (all threads call); a
 // CTA that does not use the tensor cores gives up its allocation right at
-// once so that the SM keeps taking further CTAs
-__device__ __forceinline__ void tc_begin(MoveSmem& m, int on)
+// once so that the SM keeps taking further CTAs.  `limit`: SM cycles after
+// which each bounded wait of the flush gives up (DevWalkers::wait_cycles).
+__device__ __forceinline__ void tc_begin(MoveSmem& m, int on, long long limit)
 {
   if (threadIdx.x == 0)
   {
     m.tc_on    = on;
     m.tc_abort = 0;
     m.tc_phase = 0;
+    m.tc_limit = limit;
   }
   if (!on && threadIdx.x < 32)
     tc_relinquish();
@@ -65,7 +67,7 @@ __device__ __forceinline__ void tc_begin(MoveSmem& m, int on)
       tc_alloc(&m.tc_tmem, TC_COLS);
     if (threadIdx.x == 0)
     {
-      for (int b = 0; b < 4; ++b)
+      for (int b = 0; b < 5; ++b)
         mbar_init(&m.tc_bar[b], 1);
       mbar_fence_init();
     }
@@ -75,8 +77,19 @@ __device__ __forceinline__ void tc_begin(MoveSmem& m, int on)
   if (on)
     tc_fence_after();
 }
+// After a wait gave up, MMAs the CTA issued may still be writing its TMEM
+// columns: the issuing thread (thread 0) commits once more to the drain
+// barrier, which arrives when all of them have completed, and waits for it
+// (bounded by the default limit, not the batch's, which may be tiny) before
+// the columns are released to the next CTA on this SM.
 __device__ __forceinline__ void tc_end(MoveSmem& m)
 {
+  __syncthreads();
+  if (m.tc_on && m.tc_abort && threadIdx.x == 0)
+  {
+    tc_commit(&m.tc_bar[4]);
+    mbar_wait(&m.tc_bar[4], 0u, kTcWaitCycles);
+  }
   __syncthreads();
   if (m.tc_on && threadIdx.x < 32)
   {
@@ -88,7 +101,7 @@ __device__ __forceinline__ void tc_end(MoveSmem& m)
 // all threads: bounded wait on commit barrier b; records a timeout
 __device__ __forceinline__ void tc_wait(MoveSmem& m, int b, uint32_t& ph, const WV<float>& wv)
 {
-  if (!mbar_wait(&m.tc_bar[b], (ph >> b) & 1u))
+  if (!mbar_wait(&m.tc_bar[b], (ph >> b) & 1u, m.tc_limit))
   {
     m.tc_abort = 1;
     atomicOr(wv.status, DEV_ERR_TIMEOUT);

@@ -1,4 +1,4 @@
-// kernels.cuh -- host-side launchers of the device code in kernels.cu.
+// kernels.cuh -- host-side launchers of the device code (sweep.cu, others.cu, nlpp.cu, state.cu).
 #pragma once
 
 #include "layout.cuh"

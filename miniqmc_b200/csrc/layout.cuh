@@ -130,6 +130,7 @@ struct DevWalkers
   double* out_ratio;   // [W]
   int* accept_flags;   // [W]
   unsigned* status;    // [1]
+  long long wait_cycles; // limit of each bounded tensor-core wait (SM cycles)
 };
 
 __host__ __device__ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }

@@ -1082,7 +1082,7 @@ __global__ void __launch_bounds__(256) det_engine_kernel(DevWalkers dw, int op, 
   if (threadIdx.x == 0)
     m.timing = 0;
   if constexpr (sizeof(T) == 4)
-    tc_begin(m, op == DETENG_GET_INV_ROW ? 0 : tc); // accept_row flushes when the delay fills
+    tc_begin(m, op == DETENG_GET_INV_ROW ? 0 : tc, dw.wait_cycles); // accept_row flushes when the delay fills
   else
     tc_none(m);
   if (op == DETENG_GET_INV_ROW)

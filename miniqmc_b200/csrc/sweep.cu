@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
       m.tacc[p] = 0;
   }
   if constexpr (sizeof(T) == 4)
-    tc_begin(m, tc && task.tc && DET);
+    tc_begin(m, tc && task.tc && DET, task.dw.wait_cycles);
   else
     tc_none(m);
   for (int l = 0; l < n_substeps && !m.tc_abort; ++l)

@@ -7,7 +7,8 @@
 
 namespace qmc
 {
-// a bounded wait gives up after this many SM cycles (about one second)
+// default limit of a bounded wait, in SM cycles (about one second); a batch
+// may set its own (qmc_walkers_set_wait_limit)
 constexpr long long kTcWaitCycles = 2000000000LL;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -56,13 +57,16 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t coun
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 // wait until the phase with parity `parity` of `bar` has completed; gives
-// up after kTcWaitCycles and returns false
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity)
+// up and returns false once `limit` SM cycles have passed (the clock is read
+// before each poll, so a limit of 0 gives up before the first one)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity, long long limit)
 {
   const uint32_t a   = smem_u32(bar);
   const long long t0 = clock64();
   while (true)
   {
+    if (clock64() - t0 >= limit)
+      return false;
     uint32_t ok;
     asm volatile("{\n\t.reg .pred p;\n\t"
                  "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -72,8 +76,6 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t pari
                  : "memory");
     if (ok)
       return true;
-    if (clock64() - t0 > kTcWaitCycles)
-      return false;
   }
 }
 

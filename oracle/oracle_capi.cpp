@@ -251,8 +251,12 @@ int oracle_system_create(const qmc_system_desc* d, int precision, oracle_system*
   s.spline.allocate(d->grid[0], d->grid[1], d->grid[2], d->n_orb);
   if (d->spo_fill == QMC_FILL_REFERENCE)
     s.spline.fill_reference((uint32_t)d->spo_seed);
-  else if (d->spo_fill == QMC_FILL_UNIFORM)
+  else if (d->spo_fill == QMC_FILL_UNIFORM || d->spo_fill == QMC_FILL_UNIFORM_F32)
+  {
     s.spline.fill_uniform(d->spo_seed);
+    if (d->spo_fill == QMC_FILL_UNIFORM_F32)
+      s.spline.round_to_float();
+  }
   else
     std::copy(d->spo_user_coefs, d->spo_user_coefs + s.spline.coefs.size(), s.spline.coefs.begin());
   if (precision == QMC_PREC_MIXED)

@@ -1,0 +1,76 @@
+"""The bounded waits of the tensor-core Woodbury flush run out and return.
+
+Every wait of the flush on its MMAs (mbarrier try_wait on a tcgen05.commit)
+gives up after the batch's limit (qmc_walkers_set_wait_limit).  With a limit
+of 0 the first wait gives up at once: no fault, no hang, only a short wait
+that returns.  The launch then unwinds, the CTA drains its own MMAs before it
+frees its tensor memory, and the status read reports QMC_ERR_TIMEOUT.  The
+reference has no device waits (it aborts the process on errors,
+Configuration.h:35-39), so the checks are: the sweep returns, the status is
+the timeout, the batch rebuilds from its positions and then sweeps to the
+FP64 oracle, the handle can be destroyed, and a fresh batch sweeps to the
+oracle on the same GPU context."""
+import numpy as np
+import pytest
+
+from miniqmc_b200 import api, capi
+from tests import gpu_helpers as H
+from tests.test_gpu_parity import elem_rel
+
+pytestmark = pytest.mark.gpu
+
+# NiO 2x2x2 of the 4-atom cell: 384 electrons, 192 orbitals per spin; with
+# 128 threads per walker the FP32 flush runs on the tensor cores
+KW = dict(tiling=(2, 2, 2), grid=(12, 12, 12), jastrow='synthetic')
+DELAY = 16
+
+
+def _tc_pair(walkers, seeds):
+    gw, ow = H.make_pair(precision=capi.PREC_MIXED, walkers=walkers, delay=DELAY, seeds=seeds, **KW)
+    H.product().call('walkers_set_threads', gw.h, 128)
+    H.product().call('walkers_set_tensor_cores', gw.h, 1)
+    return gw, ow
+
+
+def _sweep_matches_oracle(gw, ow, seeds, step):
+    ur, de = H.host_streams(seeds, gw.N, step + 1, 1)
+    ur, de = ur[step:step + 1], de[step:step + 1]
+    rg = gw.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    ro = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    assert np.array_equal(rg['trace'][..., 7], ro['trace'][..., 7])
+    assert np.array_equal(rg['accepted'], ro['accepted'])
+    # mixed form of a 192-orbital system: log psi to 1e-4 relative
+    assert elem_rel(rg['logpsi'], ro['logpsi']).max() < 1e-4
+
+
+def test_wait_limit_timeout_unwinds_and_recovers():
+    seeds = H.oracle_primes(2)
+    gw, ow = _tc_pair(2, seeds)
+    gw.evaluate_log()
+    ow.evaluate_log()
+    H.product().call('walkers_set_wait_limit', gw.h, 0)
+    ur, de = H.host_streams(seeds, gw.N, 1, 1)
+    with pytest.raises(api.QMCError) as ex:
+        gw.sweep(1, 1, 0.5, ur=ur, delta=de)
+    assert ex.value.status == 6  # QMC_ERR_TIMEOUT
+    # the status was read and cleared: the batch answers again
+    H.product().call('walkers_set_wait_limit', gw.h, 2000000000)
+    R = gw.positions()
+    ow.set_positions(R)
+    lg, lo = gw.evaluate_log(), ow.evaluate_log()
+    assert elem_rel(lg, lo).max() < 1e-6
+    _sweep_matches_oracle(gw, ow, seeds, 1)
+    gw.close()
+    # a fresh batch on the same context
+    g2, o2 = _tc_pair(2, seeds)
+    g2.evaluate_log()
+    o2.evaluate_log()
+    _sweep_matches_oracle(g2, o2, seeds, 0)
+    g2.close()
+
+
+def test_wait_limit_rejects_negative():
+    gw, _ = _tc_pair(1, H.oracle_primes(1))
+    with pytest.raises(api.QMCError):
+        H.product().call('walkers_set_wait_limit', gw.h, -1)
+    gw.close()
