@@ -53,6 +53,8 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-walkers', type=int, default=0)
+    ap.add_argument('--port-baseline', action='store_true',
+                    help='also time the FP64 oracle port on the host cores (beside the reference miniqmc)')
     ap.add_argument('--workload', default='nio128', choices=['nio128', 'uneven', 'serve', 'nlpp'],
                     help='nio128: the headline batch; uneven: three NiO systems in one autotuned, graph-replayed '
                          'launch; serve: Poisson-arrival request loop; nlpp: the NonLocalPP ratios')
@@ -65,6 +67,12 @@ def parse():
                     help='Woodbury flush on the tensor cores (tcgen05 3xTF32) or the CUDA cores (FP32 FMA)')
     ap.add_argument('--plain-steps', type=int, default=4,
                     help='walker-steps of the plain FP64 form (1 walker per launch, rank-1) to time; 0 = skip')
+    ap.add_argument('--fp64-steps', type=int, default=2,
+                    help='MC steps of the batched FP64 form at the same walker count to time; 0 = skip')
+    ap.add_argument('--error-walkers', type=int, default=4,
+                    help='walkers of the mixed-form error measurement; 0 = skip')
+    ap.add_argument('--error-steps', type=int, default=8,
+                    help='MC steps of the mixed-form error measurement (the refresh interval)')
     return ap.parse_args()
 
 
@@ -180,6 +188,74 @@ def plain_fp64_form(lib, args, api, capi, stream_cls):
     w.close()
     system.close()
     return spec.n_elec / (ms / 1e3), ms
+
+
+def fp64_reference_system(lib, args, api, capi):
+    """The FP64 form's system on the mixed form's table: the same
+    SplitMix64 coefficients rounded to FP32 (QMC_FILL_UNIFORM_F32), held and
+    evaluated in FP64."""
+    tiling = tuple(int(x) for x in args.tiling.split(','))
+    grid = tuple(int(x) for x in args.grid.split(','))
+    spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=grid, fill=capi.FILL_UNIFORM_F32,
+                          spo_seed=11, jastrow='synthetic')
+    return spec, api.System(lib, spec, capi.PREC_FP64)
+
+
+def mixed_form_error(lib, args, api, capi, spec, mixed_system, fp64_system):
+    """Per-quantity error of the benchmarked mixed form (same grid, delay
+    and flush engine) against the FP64 form on the same FP32-rounded table,
+    positions and random streams: --error-walkers walkers, --error-steps MC
+    steps of 1536 moves each (log-ratios and gradients of every move, log|det|
+    drift after the first and the last step).  No refresh inside the window:
+    --error-steps = the refresh interval measures the whole interval."""
+    from miniqmc_b200 import precision
+    W, S = args.error_walkers, args.error_steps
+    seeds = (np.arange(W, dtype=np.uint32) * 7919 + 1009).astype(np.uint32)
+    wm = api.Walkers(mixed_system, W, args.delay)
+    wd = api.Walkers(fp64_system, W, args.delay)
+    if args.flush == 'simt':
+        lib.call('walkers_set_tensor_cores', wm.h, 0)
+    for w in (wm, wd):
+        w.init_random(seeds)
+    rs = np.random.default_rng(23)
+    ur = rs.uniform(size=(S, W, 1, spec.n_elec))
+    de = rs.normal(size=(S, W, 1, spec.n_elec, 3))
+    pts = rs.uniform(size=(256, 3)) @ np.array(spec.ions['spo_lattice']).reshape(3, 3)
+    out = {'against': 'FP64 form on the same FP32-rounded table (QMC_FILL_UNIFORM_F32), same positions and '
+                      'streams', 'walkers': W, 'steps': S, 'delay': args.delay,
+           'flush': args.flush if args.precision == 'mixed' else 'simt',
+           'spo': precision.spo_errors(mixed_system, fp64_system, pts)}
+    out.update(precision.sweep_errors(wm, wd, ur, de, checkpoints=(1, S)))
+    wm.close()
+    wd.close()
+    return out
+
+
+def batched_fp64_form(lib, args, api, fp64_system, stream_cls):
+    """The same fused batched sweep in FP64 (table, orbitals, inverse,
+    Woodbury flush on the CUDA cores) at the bench's walker count and delay:
+    --fp64-steps timed MC steps after one warm-up step, no refresh.  Returns
+    (electron-moves/s, ms per step)."""
+    import torch
+    W = args.walkers
+    w = api.Walkers(fp64_system, W, args.delay)
+    w.init_random((np.arange(W, dtype=np.uint32) * 7919 + 1009).astype(np.uint32))
+    stream = stream_cls()
+    lib.call('walkers_set_stream', w.h, C.c_void_p(stream.cuda_stream))
+    w.evaluate_log()
+    lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
+    lib.call('walkers_sync', w.h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.fp64_steps):
+        lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
+    e1.record(stream)
+    lib.call('walkers_sync', w.h)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.fp64_steps
+    n = fp64_system.spec.n_elec
+    w.close()
+    return W * n / (ms / 1e3), ms
 
 
 def cpu_baseline(args, n_threads, sample_walkers):
@@ -410,29 +486,87 @@ def run_serve(args, lib, api, capi, torch):
                                          'speedup_of_wall': plain_s / wall}}
 
 
+REF_BIN = os.path.join(REPO, 'oracle', '_ref')
+
+
+def reference_binary(mixed=False):
+    """The reference's own miniqmc, built from its sources by
+    oracle/ref_miniqmc.mk for this host's widest ISA (x86-64-v4 with
+    AVX-512, else v3), or None when it was not built."""
+    try:
+        isa = 'v4' if ' avx512f' in open('/proc/cpuinfo').read() else 'v3'
+    except OSError:
+        isa = 'v3'
+    path = os.path.join(REF_BIN, 'miniqmc%s_%s' % ('_mixed' if mixed else '', isa))
+    return path if os.access(path, os.X_OK) else None
+
+
+def reference_miniqmc(args, n_threads, steps, mixed=False):
+    """Time the reference's own miniqmc on the host cores: one walker per
+    OpenMP thread (-w = threads), its Release build, OPENBLAS_NUM_THREADS=1.
+    The bench's NiO tiling (n1,n2,n3) of the 4-atom cell is the reference's
+    -g "n1/2 n2/2 n3/2" of its 32-atom cell (1536 e- at 4,4,2); its table is
+    the 32-atom cell's at -m 2 (74^3 points; per move the same 64 stencil
+    points x 768 orbitals), -x 0 leaves out the NLPP step.  electron-moves/s
+    = W * steps * N / Diffusion time, from the driver's own throughput line
+    (miniqmc.cpp:509-521: N_walkers * N_elec^3 / Diffusion time).  Returns
+    (moves/s, description) or raises."""
+    import re
+    import tempfile
+    exe = reference_binary(mixed)
+    if exe is None:
+        raise RuntimeError('reference miniqmc not built (oracle/ref_miniqmc.mk)')
+    t = [int(x) for x in args.tiling.split(',')]
+    if any(x % 2 for x in t):
+        raise RuntimeError('tiling %s has no reference equivalent (odd factor)' % args.tiling)
+    g = '%d %d %d' % (t[0] // 2, t[1] // 2, t[2] // 2)
+    env = dict(os.environ, OMP_NUM_THREADS=str(n_threads), OPENBLAS_NUM_THREADS='1')
+    cmd = [exe, '-g', g, '-m', '2', '-n', str(steps), '-N', '1', '-r', '0.5', '-k', str(args.delay),
+           '-w', str(n_threads), '-x', '0']
+    with tempfile.TemporaryDirectory() as d:  # the driver writes info_*.xml into its working directory
+        r = subprocess.run(cmd, cwd=d, env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError('reference miniqmc exited %d: %s' % (r.returncode, r.stderr[-300:]))
+    m = re.search(r'Diffusion throughput \( N_walkers \* N_elec\^3 / Diffusion time \) = ([0-9.eE+-]+)', r.stdout)
+    if not m:
+        raise RuntimeError('no Diffusion throughput line in the reference output')
+    n_elec = 12 * 32 * (t[0] // 2) * (t[1] // 2) * (t[2] // 2)
+    rate = float(m.group(1)) * steps / float(n_elec) ** 2
+    desc = ('reference miniqmc %s (%s build, -ffast-math -O3, OpenBLAS): -g "%s" -m 2 -k %d -w %d -n %d -x 0, '
+            'one walker per thread' % (os.path.basename(exe), 'mixed-precision' if mixed else 'FP64', g,
+                                       args.delay, n_threads, steps))
+    return rate, desc
+
+
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own miniqmc Release build on all
+    host cores (rank 0 only), each timed step one MC step of its walkers; its
+    mixed-precision build and the FP64 oracle port are reported beside it."""
     if rank != 0:
         return
     ncpu = os.cpu_count() or 1
-    os.environ.setdefault('OMP_NUM_THREADS', str(ncpu))
-    sample = args.cpu_walkers or ncpu
-    vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(args, ncpu, sample)
-    for _ in range(args.steps):
-        v, desc = cpu_baseline(args, ncpu, sample)
-        vals.append(v)
-    v = float(np.mean(vals))
+    try:
+        v, desc = reference_miniqmc(args, ncpu, args.steps)
+        kind = 'reference'
+    except Exception as ex:
+        print(json.dumps({'impl': 'reference', 'unavailable': 'reference miniqmc: %s' % ex}), flush=True)
+        return
+    extra = {}
+    try:
+        mv, mdesc = reference_miniqmc(args, ncpu, args.steps, mixed=True)
+        extra['reference_mixed'] = {'value': mv, 'unit': 'electron-moves/s', 'sample': mdesc}
+    except Exception as ex:
+        extra['reference_mixed'] = {'value': None, 'note': str(ex)}
     tiling = args.tiling
     print(json.dumps({
         'impl': 'reference', 'metric': 'electron-moves/s', 'value': v, 'unit': 'electron-moves/s',
         'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-        'config': {'workload': 'NiO %s (4-atom cell), 1536 e-, k=%d' % (tiling, args.delay)},
-        'cpu_baseline': {'value': v, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'port', 'sample': desc},
+        'config': {'workload': 'NiO %s (4-atom cell) = reference -g "%s": 1536 e-, k=%d' %
+                   (tiling, ' '.join(str(int(x) // 2) for x in tiling.split(',')), args.delay)},
+        'cpu_baseline': {'value': v, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': kind, 'sample': desc},
         'e2e': {'value': v, 'unit': 'electron-moves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
-        'note': 'the reference needs an external BLAS/LAPACK and CMake; its algorithm is timed as the CPU oracle port'
-    }), flush=True)
+        **extra}), flush=True)
 
 
 def main():
@@ -510,7 +644,11 @@ def main():
     ms_total = tmax * 1e3
     a = float((acc - acc0).sum()) / (W * N * args.steps)
 
-    # e2e through the public API: host random streams in, results out
+    # e2e through the public API: host random streams in, results out.  The
+    # streams come from the host (QMC_RNG_HOST), so the device's own stream
+    # generation is not part of this number.  The window starts at the same
+    # phase of the FP64 refresh cycle as the device-timed one, so both hold
+    # the same number of refreshes.
     e2e = None
     if not args.no_e2e:
         rs = np.random.default_rng(5 + rank)
@@ -518,7 +656,11 @@ def main():
         de = np.ascontiguousarray(rs.normal(size=(1, W, 1, N, 3)))
         pin_ur = torch.from_numpy(ur).pin_memory().numpy()
         pin_de = torch.from_numpy(de).pin_memory().numpy()
-        walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de, recompute_every=args.recompute_every)  # warm
+        R = args.recompute_every
+        done = args.warmup + args.steps
+        n_warm = 1 + ((args.warmup - done - 1) % R if R > 0 else 0)
+        for _ in range(n_warm):
+            walkers.sweep(1, 1, 0.5, ur=pin_ur, delta=pin_de, recompute_every=R)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -563,6 +705,18 @@ def main():
                   'achieved': ach, 'peak': tf32_peak, 'unit': 'TFLOP/s', 'frac': ach / tf32_peak,
                   'peak_kind': pk_kind + ' bf16 / 2',
                   'ncu_pipe_tensor_cycles_active_pct': 0.75}
+    error, batched = None, None
+    if rank == 0 and world == 1 and args.precision == 'mixed' and (args.error_walkers > 0 or args.fp64_steps > 0):
+        _, fp64_sys = fp64_reference_system(lib, args, api, capi)
+        if args.error_walkers > 0:
+            error = mixed_form_error(lib, args, api, capi, spec, system, fp64_sys)
+        if args.fp64_steps > 0:
+            bv, bms = batched_fp64_form(lib, args, api, fp64_sys, torch.cuda.Stream)
+            batched = {'value': bv, 'unit': 'electron-moves/s', 'ms_per_step': bms,
+                       'form': 'FP64 fused batched sweep, %d walkers, delay %d, CUDA-core flush, same grid'
+                               % (W, args.delay),
+                       'steps_timed': args.fp64_steps, 'value_over_batched_fp64': value / bv}
+        fp64_sys.close()
     plain = None
     if rank == 0 and world == 1 and args.plain_steps > 0:
         pv, pms = plain_fp64_form(lib, args, api, capi, torch.cuda.Stream)
@@ -572,12 +726,18 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ncpu = os.cpu_count() or 1
-        try:
-            v, desc = cpu_baseline(args, ncpu, args.cpu_walkers or ncpu)
-            cpu = {'value': v, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'port', 'sample': desc}
+        try:  # the reference's own miniqmc (2 MC steps of one walker per core)
+            v, desc = reference_miniqmc(args, ncpu, 2)
+            cpu = {'value': v, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'reference', 'sample': desc}
         except Exception as ex:  # the baseline is reported, never required
-            cpu = {'value': None, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'port',
+            cpu = {'value': None, 'unit': 'electron-moves/s', 'cores': ncpu, 'kind': 'reference',
                    'sample': 'failed: %s' % ex}
+        if args.port_baseline:
+            try:
+                v, desc = cpu_baseline(args, ncpu, args.cpu_walkers or ncpu)
+                cpu['port'] = {'value': v, 'kind': 'port', 'sample': desc}
+            except Exception as ex:
+                cpu['port'] = {'value': None, 'sample': 'failed: %s' % ex}
     if rank == 0:
         out = {
             'metric': 'electron-moves/s', 'value': value, 'unit': 'electron-moves/s', 'n_gpus': world,
@@ -595,7 +755,7 @@ def main():
                        'flush': args.flush if args.precision == 'mixed' else 'simt',
                        'recompute_every': args.recompute_every, 'recompute_ms': recompute_ms},
             'roofline': roofline, 'tensor': tensor, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk,
-            'plain_fp64': plain,
+            'plain_fp64': plain, 'batched_fp64': batched, 'error': error,
             'gpu_launches': launches,
         }
         print(json.dumps(out), flush=True)

@@ -315,6 +315,19 @@ int oracle_spo_evaluate_v(oracle_system* o, int n_pos, const double* pos, double
 }
 
 // ------------------------------------------------------------- walkers --
+// Oracle only: the arithmetic of the orbital and determinant path of the
+// walkers created afterwards on this system (each walker keeps the flags it
+// was created with; ARITH_* of qmc_oracle.hpp, 0 = FP64).  ARITH_SPO32 |
+// ARITH_DET32 | ARITH_LOG32 restates the reference's mixed-precision build
+// of that path.
+int oracle_system_set_arith(oracle_system* s, int flags)
+{
+  if (!s || flags < 0 || flags > (ARITH_SPO32 | ARITH_DET32 | ARITH_LOG32))
+    return QMC_ERR_ARG;
+  s->sys.arith = flags;
+  return 0;
+}
+
 int oracle_walkers_create(oracle_system* s, int W, int k, oracle_walkers** out)
 {
   if (!s || W <= 0 || k <= 0 || k > s->sys.norb)
@@ -499,6 +512,12 @@ int oracle_wf_get_inverse(oracle_walkers* o, int walker, int spin, double* psiM)
   Walker& w = o->w[walker];
   // apply pending delayed rows on a copy (the state itself is untouched)
   Walker::Det d = w.det[spin];
+  if (w.arith & ARITH_DET32)
+  {
+    d.eng32.updateInvMat(d.psiM32.data());
+    std::copy(d.psiM32.begin(), d.psiM32.end(), psiM);
+    return 0;
+  }
   d.eng.updateInvMat(d.psiM.data());
   std::copy(d.psiM.begin(), d.psiM.end(), psiM);
   return 0;

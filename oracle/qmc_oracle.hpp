@@ -606,41 +606,42 @@ struct Spline
       c = (double)(float)c;
   }
 
-  // getSplineBound (MultiBsplineEvalHelper.hpp:43-64)
-  static void bound(double x, double& dx, int& ind, int nmax)
+  // getSplineBound (MultiBsplineEvalHelper.hpp:43-64), in the evaluation
+  // type T (double, or float for the reference's mixed build)
+  template <typename T> static void bound(T x, T& dx, int& ind, int nmax)
   {
     if (x < 0)
     {
       ind = 0;
-      dx  = 0.0;
+      dx  = T(0);
     }
     else
     {
-      double ipart;
+      T ipart;
       dx  = std::modf(x, &ipart);
       ind = static_cast<int>(ipart);
       if (ind > nmax)
       {
         ind = nmax;
-        dx  = 1.0 - std::numeric_limits<double>::epsilon();
+        dx  = T(1) - std::numeric_limits<T>::epsilon();
       }
     }
   }
-  // MultiBsplineData<double>::compute_prefactors (MultiBsplineData.hpp:52-80)
-  static void prefactors(double a[4], double da[4], double d2a[4], double tx)
+  // MultiBsplineData<T>::compute_prefactors (MultiBsplineData.hpp:52-80)
+  template <typename T> static void prefactors(T a[4], T da[4], T d2a[4], T tx)
   {
-    const double A00 = -1.0 / 6.0, A01 = 3.0 / 6.0, A02 = -3.0 / 6.0, A03 = 1.0 / 6.0;
-    const double A10 = 3.0 / 6.0, A11 = -6.0 / 6.0, A12 = 0.0 / 6.0, A13 = 4.0 / 6.0;
-    const double A20 = -3.0 / 6.0, A21 = 3.0 / 6.0, A22 = 3.0 / 6.0, A23 = 1.0 / 6.0;
-    const double A30 = 1.0 / 6.0, A31 = 0.0 / 6.0, A32 = 0.0 / 6.0, A33 = 0.0 / 6.0;
-    const double dA01 = -0.5, dA02 = 1.0, dA03 = -0.5;
-    const double dA11 = 1.5, dA12 = -2.0, dA13 = 0.0;
-    const double dA21 = -1.5, dA22 = 1.0, dA23 = 0.5;
-    const double dA31 = 0.5, dA32 = 0.0, dA33 = 0.0;
-    const double d2A02 = -1.0, d2A03 = 1.0;
-    const double d2A12 = 3.0, d2A13 = -2.0;
-    const double d2A22 = -3.0, d2A23 = 1.0;
-    const double d2A32 = 1.0, d2A33 = 0.0;
+    const T A00 = -1.0 / 6.0, A01 = 3.0 / 6.0, A02 = -3.0 / 6.0, A03 = 1.0 / 6.0;
+    const T A10 = 3.0 / 6.0, A11 = -6.0 / 6.0, A12 = 0.0 / 6.0, A13 = 4.0 / 6.0;
+    const T A20 = -3.0 / 6.0, A21 = 3.0 / 6.0, A22 = 3.0 / 6.0, A23 = 1.0 / 6.0;
+    const T A30 = 1.0 / 6.0, A31 = 0.0 / 6.0, A32 = 0.0 / 6.0, A33 = 0.0 / 6.0;
+    const T dA01 = -0.5, dA02 = 1.0, dA03 = -0.5;
+    const T dA11 = 1.5, dA12 = -2.0, dA13 = 0.0;
+    const T dA21 = -1.5, dA22 = 1.0, dA23 = 0.5;
+    const T dA31 = 0.5, dA32 = 0.0, dA33 = 0.0;
+    const T d2A02 = -1.0, d2A03 = 1.0;
+    const T d2A12 = 3.0, d2A13 = -2.0;
+    const T d2A22 = -3.0, d2A23 = 1.0;
+    const T d2A32 = 1.0, d2A33 = 0.0;
     a[0]   = ((A00 * tx + A01) * tx + A02) * tx + A03;
     a[1]   = ((A10 * tx + A11) * tx + A12) * tx + A13;
     a[2]   = ((A20 * tx + A21) * tx + A22) * tx + A23;
@@ -654,14 +655,14 @@ struct Spline
     d2a[2] = d2A22 * tx + d2A23;
     d2a[3] = d2A32 * tx + d2A33;
   }
-  void locate(const Vec3& u, int idx[3], double a[3][4], double da[3][4], double d2a[3][4]) const
+  template <typename T> void locate(const Vec3& u, int idx[3], T a[3][4], T da[3][4], T d2a[3][4]) const
   {
     const int ng[3] = {nx, ny, nz};
     for (int d = 0; d < 3; ++d)
     {
-      double t;
-      bound(u[d] * delta_inv[d], t, idx[d], ng[d] - 1);
-      prefactors(a[d], da[d], d2a[d], t);
+      T t;
+      bound<T>((T)u[d] * (T)delta_inv[d], t, idx[d], ng[d] - 1);
+      prefactors<T>(a[d], da[d], d2a[d], t);
     }
   }
   // evaluate_v (MultiBspline.hpp:34-63)
@@ -669,7 +670,7 @@ struct Spline
   {
     int id[3];
     double a[3][4], da[3][4], d2a[3][4];
-    locate(u, id, a, da, d2a);
+    locate<double>(u, id, a, da, d2a);
     std::fill(vals, vals + norb, 0.0);
     for (int i = 0; i < 4; i++)
       for (int j = 0; j < 4; j++)
@@ -684,16 +685,22 @@ struct Spline
   // evaluate_vgh (MultiBspline.hpp:163-280): g[3][norb], h[6][norb]
   void evaluate_vgh(const Vec3& u, double* vals, double* g, double* h) const
   {
+    evaluate_vgh_t<double>(u, vals, g, h);
+  }
+  // the same in the evaluation type T: T = float restates MultiBspline<float>
+  // of the reference's mixed build (FP32 unit coordinates, prefactors and
+  // accumulators over an FP32 table; the outputs are widened to double)
+  template <typename T> void evaluate_vgh_t(const Vec3& u, double* vals, double* g, double* h) const
+  {
     int id[3];
-    double a[3][4], da[3][4], d2a[3][4];
-    locate(u, id, a, da, d2a);
+    T a[3][4], da[3][4], d2a[3][4];
+    locate<T>(u, id, a, da, d2a);
     const size_t o = norb;
-    std::fill(vals, vals + o, 0.0);
-    std::fill(g, g + 3 * o, 0.0);
-    std::fill(h, h + 6 * o, 0.0);
-    double *gx = g, *gy = g + o, *gz = g + 2 * o;
-    double *hxx = h, *hxy = h + o, *hxz = h + 2 * o, *hyy = h + 3 * o, *hyz = h + 4 * o, *hzz = h + 5 * o;
-    const double *c0 = a[2], *dc = da[2], *d2c = d2a[2];
+    std::vector<T> acc(10 * o, T(0));
+    T *vv = acc.data(), *gx = vv + o, *gy = vv + 2 * o, *gz = vv + 3 * o;
+    T *hxx = vv + 4 * o, *hxy = vv + 5 * o, *hxz = vv + 6 * o, *hyy = vv + 7 * o, *hyz = vv + 8 * o,
+      *hzz = vv + 9 * o;
+    const T *c0 = a[2], *dc = da[2], *d2c = d2a[2];
     for (int i = 0; i < 4; i++)
       for (int j = 0; j < 4; j++)
       {
@@ -701,18 +708,18 @@ struct Spline
         const double* coefs1 = coefs0 + zs;
         const double* coefs2 = coefs0 + 2 * zs;
         const double* coefs3 = coefs0 + 3 * zs;
-        const double pre20   = d2a[0][i] * a[1][j];
-        const double pre10   = da[0][i] * a[1][j];
-        const double pre00   = a[0][i] * a[1][j];
-        const double pre11   = da[0][i] * da[1][j];
-        const double pre01   = a[0][i] * da[1][j];
-        const double pre02   = a[0][i] * d2a[1][j];
+        const T pre20        = d2a[0][i] * a[1][j];
+        const T pre10        = da[0][i] * a[1][j];
+        const T pre00        = a[0][i] * a[1][j];
+        const T pre11        = da[0][i] * da[1][j];
+        const T pre01        = a[0][i] * da[1][j];
+        const T pre02        = a[0][i] * d2a[1][j];
         for (int n = 0; n < norb; n++)
         {
-          double v0 = coefs0[n], v1 = coefs1[n], v2 = coefs2[n], v3 = coefs3[n];
-          double sum0 = c0[0] * v0 + c0[1] * v1 + c0[2] * v2 + c0[3] * v3;
-          double sum1 = dc[0] * v0 + dc[1] * v1 + dc[2] * v2 + dc[3] * v3;
-          double sum2 = d2c[0] * v0 + d2c[1] * v1 + d2c[2] * v2 + d2c[3] * v3;
+          T v0 = (T)coefs0[n], v1 = (T)coefs1[n], v2 = (T)coefs2[n], v3 = (T)coefs3[n];
+          T sum0 = c0[0] * v0 + c0[1] * v1 + c0[2] * v2 + c0[3] * v3;
+          T sum1 = dc[0] * v0 + dc[1] * v1 + dc[2] * v2 + dc[3] * v3;
+          T sum2 = d2c[0] * v0 + d2c[1] * v1 + d2c[2] * v2 + d2c[3] * v3;
           hxx[n] += pre20 * sum0;
           hxy[n] += pre11 * sum0;
           hxz[n] += pre10 * sum1;
@@ -722,23 +729,24 @@ struct Spline
           gx[n] += pre10 * sum0;
           gy[n] += pre01 * sum0;
           gz[n] += pre00 * sum1;
-          vals[n] += pre00 * sum0;
+          vv[n] += pre00 * sum0;
         }
       }
-    const double dxInv = delta_inv[0], dyInv = delta_inv[1], dzInv = delta_inv[2];
-    const double dxx = dxInv * dxInv, dyy = dyInv * dyInv, dzz = dzInv * dzInv;
-    const double dxy = dxInv * dyInv, dxz = dxInv * dzInv, dyz = dyInv * dzInv;
+    const T dxInv = (T)delta_inv[0], dyInv = (T)delta_inv[1], dzInv = (T)delta_inv[2];
+    const T dxx = dxInv * dxInv, dyy = dyInv * dyInv, dzz = dzInv * dzInv;
+    const T dxy = dxInv * dyInv, dxz = dxInv * dzInv, dyz = dyInv * dzInv;
     for (size_t n = 0; n < o; n++)
     {
-      gx[n] *= dxInv;
-      gy[n] *= dyInv;
-      gz[n] *= dzInv;
-      hxx[n] *= dxx;
-      hyy[n] *= dyy;
-      hzz[n] *= dzz;
-      hxy[n] *= dxy;
-      hxz[n] *= dxz;
-      hyz[n] *= dyz;
+      vals[n]      = vv[n];
+      g[n]         = gx[n] * dxInv;
+      g[o + n]     = gy[n] * dyInv;
+      g[2 * o + n] = gz[n] * dzInv;
+      h[n]         = hxx[n] * dxx;
+      h[o + n]     = hxy[n] * dxy;
+      h[2 * o + n] = hxz[n] * dxz;
+      h[3 * o + n] = hyy[n] * dyy;
+      h[4 * o + n] = hyz[n] * dyz;
+      h[5 * o + n] = hzz[n] * dzz;
     }
   }
 };
@@ -830,28 +838,33 @@ inline bool invert_transpose(int n, const double* A, double* psiM, double& logde
 }
 
 // ------------------------------------------------------ DelayedUpdate ---
-// DelayedUpdate<double,double> (DelayedUpdate.h:28-231), row-major.
-struct DelayedUpdate
+// DelayedUpdate<T,T_FP> (DelayedUpdate.h:28-231), row-major.  T = double is
+// the FP64 build; T = float restates the arithmetic of the reference's
+// mixed-precision build (QMC_MIXED_PRECISION: ValueType float, so U, V,
+// Binv, tempMat and every product and dot of the getInvRow / acceptRow /
+// updateInvMat GEMVs and GEMMs are FP32; the inverse itself is the FP64
+// DiracMatrix<T_FP>).
+template <typename T> struct DelayedUpdateT
 {
   int norb = 0, kmax = 0, delay_count = 0;
-  std::vector<double> U, V, Binv, tempMat, p, temp;
+  std::vector<T> U, V, Binv, tempMat, p, temp;
   std::vector<int> delay_list;
 
   void resize(int n, int delay)
   {
     norb = n;
     kmax = delay;
-    U.assign((size_t)delay * n, 0.0);
-    V.assign((size_t)delay * n, 0.0);
-    Binv.assign((size_t)delay * delay, 0.0);
-    tempMat.assign((size_t)n * delay, 0.0);
-    p.assign(delay, 0.0);
-    temp.assign(n, 0.0);
+    U.assign((size_t)delay * n, T(0));
+    V.assign((size_t)delay * n, T(0));
+    Binv.assign((size_t)delay * delay, T(0));
+    tempMat.assign((size_t)n * delay, T(0));
+    p.assign(delay, T(0));
+    temp.assign(n, T(0));
     delay_list.assign(delay, 0);
     delay_count = 0;
   }
   // getInvRow (DelayedUpdate.h:95-114)
-  void getInvRow(const double* Ainv, int rowchanged, double* invRow)
+  void getInvRow(const T* Ainv, int rowchanged, T* invRow)
   {
     const int n = norb, k = kmax, dc = delay_count;
     std::copy_n(Ainv + (size_t)rowchanged * n, n, invRow);
@@ -859,30 +872,30 @@ struct DelayedUpdate
       return;
     for (int d = 0; d < dc; ++d)
     {
-      double s = 0.0;
+      T s = T(0);
       for (int j = 0; j < n; ++j)
         s += U[(size_t)d * n + j] * invRow[j];
       p[d] = s;
     }
-    double* w = &Binv[(size_t)dc * k]; // Binv[delay_count] holds the product
+    T* w = &Binv[(size_t)dc * k]; // Binv[delay_count] holds the product
     if (dc < k)
       for (int a = 0; a < dc; ++a)
       {
-        double s = 0.0;
+        T s = T(0);
         for (int b = 0; b < dc; ++b)
           s += Binv[(size_t)b * k + a] * p[b];
         w[a] = s;
       }
     for (int j = 0; j < n; ++j)
     {
-      double s = 0.0;
+      T s = T(0);
       for (int d = 0; d < dc; ++d)
         s += V[(size_t)d * n + j] * w[d];
       invRow[j] -= s;
     }
   }
   // acceptRow (DelayedUpdate.h:123-153)
-  void acceptRow(double* Ainv, int rowchanged, const double* psiV)
+  void acceptRow(T* Ainv, int rowchanged, const T* psiV)
   {
     const int n = norb, k = kmax, dc = delay_count;
     std::copy_n(Ainv + (size_t)rowchanged * n, n, &V[(size_t)dc * n]);
@@ -890,18 +903,18 @@ struct DelayedUpdate
     delay_list[dc] = rowchanged;
     for (int d = 0; d <= dc; ++d)
     {
-      double s = 0.0;
+      T s = T(0);
       for (int j = 0; j < n; ++j)
         s += V[(size_t)d * n + j] * psiV[j];
       p[d] = -s;
     }
-    double y = -p[dc];
+    T y = -p[dc];
     for (int i = 0; i < dc; i++)
       y += Binv[(size_t)dc * k + i] * p[i];
-    Binv[(size_t)dc * k + dc] = y = 1.0 / y;
+    Binv[(size_t)dc * k + dc] = y = T(1) / y;
     for (int b = 0; b < dc; ++b)
     {
-      double s = 0.0;
+      T s = T(0);
       for (int a = 0; a < dc; ++a)
         s += Binv[(size_t)b * k + a] * p[a];
       Binv[(size_t)b * k + dc] = y * s;
@@ -916,7 +929,7 @@ struct DelayedUpdate
       updateInvMat(Ainv);
   }
   // updateInvMat (DelayedUpdate.h:155-231)
-  void updateInvMat(double* Ainv)
+  void updateInvMat(T* Ainv)
   {
     const int n = norb, k = kmax, dc = delay_count;
     if (dc == 0)
@@ -925,13 +938,13 @@ struct DelayedUpdate
     {
       for (int i = 0; i < n; ++i)
       {
-        double s = 0.0;
+        T s = T(0);
         for (int j = 0; j < n; ++j)
           s += Ainv[(size_t)i * n + j] * U[j];
         temp[i] = s;
       }
-      temp[delay_list[0]] -= 1.0;
-      const double b00 = Binv[0];
+      temp[delay_list[0]] -= T(1);
+      const T b00 = Binv[0];
       for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j)
           Ainv[(size_t)i * n + j] += -b00 * V[j] * temp[i];
@@ -941,18 +954,18 @@ struct DelayedUpdate
       for (int i = 0; i < n; ++i)
         for (int d = 0; d < dc; ++d)
         {
-          double s = 0.0;
+          T s = T(0);
           for (int j = 0; j < n; ++j)
             s += U[(size_t)d * n + j] * Ainv[(size_t)i * n + j];
           tempMat[(size_t)i * k + d] = s;
         }
       for (int d = 0; d < dc; d++)
-        tempMat[(size_t)delay_list[d] * k + d] -= 1.0;
-      std::vector<double> U2((size_t)dc * n, 0.0);
+        tempMat[(size_t)delay_list[d] * k + d] -= T(1);
+      std::vector<T> U2((size_t)dc * n, T(0));
       for (int b = 0; b < dc; ++b)
         for (int a = 0; a < dc; ++a)
         {
-          const double bba = Binv[(size_t)b * k + a];
+          const T bba = Binv[(size_t)b * k + a];
           for (int j = 0; j < n; ++j)
             U2[(size_t)b * n + j] += bba * V[(size_t)a * n + j];
         }
@@ -960,7 +973,7 @@ struct DelayedUpdate
       for (int i = 0; i < n; ++i)
         for (int d = 0; d < dc; ++d)
         {
-          const double t = tempMat[(size_t)i * k + d];
+          const T t = tempMat[(size_t)i * k + d];
           for (int j = 0; j < n; ++j)
             Ainv[(size_t)i * n + j] -= t * U2[(size_t)d * n + j];
         }
@@ -968,6 +981,7 @@ struct DelayedUpdate
     delay_count = 0;
   }
 };
+using DelayedUpdate = DelayedUpdateT<double>;
 
 // -------------------------------------------------- PolynomialFunctor3D --
 // The eeI functor of the three-body Jastrow (PolynomialFunctor3D.h:38-560)
@@ -1150,6 +1164,22 @@ struct J3Func
 };
 
 // ------------------------------------------------------------ System ---
+// ARITH_SPO32: the orbitals are evaluated in FP32 arithmetic (MultiBspline<
+//   float>, the reference's mixed build; einspline_spo.hpp:172-223).
+// ARITH_DET32: the determinant's inverse, delayed rows and every dot and
+//   product of DiracDeterminant / DelayedUpdate in FP32 (ValueType float),
+//   the LU inverse in FP64 and rounded to FP32 (DiracMatrix<double>::
+//   invert_transpose of the mixed build, DiracMatrix.h:93-119 with
+//   MIXED_PRECISION, DiracDeterminant.cpp:30-60).
+// ARITH_LOG32: the log|det| accumulation of acceptMove in FP32 (LogValue is
+//   RealType = float in the mixed build, DiracDeterminant.cpp:129-146).
+enum
+{
+  ARITH_SPO32 = 1,
+  ARITH_DET32 = 2,
+  ARITH_LOG32 = 4
+};
+
 struct System
 {
   Lattice lattice;     // simulation cell (electrons and ions)
@@ -1160,6 +1190,11 @@ struct System
   std::vector<int> group_first, group_last;
   Spline spline;
   int lap_mode = 0;
+  // arithmetic of the orbital and determinant path of the walkers created
+  // next (ARITH_* flags; 0 is FP64 throughout): restates the reference's
+  // mixed-precision build piece by piece, so that each piece's share of the
+  // error can be measured
+  int arith = 0;
   bool use_det = true, use_j1 = true, use_j2 = true, use_j3 = false;
   std::vector<Functor> j1; // per ion group
   Functor j2_uu, j2_ud;
@@ -1226,6 +1261,10 @@ struct Walker
     int invRow_id = -1;
     bool partial  = false; // UpdateMode == ORB_PBYP_PARTIAL
     DelayedUpdate eng;
+    // ARITH_DET32: the FP32 inverse and delayed rows (psiM above then holds
+    // the same values widened, for evaluateGL and the inverse read-out)
+    std::vector<float> psiM32, invRow32, psiV32;
+    DelayedUpdateT<float> eng32;
   } det[2];
 
   // J1 (OneBodyJastrow.h:110-283)
@@ -1243,9 +1282,11 @@ struct Walker
   std::vector<double> G, L; // [N][3], [N]
   double LogValue = 0.0;
 
+  int arith = 0; // ARITH_* of the system when this walker was created
   void init(const System* s, int delay)
   {
     sys         = s;
+    arith       = s->arith;
     const int N = s->n_elec, I = s->n_ions;
     R.assign((size_t)N * 3, 0.0);
     for (auto* v : {&aa_r, &aa_dx, &aa_dy, &aa_dz, &row_r, &row_dx, &row_dy, &row_dz})
@@ -1267,6 +1308,13 @@ struct Walker
       d.d2psiV.assign(n, 0.0);
       d.invRow.assign(n, 0.0);
       d.eng.resize(d.n, delay);
+      if (arith & ARITH_DET32)
+      {
+        d.psiM32.assign(n * n, 0.f);
+        d.invRow32.assign(n, 0.f);
+        d.psiV32.assign(n, 0.f);
+        d.eng32.resize(d.n, delay);
+      }
     }
     j1_Vat.assign(N, 0.0);
     j1_Grad.assign((size_t)N * 3, 0.0);
@@ -1323,7 +1371,10 @@ struct Walker
     const int n = sys->norb;
     std::vector<double> v(n), g(3 * n), h(6 * n);
     Vec3 u = sys->spo_lattice.toUnit_floor(r);
-    sys->spline.evaluate_vgh(u, v.data(), g.data(), h.data());
+    if (arith & ARITH_SPO32)
+      sys->spline.evaluate_vgh_t<float>(u, v.data(), g.data(), h.data());
+    else
+      sys->spline.evaluate_vgh(u, v.data(), g.data(), h.data());
     for (int j = 0; j < n; ++j)
     {
       psi[j]          = v[j];
@@ -1340,6 +1391,20 @@ struct Walker
   }
 
   // ---- determinant ----
+  bool det32() const { return (arith & ARITH_DET32) != 0; }
+  // ARITH_DET32: the FP32 inverse widened into psiM (after every change)
+  void det_widen(Det& d)
+  {
+    for (size_t i = 0; i < d.psiM32.size(); ++i)
+      d.psiM[i] = d.psiM32[i];
+  }
+  // FP32 storage of the orbital rows the FP32 determinant keeps
+  void det_round_rows(double* p, size_t count) const
+  {
+    if (det32())
+      for (size_t i = 0; i < count; ++i)
+        p[i] = (double)(float)p[i];
+  }
   bool det_recompute(int s)
   {
     Det& d      = det[s];
@@ -1347,8 +1412,20 @@ struct Walker
     for (int i = 0; i < n; ++i)
       spo_vgh(activeR(d.first + i), &d.psiM_temp[(size_t)i * n], &d.dpsiM[(size_t)i * n * 3],
               &d.d2psiM[(size_t)i * n]);
+    det_round_rows(d.psiM_temp.data(), d.psiM_temp.size());
+    det_round_rows(d.dpsiM.data(), d.dpsiM.size());
+    det_round_rows(d.d2psiM.data(), d.d2psiM.size());
     bool ok = invert_transpose(n, d.psiM_temp.data(), d.psiM.data(), d.LogValue, d.PhaseValue);
     d.eng.delay_count = 0;
+    if (det32())
+    {
+      for (size_t i = 0; i < d.psiM.size(); ++i)
+        d.psiM32[i] = (float)d.psiM[i];
+      det_widen(d);
+      d.eng32.delay_count = 0;
+      if (arith & ARITH_LOG32)
+        d.LogValue = (double)(float)d.LogValue;
+    }
     return ok;
   }
   Vec3 det_evalGrad(int s, int iat)
@@ -1356,6 +1433,18 @@ struct Walker
     Det& d      = det[s];
     const int r = iat - d.first, n = d.n;
     d.invRow_id = r;
+    if (det32())
+    {
+      d.eng32.getInvRow(d.psiM32.data(), r, d.invRow32.data());
+      float gf[3] = {0.f, 0.f, 0.f};
+      const double* dp = &d.dpsiM[(size_t)r * n * 3];
+      for (int j = 0; j < n; ++j)
+        for (int c = 0; c < 3; ++c)
+          gf[c] += d.invRow32[j] * (float)dp[3 * j + c];
+      for (int j = 0; j < n; ++j)
+        d.invRow[j] = d.invRow32[j];
+      return Vec3{gf[0], gf[1], gf[2]};
+    }
     d.eng.getInvRow(d.psiM.data(), r, d.invRow.data());
     Vec3 g{0, 0, 0};
     const double* dp = &d.dpsiM[(size_t)r * n * 3];
@@ -1370,6 +1459,32 @@ struct Walker
     const int r = iat - d.first, n = d.n;
     spo_vgh(activeR(iat), d.psiV.data(), d.dpsiV.data(), d.d2psiV.data());
     d.partial = true;
+    if (det32())
+    {
+      // DiracDeterminant::ratioGrad in FP32 (DiracDeterminant.cpp:80-122)
+      det_round_rows(d.psiV.data(), n);
+      det_round_rows(d.dpsiV.data(), 3 * (size_t)n);
+      det_round_rows(d.d2psiV.data(), n);
+      for (int j = 0; j < n; ++j)
+        d.psiV32[j] = (float)d.psiV[j];
+      if (d.invRow_id != r)
+      {
+        d.invRow_id = r;
+        d.eng32.getInvRow(d.psiM32.data(), r, d.invRow32.data());
+      }
+      float ratio = 0.f;
+      for (int j = 0; j < n; ++j)
+        ratio += d.invRow32[j] * d.psiV32[j];
+      d.curRatio = ratio;
+      float gf[3] = {0.f, 0.f, 0.f};
+      for (int j = 0; j < n; ++j)
+        for (int c = 0; c < 3; ++c)
+          gf[c] += d.invRow32[j] * (float)d.dpsiV[3 * j + c];
+      const float rinv = 1.f / ratio;
+      for (int c = 0; c < 3; ++c)
+        grad[c] += (double)(rinv * gf[c]);
+      return ratio;
+    }
     if (d.invRow_id != r)
     {
       d.invRow_id = r;
@@ -1394,6 +1509,22 @@ struct Walker
     const int r = iat - d.first, n = d.n;
     spo_v(activeR(iat), d.psiV.data());
     d.partial = false;
+    if (det32())
+    {
+      det_round_rows(d.psiV.data(), n);
+      for (int j = 0; j < n; ++j)
+        d.psiV32[j] = (float)d.psiV[j];
+      if (d.invRow_id != r)
+      {
+        d.invRow_id = r;
+        d.eng32.getInvRow(d.psiM32.data(), r, d.invRow32.data());
+      }
+      float ratio = 0.f;
+      for (int j = 0; j < n; ++j)
+        ratio += d.invRow32[j] * d.psiV32[j];
+      d.curRatio = ratio;
+      return ratio;
+    }
     if (d.invRow_id != r)
     {
       d.invRow_id = r;
@@ -1410,8 +1541,18 @@ struct Walker
     Det& d      = det[s];
     const int r = iat - d.first, n = d.n;
     d.PhaseValue += (d.curRatio > 0) ? 0.0 : kPi;
-    d.LogValue += std::log(std::abs(d.curRatio));
-    d.eng.acceptRow(d.psiM.data(), r, d.psiV.data());
+    if (arith & ARITH_LOG32)
+      d.LogValue = (double)((float)d.LogValue + std::log(std::abs((float)d.curRatio)));
+    else
+      d.LogValue += std::log(std::abs(d.curRatio));
+    if (det32())
+    {
+      d.eng32.acceptRow(d.psiM32.data(), r, d.psiV32.data());
+      if (d.eng32.delay_count == 0) // the delay was full: updateInvMat ran
+        det_widen(d);
+    }
+    else
+      d.eng.acceptRow(d.psiM.data(), r, d.psiV.data());
     d.invRow_id = -1;
     if (d.partial)
     {
@@ -1423,7 +1564,13 @@ struct Walker
   void det_complete(int s)
   {
     det[s].invRow_id = -1;
-    det[s].eng.updateInvMat(det[s].psiM.data());
+    if (det32())
+    {
+      det[s].eng32.updateInvMat(det[s].psiM32.data());
+      det_widen(det[s]);
+    }
+    else
+      det[s].eng.updateInvMat(det[s].psiM.data());
   }
   void det_GL(int s)
   {

@@ -1,9 +1,11 @@
-# Compiles the reference's own sources (from /root/reference/src, read-only)
-# with the golden-dump driver oracle/ref_harness.cpp into oracle/_ref/.
+# Compiles the reference's own sources (read-only, where MINIQMC_REFERENCE
+# points) with the golden-dump driver oracle/ref_harness.cpp into
+# oracle/_ref/.  Without the reference tree the target is skipped.
 # Test infrastructure only: not the reference's CMake build, no external
 # libraries; the hand-written oracle/ref_harness_config.h replaces the
 # CMake-generated config.h.
-REF ?= /root/reference/src
+MINIQMC_REFERENCE ?= /root/reference
+REF := $(MINIQMC_REFERENCE)/src
 HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
 OUT := $(HERE)_ref
 REF_CXX ?= $(shell test -x /usr/bin/g++ && echo /usr/bin/g++ || echo g++)
@@ -16,7 +18,12 @@ SRCS := $(REF)/Particle/ParticleSet.cpp $(REF)/Particle/ParticleSet.BC.cpp \
         $(REF)/Utilities/InfoStream.cpp $(REF)/Utilities/XMLWriter.cpp \
         $(REF)/Utilities/tinyxml/tinyxml2.cpp
 
+ifeq ($(wildcard $(REF)/Particle/ParticleSet.cpp),)
+all:
+	@echo "reference tree not found (set MINIQMC_REFERENCE): golden-dump harness not built"
+else
 all: $(OUT)/ref_harness
+endif
 
 $(OUT)/include/config.h: $(HERE)ref_harness_config.h
 	mkdir -p $(OUT)/include

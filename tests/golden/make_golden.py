@@ -1,8 +1,8 @@
 """Regenerate the golden fixtures in tests/golden from the reference.
 
-Run in a container that has the reference source tree (default
-/root/reference); the GPU box does not need it because the fixtures are
-committed.  Two sources:
+Run where the reference source tree is (its root given by --reference or the
+MINIQMC_REFERENCE environment variable); the GPU runs do not need it because
+the fixtures are committed.  Two sources:
 
 1. reference_dump.json -- output of oracle/_ref/ref_harness, which is built by
    oracle/ref_harness.mk from the reference's own ParticleSet, distance-table,
@@ -17,7 +17,7 @@ committed.  Two sources:
      src/Particle/tests/test_particle.cpp               (PBC AA distance)
      src/Utilities/tests/test_PrimeNumberSet.cpp        (primes)
 
-Usage:  python tests/golden/make_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_golden.py [--reference <reference root>]
 """
 import argparse
 import json
@@ -106,12 +106,13 @@ def known_answers(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', default=os.environ.get('MINIQMC_REFERENCE'),
+                    help='root of the reference source tree (default: $MINIQMC_REFERENCE)')
     args = ap.parse_args()
-    if not os.path.isdir(args.reference):
-        sys.exit('reference tree not found: %s' % args.reference)
+    if not args.reference or not os.path.isdir(os.path.join(args.reference, 'src')):
+        sys.exit('reference tree not found: pass --reference or set MINIQMC_REFERENCE')
     subprocess.check_call(['make', '-s', '-f', os.path.join(REPO, 'oracle', 'ref_harness.mk'),
-                           'REF=%s' % os.path.join(args.reference, 'src')])
+                           'MINIQMC_REFERENCE=%s' % args.reference])
     dump = subprocess.check_output([os.path.join(REPO, 'oracle', '_ref', 'ref_harness')])
     dump = json.loads(dump)
     dump['_generator'] = 'oracle/ref_harness.cpp compiled from the reference sources'

@@ -18,6 +18,13 @@ GOLDEN = os.path.join(REPO, 'tests', 'golden')
 
 _lib = None
 
+# arithmetic of the oracle's orbital and determinant path (qmc_oracle.hpp
+# ARITH_*): FP32 orbitals, FP32 determinant algebra, FP32 log|det|
+# accumulation; all three together restate the reference's mixed-precision
+# build of that path
+ARITH_SPO32, ARITH_DET32, ARITH_LOG32 = 1, 2, 4
+ARITH_REFERENCE_MIXED = ARITH_SPO32 | ARITH_DET32 | ARITH_LOG32
+
 
 def build():
     src = [os.path.join(REPO, 'oracle', f) for f in ('oracle_capi.cpp', 'qmc_oracle.hpp')]
@@ -43,6 +50,7 @@ def library():
             'walkers_skip': (C.c_int, [C.c_void_p, C.c_int]),
             'num_threads': (C.c_int, []),
             'detengine_delay_count': (C.c_int, [C.c_void_p]),
+            'system_set_arith': (C.c_int, [C.c_void_p, C.c_int]),
         }
         _lib = api.Library(ORACLE_SO, prefix='oracle_', extra=extra)
     return _lib

@@ -1,13 +1,29 @@
-"""Per-quantity error of the mixed-precision form (and of the FP64 form)
-against the FP64 oracle at the NiO-128 size: SPO values / gradients /
-Hessians, log-ratios and gradients of one MC step of all 1536 electrons, and
-the post-sweep drift of the log-determinant accumulated through the ratios
-from a fresh FP64 evaluation at the final positions.
+"""Per-quantity error of the mixed-precision form against FP64 at the NiO-128
+size, and the attribution of that error.
 
-    python tests/precision_report.py [--grid 24,24,12] [--delay 32] > report.json
+Measured, on the same FP32-rounded spline table, positions and random
+streams: SPO values / gradients / Hessians, the log-ratio and gradient of
+every move (with per-step statistics), and the drift of the log-determinant
+accumulated through the ratios from a fresh FP64 evaluation at the same
+positions, after the first MC step and after the last (no refresh between).
 
-Needs a GPU.  The oracle is the checker: both sides see the same
-FP32-rounded spline table and the same random streams."""
+    python tests/precision_report.py [--grid 148,148,74] [--delays 16,32,64]
+        [--walkers 4] [--steps 8] [--oracle-variants spo32,det32,ref_mixed]
+        [--oracle-steps 2] > report.json
+
+Product forms ('tc': mixed with the tensor-core flush, 'simt': mixed with the
+CUDA-core flush) are measured against the product's FP64 form on the mixed
+form's table (QMC_FILL_UNIFORM_F32: the same coefficients rounded to FP32,
+evaluated in FP64; the FP64 parity tests pin it to the oracle at 1e-10).
+
+Oracle variants restate pieces of the reference's own mixed-precision build
+in the CPU oracle (qmc_oracle.hpp ARITH_*) and are measured against the FP64
+oracle on the same table: 'spo32' FP32 orbital evaluation with an FP64
+determinant; 'det32' FP64 orbitals with the FP32 determinant algebra
+(DelayedUpdate<float, double>: FP32 inverse, delayed rows, Binv, GEMVs and
+GEMMs; FP64 LU); 'ref_mixed' both plus the FP32 log|det| accumulation, i.e.
+the reference's mixed build of this path (DelayedUpdate.h:28-50,
+DiracMatrix.h:93-119, DiracDeterminant.cpp:129-146).  Needs a GPU."""
 import argparse
 import json
 import os
@@ -17,66 +33,84 @@ import numpy as np
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
-from miniqmc_b200 import api, capi  # noqa: E402
+from miniqmc_b200 import api, capi, precision  # noqa: E402
 from tests import gpu_helpers as H  # noqa: E402
+from tests import oracle_lib  # noqa: E402
 
-
-def stats(e):
-    e = np.asarray(e, dtype=float).ravel()
-    return {'median': float(np.median(e)), 'p99': float(np.percentile(e, 99)), 'max': float(e.max())}
-
-
-def normwise(a, b):
-    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
-
-
-def spo_errors(gs, os_, rng):
-    pos = rng.uniform(size=(256, 3)) @ np.array(gs.spec.desc.lattice[:]).reshape(3, 3)
-    vg, gg, hg = gs.spo_vgh(pos)
-    vo, go, ho = os_.spo_vgh(pos)
-    return {'v_normwise': normwise(vg, vo), 'g_normwise': normwise(gg, go), 'h_normwise': normwise(hg, ho)}
-
-
-def step_errors(gw, ow, seeds):
-    gw.evaluate_log()
-    ow.evaluate_log()
-    ur, de = H.host_streams(seeds, gw.N, 1, 1)
-    rg = gw.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
-    ro = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
-    tg, to = rg['trace'].reshape(-1, 8), ro['trace'].reshape(-1, 8)
-    lr = np.abs(np.log(np.abs(tg[:, 0])) - np.log(np.abs(to[:, 0])))
-    gerr = np.linalg.norm(tg[:, 1:4] - to[:, 1:4], axis=1) / np.maximum(np.linalg.norm(to[:, 1:4], axis=1), 1e-300)
-    same_accepts = bool(np.array_equal(tg[:, 7], to[:, 7]))
-    # log|det| accumulated through the step's ratios vs a fresh FP64 evaluation
-    cg = gw.components()[0]
-    ow.evaluate_log()
-    co = ow.components()[0]
-    drift = [abs(cg[s] - co[s]) / abs(co[s]) for s in (0, 1)]
-    return {'log_ratio_abs': stats(lr), 'grad_rel': stats(gerr), 'accept_sequence_identical': same_accepts,
-            'logdet_drift_rel': drift, 'logpsi_rel': float(abs(rg['logpsi'][0] - ro['logpsi'][0]) /
-                                                             abs(ro['logpsi'][0]))}
+ORACLE_ARITH = {'spo32': oracle_lib.ARITH_SPO32, 'det32': oracle_lib.ARITH_DET32,
+                'ref_mixed': oracle_lib.ARITH_REFERENCE_MIXED}
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--grid', default='24,24,12')
-    ap.add_argument('--delay', type=int, default=32)
+    ap.add_argument('--grid', default='148,148,74')
+    ap.add_argument('--tiling', default='4,4,2')
+    ap.add_argument('--delays', default='16,32,64')
+    ap.add_argument('--walkers', type=int, default=4)
+    ap.add_argument('--steps', type=int, default=8)
+    ap.add_argument('--forms', default='tc,simt')
+    ap.add_argument('--oracle-variants', default='spo32,det32,ref_mixed')
+    ap.add_argument('--oracle-steps', type=int, default=2)
+    ap.add_argument('--oracle-delay', type=int, default=32)
     args = ap.parse_args()
     grid = tuple(int(x) for x in args.grid.split(','))
-    seeds = H.oracle_primes(1)
-    rng = np.random.default_rng(17)
-    out = {'system': 'NiO 4x4x2 of the 4-atom cell (1536 e-, 768 orbitals/spin)', 'grid': grid,
-           'delay': args.delay, 'walkers': 1, 'moves': 1536}
-    for name, prec, tc in (('mixed_tensor_core_flush', capi.PREC_MIXED, 1), ('mixed_cuda_core_flush', capi.PREC_MIXED, 0),
-                           ('fp64', capi.PREC_FP64, None)):
-        gw, ow = H.make_pair(precision=prec, walkers=1, delay=args.delay, tiling=(4, 4, 2), grid=grid,
-                             jastrow='synthetic', seeds=seeds)
-        if tc is not None:
-            H.product().call('walkers_set_tensor_cores', gw.h, tc)
-        res = {'spo': spo_errors(gw.sys, ow.sys, rng)}
-        res.update(step_errors(gw, ow, seeds))
-        out[name] = res
-        print(name, json.dumps(res), file=sys.stderr, flush=True)
+    tiling = tuple(int(x) for x in args.tiling.split(','))
+    W, S = args.walkers, args.steps
+    lib = H.product()
+    seeds = (np.arange(W, dtype=np.uint32) * 7919 + 1009).astype(np.uint32)
+    kw = dict(cell=capi.NIO_PRIM4, tiling=tiling, grid=grid, spo_seed=11, jastrow='synthetic')
+    sm_spec = api.SystemSpec(lib, fill=capi.FILL_UNIFORM, **kw)
+    sm = api.System(lib, sm_spec, capi.PREC_MIXED)
+    sr = api.System(lib, api.SystemSpec(lib, fill=capi.FILL_UNIFORM_F32, **kw), capi.PREC_FP64)
+    N = sm_spec.n_elec
+    rs = np.random.default_rng(23)
+    ur = rs.uniform(size=(S, W, 1, N))
+    de = rs.normal(size=(S, W, 1, N, 3))
+    pts = rs.uniform(size=(256, 3)) @ np.array(sm_spec.ions['spo_lattice']).reshape(3, 3)
+    out = {'system': 'NiO %s of the 4-atom cell (%d e-, %d orbitals/spin)' % (args.tiling, N, sm_spec.n_orb),
+           'grid': grid, 'walkers': W, 'steps': S, 'moves_per_step': N,
+           'spo_mixed_vs_fp64': precision.spo_errors(sm, sr, pts), 'product': {}, 'oracle': {}}
+    forms = [f for f in args.forms.split(',') if f]
+    for k in (int(x) for x in args.delays.split(',')):
+        for form in forms:
+            wt = api.Walkers(sm, W, k)
+            if form == 'simt':
+                lib.call('walkers_set_tensor_cores', wt.h, 0)
+            else:
+                try:
+                    lib.call('walkers_set_tensor_cores', wt.h, 1)
+                except api.QMCError:
+                    wt.close()
+                    continue  # the tensor-core flush takes k <= 32
+            wr = api.Walkers(sr, W, k)
+            for w in (wt, wr):
+                w.init_random(seeds)
+            res = precision.sweep_errors(wt, wr, ur, de, checkpoints=(1, S))
+            name = '%s_k%d' % (form, k)
+            out['product'][name] = res
+            print(name, json.dumps(res), file=sys.stderr, flush=True)
+            wt.close()
+            wr.close()
+    sm.close()
+    sr.close()
+    variants = [v for v in args.oracle_variants.split(',') if v]
+    if variants:
+        olib = H.oracle()
+        so = api.System(olib, api.SystemSpec(olib, fill=capi.FILL_UNIFORM_F32, **kw), capi.PREC_FP64)
+        So = args.oracle_steps
+        for v in variants:
+            olib.call('system_set_arith', so.h, ORACLE_ARITH[v])
+            wt = api.Walkers(so, W, args.oracle_delay)
+            olib.call('system_set_arith', so.h, 0)
+            wr = api.Walkers(so, W, args.oracle_delay)
+            for w in (wt, wr):
+                w.init_random(seeds)
+            res = precision.sweep_errors(wt, wr, ur[:So], de[:So], checkpoints=(1, So))
+            name = '%s_k%d' % (v, args.oracle_delay)
+            out['oracle'][name] = res
+            print('oracle', name, json.dumps(res), file=sys.stderr, flush=True)
+            wt.close()
+            wr.close()
     print(json.dumps(out), flush=True)
 
 
