@@ -69,6 +69,8 @@ def parse():
                     help='walker-steps of the plain FP64 form (1 walker per launch, rank-1) to time; 0 = skip')
     ap.add_argument('--fp64-steps', type=int, default=2,
                     help='MC steps of the batched FP64 form at the same walker count to time; 0 = skip')
+    ap.add_argument('--refresh1-steps', type=int, default=2,
+                    help='MC steps timed with the FP64 refresh after every step (0 = skip)')
     ap.add_argument('--error-walkers', type=int, default=4,
                     help='walkers of the mixed-form error measurement; 0 = skip')
     ap.add_argument('--error-steps', type=int, default=8,
@@ -188,6 +190,19 @@ def plain_fp64_form(lib, args, api, capi, stream_cls):
     w.close()
     system.close()
     return spec.n_elec / (ms / 1e3), ms
+
+
+def operating_points(value, refresh1, R, error):
+    """Throughput beside the median log-ratio error it is reached at: the
+    configured refresh interval R (the error window is R steps after a
+    refresh) and the FP64 refresh after every step (the first step's
+    error after a fresh inverse)."""
+    pts = [{'recompute_every': R, 'value': value,
+            'log_ratio_median': error['log_ratio_abs']['median'] if error else None}]
+    if refresh1 is not None:
+        pts.append({'recompute_every': 1, 'value': refresh1,
+                    'log_ratio_median': error['log_ratio_abs_per_step'][0]['median'] if error else None})
+    return pts
 
 
 def fp64_reference_system(lib, args, api, capi):
@@ -670,6 +685,22 @@ def main():
         e2e = {'value': job_rate(W * N * args.steps, dt, world, device='cuda')[0], 'unit': 'electron-moves/s',
                'h2d_bytes_per_step': int(ur.nbytes + de.nbytes), 'd2h_bytes_per_step': int(W * 16)}
 
+    # the same sweep with the FP64 refresh after every step (the accurate
+    # operating point: every step starts from a fresh FP64 inverse)
+    refresh1 = None
+    if args.refresh1_steps > 0 and args.recompute_every != 1:
+        lib.call('sweep_async', walkers.h, 1, 1, 0.5, 1)  # warm
+        barrier()
+        with torch.cuda.stream(stream):
+            r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            r0.record(stream)
+            for _ in range(args.refresh1_steps):
+                lib.call('sweep_async', walkers.h, 1, 1, 0.5, 1)
+            r1.record(stream)
+        lib.call('walkers_sync', walkers.h)
+        barrier()
+        refresh1 = job_rate(W * N * args.refresh1_steps, r0.elapsed_time(r1) / 1e3, world, device='cuda')[0]
+
     pk, pk_kind = peaks()
     n, I, k = spec.n_orb, spec.n_ions, args.delay
     s = 4 if args.precision == 'mixed' else 8
@@ -756,6 +787,7 @@ def main():
                        'recompute_every': args.recompute_every, 'recompute_ms': recompute_ms},
             'roofline': roofline, 'tensor': tensor, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk,
             'plain_fp64': plain, 'batched_fp64': batched, 'error': error,
+            'operating_points': operating_points(value, refresh1, args.recompute_every, error),
             'gpu_launches': launches,
         }
         print(json.dumps(out), flush=True)

@@ -127,9 +127,44 @@ def test_sweep_nio128_tensor_core_flush():
     assert np.array_equal(r_tc['trace'][..., 7], r_o['trace'][..., 7])
     assert np.array_equal(r_tc['accepted'], r_o['accepted'])
     lt, ls = _logratio_err(r_tc, r_o), _logratio_err(r_simt, r_o)
+    print('NiO-128 24x24x12: tc median %.3e p99 %.3e logpsi %.3e; simt median %.3e p99 %.3e logpsi %.3e' % (
+        np.median(lt), np.percentile(lt, 99), elem_rel(r_tc['logpsi'], r_o['logpsi']).max(), np.median(ls),
+        np.percentile(ls, 99), elem_rel(r_simt['logpsi'], r_o['logpsi']).max()))
     assert np.median(lt) < 1e-2, np.median(lt)
     assert np.median(lt) < 4 * max(np.median(ls), 1e-7), (np.median(lt), np.median(ls))
     assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-3
+
+
+def test_mixed_form_beats_reference_mixed_algebra():
+    """The mixed form against the FP64 oracle, and beside it the oracle's
+    restatement of the reference's own mixed-precision algebra for this path
+    (FP32 orbitals and DelayedUpdate<float, double>: FP32 inverse, delayed
+    rows, Binv and products; FP64 LU; FP32 log accumulation --
+    DelayedUpdate.h:28-50, DiracMatrix.h:93-119, DiracDeterminant.cpp:
+    129-146) on the same table, positions and streams: NiO-128, 24x24x12,
+    one walker, one step.  The product keeps Binv, the second stage of
+    getInvRow, the block reductions and the log|det| in FP64, which the
+    reference's mixed build does not; its error must stay well below the
+    reference algebra's (measured: 1.4e-3 / 9e-4 median against 0.11)."""
+    from tests import oracle_lib
+    seeds = H.oracle_primes(1)
+    g_tc, ow = _nio128_pair(capi.PREC_MIXED, True)
+    g_simt, _ = _nio128_pair(capi.PREC_MIXED, False)
+    olib = H.oracle()
+    spec = api.SystemSpec(olib, tiling=(4, 4, 2), grid=(24, 24, 12), jastrow='synthetic')
+    so = api.System(olib, spec, capi.PREC_MIXED)  # the same FP32-rounded table
+    olib.call('system_set_arith', so.h, oracle_lib.ARITH_REFERENCE_MIXED)
+    w_ref_mixed = api.Walkers(so, 1, 32)
+    w_ref_mixed.init_random(seeds)
+    for w in (g_tc, g_simt, ow, w_ref_mixed):
+        w.evaluate_log()
+    ur, de = H.host_streams(seeds, g_tc.N, 1, 1)
+    r = [w.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True) for w in (g_tc, g_simt, w_ref_mixed, ow)]
+    e_tc, e_simt, e_ref = (np.median(_logratio_err(x, r[3])) for x in r[:3])
+    print('NiO-128 24x24x12 median log-ratio error: tc %.3e simt %.3e reference mixed algebra %.3e' % (
+        e_tc, e_simt, e_ref))
+    assert np.array_equal(r[2]['trace'][..., 7], r[3]['trace'][..., 7])
+    assert e_tc < 0.1 * e_ref and e_simt < 0.1 * e_ref, (e_tc, e_simt, e_ref)
 
 
 def _phase_times(gw):

@@ -353,6 +353,8 @@ def test_sweep_mixed_precision():
     ro = ow.sweep(1, 2, 0.5, ur=ur, delta=de, trace=True)
     assert np.array_equal(rg['trace'][..., 7], ro['trace'][..., 7])
     lr = np.abs(np.log(np.abs(rg['trace'][..., 0])) - np.log(np.abs(ro['trace'][..., 0]))).ravel()
+    print('mixed 48e: log-ratio median %.3e p99 %.3e logpsi %.3e' % (
+        np.median(lr), np.percentile(lr, 99), elem_rel(rg['logpsi'], ro['logpsi']).max()))
     assert np.median(lr) < 1e-5, np.median(lr)
     assert np.percentile(lr, 99) < 1e-2, np.percentile(lr, 99)
     assert elem_rel(rg['logpsi'], ro['logpsi']).max() < 1e-4

@@ -19,15 +19,14 @@ from tests.test_gpu_parity import elem_rel
 
 pytestmark = pytest.mark.gpu
 
-# NiO 2x2x2 of the 4-atom cell: 384 electrons, 192 orbitals per spin; with
-# 128 threads per walker the FP32 flush runs on the tensor cores
-KW = dict(tiling=(2, 2, 2), grid=(12, 12, 12), jastrow='synthetic')
-DELAY = 16
+# NiO 4x4x2 of the 4-atom cell (768 orbitals per spin: 192 threads per
+# walker, so the FP32 flush runs on the tensor cores), on a coarse grid
+KW = dict(tiling=(4, 4, 2), grid=(24, 24, 12), jastrow='synthetic')
+DELAY = 32
 
 
 def _tc_pair(walkers, seeds):
     gw, ow = H.make_pair(precision=capi.PREC_MIXED, walkers=walkers, delay=DELAY, seeds=seeds, **KW)
-    H.product().call('walkers_set_threads', gw.h, 128)
     H.product().call('walkers_set_tensor_cores', gw.h, 1)
     return gw, ow
 
@@ -39,8 +38,9 @@ def _sweep_matches_oracle(gw, ow, seeds, step):
     ro = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
     assert np.array_equal(rg['trace'][..., 7], ro['trace'][..., 7])
     assert np.array_equal(rg['accepted'], ro['accepted'])
-    # mixed form of a 192-orbital system: log psi to 1e-4 relative
-    assert elem_rel(rg['logpsi'], ro['logpsi']).max() < 1e-4
+    # the mixed form at this size: log psi to 1e-3 relative, as the
+    # tensor-core flush test at NiO-128 allows
+    assert elem_rel(rg['logpsi'], ro['logpsi']).max() < 1e-3
 
 
 def test_wait_limit_timeout_unwinds_and_recovers():
@@ -58,7 +58,7 @@ def test_wait_limit_timeout_unwinds_and_recovers():
     R = gw.positions()
     ow.set_positions(R)
     lg, lo = gw.evaluate_log(), ow.evaluate_log()
-    assert elem_rel(lg, lo).max() < 1e-6
+    assert elem_rel(lg, lo).max() < 1e-7
     _sweep_matches_oracle(gw, ow, seeds, 1)
     gw.close()
     # a fresh batch on the same context
