@@ -103,9 +103,10 @@ def test_sweep_nio128_tensor_core_flush():
     CUDA-core flush, on the same streams.  At this size the error of both is
     set by the FP32 orbital evaluation amplified by the conditioning of the
     768 x 768 Slater matrices (the initial FP32 inverse already differs from
-    the FP64 one by ~1e-5 of its largest entry; measured log-ratio median
-    9e-4 with the CUDA-core flush); the 3xTF32 flush may add a few times
-    that (measured 1.6x).
+    the FP64 one by ~1e-5 of its largest entry).  Measured on this case:
+    log-ratio median 1.38e-3 (tensor cores) and 8.5e-4 (CUDA cores), p99
+    0.25 and 0.15; the bounds below are about twice the tensor-core
+    figures.
 
     log psi after the step sums the log-ratios of the accepted moves, and the
     threshold accept rule takes near-node moves (|ratio| << 1), whose errors
@@ -114,7 +115,9 @@ def test_sweep_nio128_tensor_core_flush():
     9e-6 and 1.3e-4 with this flush (1.6e-5 and 6e-7 with the CUDA-core
     one) at the same median log-ratio error.  The bound is set above that
     spread; a wrong update gives O(1) errors or a different accept
-    sequence."""
+    sequence.  Measured log psi: 9.4e-6 (tensor cores), 8.7e-6 (CUDA
+    cores); the bound is 3x that, so a change of summation order may need a
+    re-measurement."""
     seeds = H.oracle_primes(1)
     g_tc, ow = _nio128_pair(capi.PREC_MIXED, True)
     g_simt, _ = _nio128_pair(capi.PREC_MIXED, False)
@@ -130,9 +133,11 @@ def test_sweep_nio128_tensor_core_flush():
     print('NiO-128 24x24x12: tc median %.3e p99 %.3e logpsi %.3e; simt median %.3e p99 %.3e logpsi %.3e' % (
         np.median(lt), np.percentile(lt, 99), elem_rel(r_tc['logpsi'], r_o['logpsi']).max(), np.median(ls),
         np.percentile(ls, 99), elem_rel(r_simt['logpsi'], r_o['logpsi']).max()))
-    assert np.median(lt) < 1e-2, np.median(lt)
+    assert np.median(lt) < 3e-3, np.median(lt)
+    assert np.percentile(lt, 99) < 0.5, np.percentile(lt, 99)
+    assert np.median(ls) < 2e-3, np.median(ls)
     assert np.median(lt) < 4 * max(np.median(ls), 1e-7), (np.median(lt), np.median(ls))
-    assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-3
+    assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 3e-5
 
 
 def test_mixed_form_beats_reference_mixed_algebra():

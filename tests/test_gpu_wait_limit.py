@@ -31,16 +31,10 @@ def _tc_pair(walkers, seeds):
     return gw, ow
 
 
-def _sweep_matches_oracle(gw, ow, seeds, step):
-    ur, de = H.host_streams(seeds, gw.N, step + 1, 1)
+def _sweep_pair(a, b, seeds, step):
+    ur, de = H.host_streams(seeds, a.N, step + 1, 1)
     ur, de = ur[step:step + 1], de[step:step + 1]
-    rg = gw.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
-    ro = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
-    assert np.array_equal(rg['trace'][..., 7], ro['trace'][..., 7])
-    assert np.array_equal(rg['accepted'], ro['accepted'])
-    # the mixed form at this size: log psi to 1e-3 relative, as the
-    # tensor-core flush test at NiO-128 allows
-    assert elem_rel(rg['logpsi'], ro['logpsi']).max() < 1e-3
+    return (a.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True), b.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True))
 
 
 def test_wait_limit_timeout_unwinds_and_recovers():
@@ -53,19 +47,32 @@ def test_wait_limit_timeout_unwinds_and_recovers():
     with pytest.raises(api.QMCError) as ex:
         gw.sweep(1, 1, 0.5, ur=ur, delta=de)
     assert ex.value.status == 6  # QMC_ERR_TIMEOUT
-    # the status was read and cleared: the batch answers again
+    # the status was read and cleared: the batch answers again.  Rebuilt
+    # from its positions it must sweep exactly like a batch that never
+    # timed out, placed at the same positions, and keep the oracle's accept
+    # sequence.
     H.product().call('walkers_set_wait_limit', gw.h, 2000000000)
     R = gw.positions()
-    ow.set_positions(R)
-    lg, lo = gw.evaluate_log(), ow.evaluate_log()
+    g_new, _ = _tc_pair(2, seeds)
+    for w in (ow, g_new):
+        w.set_positions(R)
+    lg, ln, lo = gw.evaluate_log(), g_new.evaluate_log(), ow.evaluate_log()
+    assert np.array_equal(lg, ln)
     assert elem_rel(lg, lo).max() < 1e-7
-    _sweep_matches_oracle(gw, ow, seeds, 1)
+    rg, rn = _sweep_pair(gw, g_new, seeds, 1)
+    assert np.array_equal(rg['trace'], rn['trace'])
+    assert np.array_equal(rg['logpsi'], rn['logpsi'])
+    _, ro = _sweep_pair(gw, ow, seeds, 1)  # the oracle's step 1 (gw's output unused)
+    assert np.array_equal(rg['trace'][..., 7], ro['trace'][..., 7])
     gw.close()
-    # a fresh batch on the same context
+    g_new.close()
+    # a fresh batch on the same context keeps the oracle's accept sequence
     g2, o2 = _tc_pair(2, seeds)
     g2.evaluate_log()
     o2.evaluate_log()
-    _sweep_matches_oracle(g2, o2, seeds, 0)
+    r2, r2o = _sweep_pair(g2, o2, seeds, 0)
+    assert np.array_equal(r2['trace'][..., 7], r2o['trace'][..., 7])
+    assert np.array_equal(r2['accepted'], r2o['accepted'])
     g2.close()
 
 
