@@ -248,9 +248,11 @@ def mixed_form_error(lib, args, api, capi, spec, mixed_system, fp64_system):
 
 def batched_fp64_form(lib, args, api, fp64_system, stream_cls):
     """The same fused batched sweep in FP64 (table, orbitals, inverse,
-    Woodbury flush on the CUDA cores) at the bench's walker count and delay:
-    --fp64-steps timed MC steps after one warm-up step, no refresh.  Returns
-    (electron-moves/s, ms per step)."""
+    Woodbury flush on the CUDA cores) at the bench's walker count and delay,
+    at its best block size: the default (one thread per 16-byte vector of
+    orbitals, 256) or 192 threads per walker, which lets four walkers share
+    an SM; --fp64-steps timed MC steps after one warm-up step each, no
+    refresh.  Returns (electron-moves/s, ms per step, threads)."""
     import torch
     W = args.walkers
     w = api.Walkers(fp64_system, W, args.delay)
@@ -258,19 +260,27 @@ def batched_fp64_form(lib, args, api, fp64_system, stream_cls):
     stream = stream_cls()
     lib.call('walkers_set_stream', w.h, C.c_void_p(stream.cuda_stream))
     w.evaluate_log()
-    lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
-    lib.call('walkers_sync', w.h)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.fp64_steps):
+    best = None
+    for threads in (0, 192):
+        if threads:
+            lib.call('walkers_set_threads', w.h, threads)
         lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
-    e1.record(stream)
-    lib.call('walkers_sync', w.h)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.fp64_steps
+        lib.call('walkers_sync', w.h)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.fp64_steps):
+            lib.call('sweep_async', w.h, 1, 1, 0.5, 0)
+        e1.record(stream)
+        lib.call('walkers_sync', w.h)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.fp64_steps
+        t = C.c_int()
+        lib.call('walkers_get_config', w.h, C.byref(t), None, None)
+        if best is None or ms < best[0]:
+            best = (ms, t.value)
     n = fp64_system.spec.n_elec
     w.close()
-    return W * n / (ms / 1e3), ms
+    return W * n / (best[0] / 1e3), best[0], best[1]
 
 
 def cpu_baseline(args, n_threads, sample_walkers):
@@ -401,7 +411,7 @@ def run_uneven(args, lib, api, capi, torch):
         spec, system = nio_system(lib, api, capi, tiling, capi.PREC_MIXED)
         systems.append(system)
         if args.no_tune:
-            best = {'delay': 16, 'threads': None, 'tensor_cores': None, 'ms_per_step': None}
+            best = {'delay': 16, 'threads': None, 'tensor_cores': None, 'max_moves': 1, 'ms_per_step': None}
         else:
             t0 = time.perf_counter()
             best, _ = api.autotune(lib, system, W, delays=(8, 16, 32), n_steps=2)
@@ -412,6 +422,7 @@ def run_uneven(args, lib, api, capi, torch):
             lib.call('walkers_set_threads', w.h, best['threads'])
             if best['tensor_cores']:
                 lib.call('walkers_set_tensor_cores', w.h, 1)
+            lib.call('walkers_set_move_batching', w.h, best['max_moves'])
         w.init_random((np.arange(W, dtype=np.uint32) * 7919 + 1009).astype(np.uint32))
         w.evaluate_log()
         batches.append((spec, W, w))
@@ -742,10 +753,10 @@ def main():
         if args.error_walkers > 0:
             error = mixed_form_error(lib, args, api, capi, spec, system, fp64_sys)
         if args.fp64_steps > 0:
-            bv, bms = batched_fp64_form(lib, args, api, fp64_sys, torch.cuda.Stream)
+            bv, bms, bthr = batched_fp64_form(lib, args, api, fp64_sys, torch.cuda.Stream)
             batched = {'value': bv, 'unit': 'electron-moves/s', 'ms_per_step': bms,
-                       'form': 'FP64 fused batched sweep, %d walkers, delay %d, CUDA-core flush, same grid'
-                               % (W, args.delay),
+                       'form': 'FP64 fused batched sweep, %d walkers, delay %d, CUDA-core flush, same grid, '
+                               '%d threads per walker' % (W, args.delay, bthr),
                        'steps_timed': args.fp64_steps, 'value_over_batched_fp64': value / bv}
         fp64_sys.close()
     plain = None

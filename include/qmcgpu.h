@@ -346,6 +346,19 @@ int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable);
  * undefined: call qmc_wf_evaluate_log (which rebuilds them from the
  * positions) or destroy the batch.  0 makes the first wait give up at once. */
 int qmc_walkers_set_wait_limit(qmc_walkers* w, long long cycles);
+/* Moves the fused sweep evaluates together, 1 to 4 (default 1).  The
+ * reference's accept rule compares each move's uniform with a fixed
+ * threshold (miniqmc.cpp:445), so the moves from one accepted move to the
+ * next -- rejected ones that change nothing, then the accepted one -- all see
+ * the same walker state.  The sweep evaluates up to max_moves of them in one
+ * pass (one getInvRow pass over the delayed rows for all of them, one
+ * reduction); the ratios, gradients and trajectory are those of one move at
+ * a time, bit for bit.  1 moves one electron at a time.  Fewer dependent
+ * round trips per move help when few walkers share an SM; with 3-4 walkers
+ * per SM the L2 holds less of each walker's next stencil and one move at a
+ * time measured faster, so qmc_autotune chooses.  No reference counterpart
+ * (the reference loops over electrons one by one). */
+int qmc_walkers_set_move_batching(qmc_walkers* w, int max_moves);
 /* Threads (one CTA) per walker: a multiple of 32 in [max(64, 2 delay), 256];
  * the default covers the padded orbitals with 16-byte vectors.  The kernels
  * stride over any block size; >= 128 is needed for the tensor-core flush. */
@@ -385,12 +398,14 @@ int qmc_group_stream(const qmc_group* g, void** stream);
 /* Autotuner (no reference counterpart): times n_steps sweeps of n_walkers
  * walkers of `sys` for each delay rank in `delays` x threads per walker
  * {default, 128, 192, 256 above it} x flush engine {CUDA cores, tensor cores
- * where it applies}, and returns the fastest in `best` (all timings in
- * results[0 .. min(n, max_results)), n in *n_results). */
+ * where it applies} x moves evaluated together {1, 4}
+ * (qmc_walkers_set_move_batching), and returns the fastest in `best` (all
+ * timings in results[0 .. min(n, max_results)), n in *n_results). */
 typedef struct {
   int delay;
   int threads;
   int tensor_cores;
+  int max_moves;
   double ms_per_step;
 } qmc_tune_result;
 int qmc_autotune(qmc_system* sys, int n_walkers, const int* delays, int n_delays, int n_steps,

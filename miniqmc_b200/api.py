@@ -508,7 +508,8 @@ def autotune(lib, system, n_walkers, delays=(8, 16, 32), n_steps=2):
     lib.call('autotune', system.h, n_walkers, d, len(delays), n_steps, res, 64, C.byref(n), C.byref(best))
 
     def as_dict(r):
-        return dict(delay=r.delay, threads=r.threads, tensor_cores=r.tensor_cores, ms_per_step=r.ms_per_step)
+        return dict(delay=r.delay, threads=r.threads, tensor_cores=r.tensor_cores, max_moves=r.max_moves,
+                    ms_per_step=r.ms_per_step)
     return as_dict(best), [as_dict(res[i]) for i in range(min(n.value, 64))]
 
 

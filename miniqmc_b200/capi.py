@@ -53,7 +53,8 @@ class SweepOpts(C.Structure):
 
 
 class TuneResult(C.Structure):
-    _fields_ = [('delay', C.c_int), ('threads', C.c_int), ('tensor_cores', C.c_int), ('ms_per_step', C.c_double)]
+    _fields_ = [('delay', C.c_int), ('threads', C.c_int), ('tensor_cores', C.c_int), ('max_moves', C.c_int),
+                ('ms_per_step', C.c_double)]
 
 
 JOB_WAITING, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
@@ -128,6 +129,7 @@ PRODUCT_ONLY = {
     'detengine_set_tensor_cores': (I, [P, I]),
     'walkers_set_tensor_cores': (I, [P, I]),
     'walkers_set_wait_limit': (I, [P, C.c_longlong]),
+    'walkers_set_move_batching': (I, [P, I]),
     'walkers_set_threads': (I, [P, I]),
     'walkers_set_prefetch': (I, [P, I]),
     'local_kinetic': (I, [P, PD]),

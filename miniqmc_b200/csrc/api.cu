@@ -561,7 +561,7 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
   st |= dalloc(L, B, &d.words, W * (8 * N + 8));
   st |= dalloc(L, B, &d.ur, W * N);
   st |= dalloc(L, B, &d.delta, W * 3 * N);
-  st |= T(&d.invRow, W * np);
+  st |= T(&d.invRow, W * EPOCH_MAX * np);
   st |= T(&d.psiV, W * np);
   st |= T(&d.dpsiV, W * 3 * np);
   st |= T(&d.d2psiV, W * np);
@@ -760,6 +760,13 @@ int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable)
     return fail(QMC_ERR_ARG, "tensor-core flush needs FP32 walkers, the determinant, delay rank <= 32 and >= 128 "
                              "threads per walker (480 or more orbitals per spin in FP32 give that)");
   w->use_tc = enable != 0;
+  return QMC_OK;
+}
+int qmc_walkers_set_move_batching(qmc_walkers* w, int max_moves)
+{
+  if (!w || max_moves < 1 || max_moves > EPOCH_MAX)
+    return fail(QMC_ERR_ARG, "null handle or max_moves outside [1, 4]");
+  w->max_moves = max_moves;
   return QMC_OK;
 }
 int qmc_walkers_set_wait_limit(qmc_walkers* w, long long cycles)
@@ -1266,7 +1273,7 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
                          w->stream));
     }
     CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k, w->stream,
-                    w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0));
+                    w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0, w->max_moves > 1));
     w->launches++;
     if (trace)
       CK(cudaMemcpyAsync(trace + (size_t)step * W * n_substeps * N * 8, w->d_trace,
@@ -1300,6 +1307,7 @@ SweepTask sweep_task(qmc_walkers* w, int first_block)
   task.first_block = first_block;
   task.timers      = w->d_timers;
   task.tc          = w->use_tc ? 1 : 0;
+  task.max_moves   = w->max_moves;
   // next-move L2 prefetch only while the batch's in-flight stencils (16 rows
   // of 4 npad coefficients per walker) stay well inside the 126 MB L2
   task.prefetch = w->prefetch_mode == QMC_PREFETCH_ON ||

@@ -65,6 +65,7 @@ struct MoveSmem
   double ratio_det, curAt, curLap, curGrad[3], curUat, y;
   long long next_base;
   int accept, dc, ok;
+  int eG; // moves in the current epoch (do_epoch)
   // tensor-core flush state: commit barriers (GEMM1 stages 0/1, GEMM2
   // accumulators 0/1, and the drain barrier of an aborted CTA), their phase
   // bits, the TMEM base, the abort flag and the limit of each bounded wait
@@ -180,7 +181,7 @@ template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
   v.words     = d.words + (size_t)w * (8 * (size_t)d.N + 8);
   v.ur        = d.ur + (size_t)w * d.N;
   v.delta     = d.delta + (size_t)w * 3 * d.N;
-  v.invRow    = (T*)d.invRow + (size_t)w * d.npad;
+  v.invRow    = (T*)d.invRow + (size_t)w * EPOCH_MAX * d.npad;
   v.psiV      = (T*)d.psiV + (size_t)w * d.npad;
   v.dpsiV     = (T*)d.dpsiV + (size_t)w * 3 * d.npad;
   v.d2psiV    = (T*)d.d2psiV + (size_t)w * d.npad;
@@ -1342,6 +1343,418 @@ __device__ void do_move(const SysSmem<T>& ss, const DevSystem* __restrict__ sys,
     __syncthreads();
     phase_mark(m, PH_POSITION);
   }
+}
+
+
+// ------------------------------------------------------ move epochs -----
+// The accept rule of the reference driver compares a uniform with a fixed
+// threshold (miniqmc.cpp:445: ur[iel] < accept), so which moves of a
+// substep are accepted is known before any ratio is.  A rejected move
+// changes no state (rejectMove / restore), hence the moves from one
+// accepted move to the next -- the rejected ones and the accepted one that
+// ends the run -- all see the same inverse, delayed rows, Jastrow arrays and
+// positions.  The fused sweep evaluates such a run ("epoch", at most
+// EPOCH_MAX moves, within one spin) together: one set-up, one getInvRow pass
+// over the delayed rows U and V for all its rows, one block reduction, and
+// the accept bookkeeping of its last move only.  Per move the arithmetic is
+// that of do_move (same loops, same summation order), so the trajectory and
+// every ratio are the same bit for bit; what changes is the number of
+// dependent round trips and barriers per move and the U/V traffic.
+
+// shared-memory bytes an epoch needs beyond the J2 candidate lists (the
+// stencil weights of its moves)
+template <typename T> __host__ __device__ constexpr size_t epoch_smem_bytes()
+{
+  return ((sizeof(SplineSmem<T>) * EPOCH_MAX + 15) / 16) * 16;
+}
+
+// DelayedUpdate::getInvRow for the rows r[0..G) of one spin at once, into
+// wv.invRow + g npad; with no delayed row the caller reads the Ainv rows
+// themselves.  Row dc of Binv receives the last row's Binv^T p (the last
+// move of an epoch is the only one that may be accepted, and acceptRow
+// reads that row).  Per row the arithmetic of get_inv_row.  Block-wide.
+// Scratch: m.red holds p[g][d] (first EPOCH_MAX * MAXK) and w[g][a] (next).
+template <typename T> __device__ void get_inv_rows(const WV<T>& wv, MoveSmem& m, int s, const int* r, int G, int dc)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const int nvec = wv.npad / VW;
+  double* P      = m.red;
+  double* Wg     = m.red + EPOCH_MAX * MAXK;
+  const T* A     = wv.ainv(s);
+  const T* U     = wv.u(s);
+  const T* V     = wv.v(s);
+  const Vt* arow[EPOCH_MAX];
+#pragma unroll
+  for (int g = 0; g < EPOCH_MAX; ++g)
+    arow[g] = reinterpret_cast<const Vt*>(A + (size_t)r[g < G ? g : 0] * wv.npad);
+  for (int d = wid; d < dc; d += nw)
+  {
+    const Vt* ud = reinterpret_cast<const Vt*>(U + (size_t)d * wv.npad);
+    T acc[EPOCH_MAX];
+#pragma unroll
+    for (int g = 0; g < EPOCH_MAX; ++g)
+      acc[g] = T(0);
+#pragma unroll 4
+    for (int jv = lane; jv < nvec; jv += 32)
+    {
+      const Vt x = ud[jv];
+#pragma unroll
+      for (int g = 0; g < EPOCH_MAX; ++g)
+        if (g < G)
+        {
+          const Vt y = arow[g][jv];
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            acc[g] += reinterpret_cast<const T*>(&x)[e] * reinterpret_cast<const T*>(&y)[e];
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < EPOCH_MAX; ++g)
+      if (g < G)
+      {
+        const double sum = warp_sum((double)acc[g]);
+        if (lane == 0)
+          P[g * MAXK + d] = sum;
+      }
+  }
+  __syncthreads();
+  double* B = wv.binv(s);
+  for (int idx = tid; idx < G * dc; idx += NT)
+  {
+    const int g = idx / dc, a = idx - g * dc;
+    double acc = 0.0;
+    for (int b = 0; b < dc; ++b)
+      acc += B[b * wv.k + a] * P[g * MAXK + b];
+    Wg[g * MAXK + a] = acc;
+    if (g == G - 1 && dc < wv.k)
+      B[dc * wv.k + a] = acc;
+  }
+  __syncthreads();
+  // invRow_g = Ainv[r_g] - V^T w_g with FP64 accumulation; the rows two at a
+  // time, so that each V element loaded serves both
+  for (int q = tid; q < nvec; q += NT)
+    for (int g0 = 0; g0 < G; g0 += 2)
+    {
+      const bool two = g0 + 1 < G;
+      double acc0[VW], acc1[VW];
+#pragma unroll
+      for (int e = 0; e < VW; ++e)
+        acc0[e] = acc1[e] = 0.0;
+#pragma unroll 4
+      for (int d = 0; d < dc; ++d)
+      {
+        Vt vv            = reinterpret_cast<const Vt*>(V + (size_t)d * wv.npad)[q];
+        const double wd0 = Wg[g0 * MAXK + d];
+        const double wd1 = two ? Wg[(g0 + 1) * MAXK + d] : 0.0;
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+        {
+          acc0[e] += (double)reinterpret_cast<T*>(&vv)[e] * wd0;
+          acc1[e] += (double)reinterpret_cast<T*>(&vv)[e] * wd1;
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+      {
+        if (h == 1 && !two)
+          break;
+        const int g = g0 + h;
+        Vt a        = arow[g][q];
+        T* ap       = reinterpret_cast<T*>(&a);
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+          ap[e] = (T)((double)ap[e] - (h ? acc1[e] : acc0[e]));
+        reinterpret_cast<Vt*>(wv.invRow + (size_t)g * wv.npad)[q] = a;
+      }
+    }
+  __syncthreads(); // the callers' reductions reuse m.red
+}
+
+// One epoch of the fused sweep: the moves iel0 .. iel0+G-1 of one spin
+// (G <= min(max_moves, lim - iel0)), ending at the first accepted one; the
+// same arithmetic per move as do_move (without the three-body Jastrow).
+// Returns G (read from shared memory after the set-up barrier).  esp: the
+// moves' stencil weights (epoch_smem_bytes, in the dynamic shared memory
+// after the J2 candidate lists).  Block-wide.
+template <typename T>
+__device__ int do_epoch(const SysSmem<T>& ss, const DevSystem* __restrict__ sys, const WV<T>& wv, MoveSmem& m,
+                        SplineSmem<T>* esp, const T* __restrict__ ions, int iel0, int lim, int max_moves,
+                        double accept_thr, const double* urp, const double* dlt, double* trace, T* smem,
+                        bool prefetch_next)
+{
+  using Vt         = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::width;
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
+  const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
+  const int s = iel0 < ss.n_up ? 0 : 1, rbase = s ? ss.n_up : 0;
+  const int npad = wv.npad, nvec = npad / VW, N = wv.N;
+  // epoch positions in m.sums: old [0, 12), new [12, 24)
+  double* epos_old = m.sums;
+  double* epos_new = m.sums + 3 * EPOCH_MAX;
+  if (tid < 32)
+  {
+    // warp 0 finds the epoch (the first accepted move among the next
+    // navail) and sets up each of its moves: lanes 3g..3g+2 the three
+    // dimensions of move g's proposed position and stencil; lanes 12-14 the
+    // move after the epoch when its stencil is prefetched
+    const int navail = min(min(max_moves, EPOCH_MAX), lim - iel0);
+    const bool acc_l = lane < navail && urp[lane] < accept_thr;
+    const unsigned ab = __ballot_sync(0xffffffffu, acc_l);
+    const int G       = ab ? __ffs(ab) : navail;
+    const int g = lane / 3, d = lane % 3, inext = iel0 + G;
+    const bool cur = lane < 3 * G;
+    const bool nxt = lane >= 12 && lane < 15 && prefetch_next && inext < N;
+    double r = 0.0, pn = 0.0;
+    if (cur)
+    {
+      r  = wv.R[3 * (iel0 + g) + d];
+      pn = r + dlt[3 * g + d];
+    }
+    else if (nxt)
+    {
+      r  = wv.R[3 * inext + d];
+      pn = r + dlt[3 * G + d];
+    }
+    const int g0    = cur ? 3 * g : 12;
+    const double p0 = __shfl_sync(0xffffffffu, pn, g0), p1 = __shfl_sync(0xffffffffu, pn, g0 + 1),
+                 p2 = __shfl_sync(0xffffffffu, pn, g0 + 2);
+    const double u  = p0 * ss.spoG[d] + p1 * ss.spoG[3 + d] + p2 * ss.spoG[6 + d];
+    long long b     = 0;
+    if (DET && (cur || nxt))
+      b = spline_dim<T>(u, ss.sdinv[d], ss.sgrid[d], ss.sstride[d], cur ? esp[g].a[d] : nullptr,
+                        cur ? esp[g].da[d] : nullptr, cur ? esp[g].d2a[d] : nullptr);
+    const int gb       = cur ? 3 * g : 12;
+    const long long bs = __shfl_sync(0xffffffffu, b, gb) + __shfl_sync(0xffffffffu, b, gb + 1) +
+        __shfl_sync(0xffffffffu, b, gb + 2);
+    if (cur)
+    {
+      epos_old[3 * g + d] = r;
+      epos_new[3 * g + d] = pn;
+      if (g == G - 1)
+      {
+        m.pos_old[d] = r;
+        m.pos_new[d] = pn;
+      }
+      if (d == 0 && DET)
+        esp[g].base = bs;
+    }
+    if (lane == 12 && nxt && DET)
+      m.next_base = bs;
+    if (lane == 0)
+    {
+      m.eG     = G;
+      m.accept = ab ? 1 : 0;
+      m.dc     = DET ? wv.dcount[s] : 0;
+    }
+  }
+  __syncthreads();
+  phase_mark(m, PH_SETUP);
+  const int G = m.eG;
+  // the first move's stencil starts towards L2 now (16 rows), so that its
+  // HBM latency overlaps getInvRow; each later move's starts when the move
+  // before it has read its own (all of them at once, or two per walker at a
+  // time, would not stay in the L2 with hundreds of walkers)
+  if (DET && tid >= 32 && tid < 48)
+    prefetch_l2((const T*)sys->coefs + esp[0].base + ((tid - 32) >> 2) * sys->xs + ((tid - 32) & 3) * sys->ys,
+                (unsigned)(4 * sys->zs * sizeof(T)));
+  if (DET && prefetch_next && iel0 + G < N && tid < 18)
+  {
+    const int i2 = iel0 + G, s2 = i2 < ss.n_up ? 0 : 1, r2 = i2 - (s2 ? ss.n_up : 0);
+    if (tid < 16)
+      prefetch_l2((const T*)sys->coefs + m.next_base + (tid >> 2) * sys->xs + (tid & 3) * sys->ys,
+                  (unsigned)(4 * sys->zs * sizeof(T)));
+    else if (tid == 16)
+      prefetch_l2(wv.ainv(s2) + (size_t)r2 * npad, (unsigned)(npad * sizeof(T)));
+    else
+      prefetch_l2(wv.dpsi(s2) + (size_t)r2 * 3 * npad, (unsigned)(3 * npad * sizeof(T)));
+  }
+  phase_mark(m, PH_REDUCE);
+  int rows[EPOCH_MAX];
+#pragma unroll
+  for (int g = 0; g < EPOCH_MAX; ++g)
+    rows[g] = iel0 + (g < G ? g : 0) - rbase;
+  const int dc = m.dc;
+  if (DET && dc > 0)
+    get_inv_rows(wv, m, s, rows, G, dc);
+  phase_mark(m, PH_INVROW);
+  const T* coefs       = (const T*)sys->coefs;
+  const long long xs = sys->xs, ys = sys->ys, zs = sys->zs;
+  const double dinv[3] = {sys->dinv[0], sys->dinv[1], sys->dinv[2]};
+  const bool trace_lap = ss.lap_mode == QMC_LAP_TRACE;
+  const uint64_t dpol  = l2_evict_first();
+  for (int g = 0; g < G; ++g)
+  {
+    const bool last = g == G - 1;
+    T part[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      part[i] = T(0);
+    if (DET)
+    {
+      const int r    = rows[g];
+      const T* irow  = dc > 0 ? wv.invRow + (size_t)g * npad : wv.ainv(s) + (size_t)r * npad;
+      const T* dprow = wv.dpsi(s) + (size_t)r * 3 * npad;
+      for (int q = tid; q < nvec; q += NT)
+      {
+        Vt iv        = reinterpret_cast<const Vt*>(irow)[q];
+        const T* ivp = reinterpret_cast<const T*>(&iv);
+        for (int c = 0; c < 3; ++c)
+        {
+          Vt gr = ld_stream_rw(reinterpret_cast<const Vt*>(dprow + (size_t)c * npad) + q, dpol);
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            part[4 + c] += ivp[e] * reinterpret_cast<T*>(&gr)[e];
+        }
+        SplineOut<T> o;
+        spline_eval<T, false>(coefs, xs, ys, zs, esp[g], dinv, q * VW, o);
+        Vt pv, gxv, gyv, gzv, lv;
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+        {
+          reinterpret_cast<T*>(&pv)[e]  = o.v[e];
+          reinterpret_cast<T*>(&gxv)[e] = o.gx[e];
+          reinterpret_cast<T*>(&gyv)[e] = o.gy[e];
+          reinterpret_cast<T*>(&gzv)[e] = o.gz[e];
+          reinterpret_cast<T*>(&lv)[e]  = trace_lap ? o.hxx[e] + o.hyy[e] + o.hzz[e] : o.hxx[e];
+          part[0] += ivp[e] * o.v[e];
+          part[1] += ivp[e] * o.gx[e];
+          part[2] += ivp[e] * o.gy[e];
+          part[3] += ivp[e] * o.gz[e];
+        }
+        if (last) // the only move of the epoch whose rows acceptMove may need
+        {
+          reinterpret_cast<Vt*>(wv.psiV)[q]             = pv;
+          reinterpret_cast<Vt*>(wv.dpsiV)[q]            = gxv;
+          reinterpret_cast<Vt*>(wv.dpsiV + npad)[q]     = gyv;
+          reinterpret_cast<Vt*>(wv.dpsiV + 2 * npad)[q] = gzv;
+          reinterpret_cast<Vt*>(wv.d2psiV)[q]           = lv;
+        }
+      }
+      phase_mark(m, PH_SPO);
+    }
+    // the next move's stencil starts towards L2 once this move's has been
+    // read, so that its latency overlaps this move's Jastrow sums
+    if (DET && g + 1 < G && tid >= 32 && tid < 48)
+      prefetch_l2((const T*)sys->coefs + esp[g + 1].base + ((tid - 32) >> 2) * xs + ((tid - 32) & 3) * ys,
+                  (unsigned)(4 * zs * sizeof(T)));
+    if (J1)
+      j1_partials(ss, ions, epos_new + 3 * g, part + 7);
+    if (J2)
+      j2_partials(ss, wv.Rs, wv.Npad, iel0 + g, epos_new + 3 * g, part + 12, true, reinterpret_cast<int*>(smem));
+    phase_mark(m, PH_JASTROW);
+    // the first half of block_sum<16>: warp sums into this move's slice
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+    {
+      const double sw = warp_sum((double)part[i]);
+      if (lane == 0)
+        m.red[(g * nw + wid) * 16 + i] = sw;
+    }
+  }
+  __syncthreads();
+  // the second half: warp g (mod the warp count) sums move g's slices over
+  // the warps
+  double* esum = m.col; // [EPOCH_MAX][16]
+  for (int g = wid; g < G; g += nw)
+  {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+    {
+      double sw = lane < nw ? m.red[(g * nw + lane) * 16 + i] : 0.0;
+      sw        = warp_sum(sw);
+      if (lane == 0)
+        esum[g * 16 + i] = sw;
+    }
+  }
+  __syncthreads();
+  if (tid < G)
+  {
+    // ratio and gradients of move g = tid (do_move's assembly)
+    const int g = tid, iel = iel0 + g;
+    const double* S = esum + 16 * g;
+    const double rdet = DET ? S[0] : 1.0;
+    double ratio      = rdet;
+    double gn[3], gq[3];
+    for (int c = 0; c < 3; ++c)
+    {
+      gn[c] = DET ? (1.0 / rdet) * S[1 + c] : 0.0;
+      gq[c] = DET ? S[4 + c] : 0.0;
+    }
+    if (J1)
+    {
+      for (int c = 0; c < 3; ++c)
+      {
+        gn[c] += S[8 + c];
+        gq[c] += (double)wv.Grad[c * wv.N + iel];
+      }
+      ratio *= exp((double)wv.Vat[iel] - S[7]);
+    }
+    if (J2)
+    {
+      for (int c = 0; c < 3; ++c)
+      {
+        gn[c] += S[13 + c];
+        gq[c] += (double)wv.dUat[c * wv.N + iel];
+      }
+      ratio *= exp((double)wv.Uat[iel] - S[12]);
+    }
+    if (!isfinite(ratio))
+      atomicOr(wv.status, DEV_ERR_NONFINITE);
+    const bool acc_g = g == G - 1 && m.accept;
+    if (trace)
+    {
+      double* tr = trace + (size_t)g * 8;
+      tr[0]      = ratio;
+      tr[1] = gn[0], tr[2] = gn[1], tr[3] = gn[2];
+      tr[4] = gq[0], tr[5] = gq[1], tr[6] = gq[2];
+      tr[7] = acc_g ? 1.0 : 0.0;
+    }
+    if (g == G - 1)
+    {
+      m.ratio_det = rdet;
+      if (J1)
+      {
+        m.curAt  = S[7];
+        m.curLap = S[11];
+        for (int c = 0; c < 3; ++c)
+          m.curGrad[c] = S[8 + c];
+      }
+      if (J2)
+        m.curUat = S[12];
+    }
+  }
+  __syncthreads();
+  phase_mark(m, PH_REDUCE);
+  if (m.accept)
+  {
+    const int iel = iel0 + G - 1, r = iel - rbase;
+    if (DET)
+      det_accept(wv, m, s, r, m.ratio_det, true, true, smem);
+    phase_mark(m, PH_DET_ACCEPT);
+    if (J1 && tid == 0)
+    {
+      wv.jlog[0] += (double)wv.Vat[iel] - m.curAt;
+      wv.Vat[iel] = (T)m.curAt;
+      for (int c = 0; c < 3; ++c)
+        wv.Grad[c * wv.N + iel] = (T)m.curGrad[c];
+      wv.Lap[iel] = (T)m.curLap;
+    }
+    if (J2)
+      j2_accept(ss, wv, m, iel, reinterpret_cast<int*>(smem));
+    __syncthreads();
+    phase_mark(m, PH_J2_ACCEPT);
+    if (tid == 0)
+      for (int c = 0; c < 3; ++c)
+      {
+        wv.R[3 * iel + c]        = m.pos_new[c];
+        wv.Rs[c * wv.Npad + iel] = (T)m.pos_new[c];
+      }
+    __syncthreads();
+    phase_mark(m, PH_POSITION);
+  }
+  return G;
 }
 
 } // namespace qmc

@@ -57,6 +57,7 @@ struct qmc_walkers_s
   long long* d_timers = nullptr;
   bool tc_capable = false; // FP32, >= 128 threads, k <= 32, determinant on
   bool use_tc     = false; // Woodbury flushes on the tensor cores
+  int max_moves   = 1; // moves the fused sweep evaluates together (qmc_walkers_set_move_batching)
 };
 
 // the tensor-core flush keeps (Binv V)^T as 32-row hi/lo tiles of up to 32

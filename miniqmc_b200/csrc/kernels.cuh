@@ -40,6 +40,7 @@ struct SweepTask
   int first_block;      // first CTA of this task in the launch
   int prefetch;         // warm L2 with the next move's coefficients
   int tc;               // Woodbury flushes on the tensor cores (needs dw.tci)
+  int max_moves;        // most moves evaluated together (an epoch, do_epoch)
 };
 
 struct LaunchCfg
@@ -53,8 +54,11 @@ struct LaunchCfg
 // tc: FP32 Woodbury flushes on the tensor cores (every task has dw.tci,
 // k <= 32, threads >= 128); j3: some task's wavefunction has the three-body
 // Jastrow (its shared-memory scratch is added to the launch)
+// epoch: evaluate the moves an epoch at a time (each task's max_moves);
+// ignored with j3
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
-                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3);
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3,
+                         bool epoch);
 
 // evaluateLog pieces
 // ratio_mode_only: only the derivative rows of the determinants whose last

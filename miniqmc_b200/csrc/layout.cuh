@@ -66,6 +66,12 @@ struct DevSystem
   const void* j3_gamma;
 };
 
+// most moves the fused sweep evaluates together: one epoch is a run of
+// rejected moves and the accepted move that ends it, which all see the same
+// walker state (the accept rule compares a uniform with a fixed threshold,
+// miniqmc.cpp:445, so the run is known before its ratios are)
+constexpr int EPOCH_MAX = 4;
+
 // scalars of the move in progress, per walker (drop-in verb API)
 struct MoveState
 {
@@ -113,7 +119,7 @@ struct DevWalkers
   uint32_t* words; // [W][8N+4]
   double* ur;      // [W][N]
   double* delta;   // [W][N][3]
-  void* invRow;    // [W][npad]
+  void* invRow;    // [W][EPOCH_MAX][npad] (the verbs use row 0)
   void* psiV;      // [W][npad]
   void* dpsiV;     // [W][3][npad]
   void* d2psiV;    // [W][npad]

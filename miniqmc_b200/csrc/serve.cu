@@ -34,7 +34,7 @@ struct TaskList
 {
   SweepTask* d = nullptr;
   int cap = 0, n = 0, blocks = 0, threads = 64, max_npad = 0, max_k = 0;
-  bool fp32 = true, tc = false, j3 = false;
+  bool fp32 = true, tc = false, j3 = false, epoch = false;
 
   ~TaskList() { cudaFree(d); }
 
@@ -51,7 +51,7 @@ struct TaskList
       cap = n;
     }
     std::vector<SweepTask> h;
-    blocks = 0, max_npad = 0, max_k = 0, tc = false, j3 = false;
+    blocks = 0, max_npad = 0, max_k = 0, tc = false, j3 = false, epoch = false;
     threads = launch_threads;
     double inflight = 0;
     for (auto* w : batches)
@@ -65,6 +65,7 @@ struct TaskList
       inflight += (double)w->dw.W * 16 * 4 * w->dw.npad * (w->fp32 ? 4 : 8);
       fp32 = w->fp32;
       j3   = j3 || (w->sys->h.comp & QMC_WF_J3) != 0;
+      epoch = epoch || w->max_moves > 1;
       h.push_back(t);
     }
     // the next-move L2 prefetch only while all walkers' stencils fit well
@@ -80,7 +81,7 @@ struct TaskList
 
   cudaError_t launch(int n_substeps, double accept, cudaStream_t st) const
   {
-    return launch_sweep(fp32, d, n, blocks, n_substeps, accept, threads, max_npad, max_k, st, tc, j3);
+    return launch_sweep(fp32, d, n, blocks, n_substeps, accept, threads, max_npad, max_k, st, tc, j3, epoch);
   }
 };
 
@@ -323,26 +324,28 @@ int qmc_autotune(qmc_system* sys, int n_walkers, const int* delays, int n_delays
     }
     for (int threads : thread_opts)
       for (int tc = 0; tc <= 1 && status == QMC_OK; ++tc)
-      {
-        if (tc && !(w->tc_capable && threads >= 128))
-          continue;
-        w->use_tc = false;
-        if (qmc_walkers_set_threads(w, threads) != QMC_OK)
-          continue;
-        w->use_tc = tc != 0;
-        if ((status = qmc_sweep_async(w, 1, 1, 0.5, 0)))
-          break;
-        CK(cudaEventRecord(e0, w->stream));
-        if ((status = qmc_sweep_async(w, n_steps, 1, 0.5, 0)))
-          break;
-        CK(cudaEventRecord(e1, w->stream));
-        CK(cudaEventSynchronize(e1));
-        if ((status = device_status(w)))
-          break;
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        all.push_back({k, threads, tc, (double)ms / n_steps});
-      }
+        for (int moves : {1, EPOCH_MAX})
+        {
+          if (tc && !(w->tc_capable && threads >= 128))
+            continue;
+          w->use_tc = false;
+          if (qmc_walkers_set_threads(w, threads) != QMC_OK)
+            continue;
+          w->use_tc    = tc != 0;
+          w->max_moves = moves;
+          if ((status = qmc_sweep_async(w, 1, 1, 0.5, 0)))
+            break;
+          CK(cudaEventRecord(e0, w->stream));
+          if ((status = qmc_sweep_async(w, n_steps, 1, 0.5, 0)))
+            break;
+          CK(cudaEventRecord(e1, w->stream));
+          CK(cudaEventSynchronize(e1));
+          if ((status = device_status(w)))
+            break;
+          float ms = 0;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          all.push_back({k, threads, tc, moves, (double)ms / n_steps});
+        }
     qmc_walkers_destroy(w);
   }
   cudaEventDestroy(e0);

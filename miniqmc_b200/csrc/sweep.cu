@@ -12,7 +12,11 @@
 
 namespace qmc
 {
-template <typename T, bool HAS_J3>
+// EPOCH: the moves are evaluated an epoch at a time (do_epoch: a run of
+// rejected moves and the accepted move that ends it, up to the task's
+// max_moves), else one at a time (do_move); the three-body Jastrow runs one
+// at a time.
+template <typename T, bool HAS_J3, bool EPOCH>
 __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restrict__ tasks, int n_tasks, int n_substeps,
                                                     double accept_thr, int tc)
 {
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
     }
     if (DET)
       load_binv(0);
-    for (int iel = 0; iel < N; ++iel)
+    for (int iel = 0; iel < N;)
     {
       if (DET && iel == ss.n_up)
       {
@@ -95,8 +99,21 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepTask* __restri
         load_binv(1);
       }
       double* tr = task.trace ? task.trace + (((size_t)w * n_substeps + l) * N + iel) * 8 : nullptr;
-      do_move<T, HAS_J3>(ss, sys, wv, m, sp, ions, iel, accept_thr, urp + iel, dp + 3 * iel, tr, smem,
-                         task.prefetch && iel + 1 < N);
+      if constexpr (EPOCH)
+      {
+        // an epoch stays within one spin's moves
+        const int lim = iel < ss.n_up ? ss.n_up : N;
+        auto* esp     = reinterpret_cast<SplineSmem<T>*>(reinterpret_cast<unsigned char*>(smem) + j2_list_bytes());
+        const int G   = do_epoch<T>(ss, sys, wv, m, esp, ions, iel, lim, task.max_moves, accept_thr, urp + iel,
+                                  dp + 3 * iel, tr, smem, task.prefetch);
+        iel += G;
+      }
+      else
+      {
+        do_move<T, HAS_J3>(ss, sys, wv, m, sp, ions, iel, accept_thr, urp + iel, dp + 3 * iel, tr, smem,
+                           task.prefetch && iel + 1 < N);
+        ++iel;
+      }
       acc += m.accept ? 1 : 0;
       __syncthreads(); // m.accept is rewritten by the next move
       if (m.tc_abort)
@@ -197,52 +214,64 @@ cudaError_t launch_step(bool fp32, bool j3, const DevSystem* sys, const DevWalke
   return cudaGetLastError();
 }
 
-template <typename T, bool HAS_J3> static void set_smem_attr(size_t bytes)
+template <typename T, bool HAS_J3, bool EPOCH> static void set_smem_attr(size_t bytes)
 {
   static size_t done = 0;
   if (bytes > done)
   {
-    cudaFuncSetAttribute(sweep_kernel<T, HAS_J3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(sweep_kernel<T, HAS_J3, EPOCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     done = bytes;
   }
 }
 template <typename T>
-static void launch_sweep_t(bool j3, size_t bytes, const SweepTask* d_tasks, int n_tasks, int total_blocks,
-                           int n_substeps, double accept, int threads, cudaStream_t st, int tc)
+static void launch_sweep_t(bool j3, bool epoch, size_t bytes, const SweepTask* d_tasks, int n_tasks,
+                           int total_blocks, int n_substeps, double accept, int threads, cudaStream_t st, int tc)
 {
   if (j3)
   {
-    set_smem_attr<T, true>(bytes);
-    sweep_kernel<T, true><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
+    set_smem_attr<T, true, false>(bytes);
+    sweep_kernel<T, true, false><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
+  }
+  else if (epoch)
+  {
+    set_smem_attr<T, false, true>(bytes);
+    sweep_kernel<T, false, true><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
   }
   else
   {
-    set_smem_attr<T, false>(bytes);
-    sweep_kernel<T, false><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
+    set_smem_attr<T, false, false>(bytes);
+    sweep_kernel<T, false, false><<<total_blocks, threads, bytes, st>>>(d_tasks, n_tasks, n_substeps, accept, tc);
   }
 }
 
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
-                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3)
+                         double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3,
+                         bool epoch)
 {
   (void)max_npad;
   if (max_k > MAXK || (tc && (!fp32 || threads < 128))) // a task flushes on the tensor cores only if its k <= 32
     return cudaErrorInvalidValue;
+  epoch = epoch && !j3;
+  // dynamic shared memory between flushes: the J2 candidate lists, then the
+  // epoch's stencil weights
   if (fp32)
   {
-    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<float>(threads, max_k), j2_list_bytes());
+    const size_t moves = j2_list_bytes() + (epoch ? epoch_smem_bytes<float>() : 0);
+    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<float>(threads, max_k), moves);
     if (tc && tc_flush_smem_bytes() > bytes)
       bytes = tc_flush_smem_bytes(); // the tiles overlay the cached Binv
     if (j3)
       bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<float>));
-    launch_sweep_t<float>(j3, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, tc ? 1 : 0);
+    launch_sweep_t<float>(j3, epoch, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st,
+                          tc ? 1 : 0);
   }
   else
   {
-    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<double>(threads, max_k), j2_list_bytes());
+    const size_t moves = j2_list_bytes() + (epoch ? epoch_smem_bytes<double>() : 0);
+    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<double>(threads, max_k), moves);
     if (j3)
       bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<double>));
-    launch_sweep_t<double>(j3, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, 0);
+    launch_sweep_t<double>(j3, epoch, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, 0);
   }
   return cudaGetLastError();
 }
