@@ -7,7 +7,9 @@ the fixtures are committed.  Two sources:
 1. reference_dump.json -- output of oracle/_ref/ref_harness, which is built by
    oracle/ref_harness.mk from the reference's own ParticleSet, distance-table,
    lattice, einspline SPO, BsplineFunctor, One/TwoBodyJastrow, StdRandom and
-   NiO-input code (FP64, no fast-math).
+   NiO-input code (FP64, no fast-math); reference_det_dump.json -- output of
+   oracle/_ref/ref_det_harness: the reference's DiracDeterminant /
+   DelayedUpdate / DiracMatrix over OpenBLAS on a well-conditioned table.
 2. known_answers.json -- the numbers the reference's Catch unit tests assert,
    read from the test sources as text:
      src/QMCWaveFunctions/tests/test_dirac_matrix.cpp  (3x3 inverse, log|det|,
@@ -118,6 +120,12 @@ def main():
     dump['_generator'] = 'oracle/ref_harness.cpp compiled from the reference sources'
     with open(os.path.join(HERE, 'reference_dump.json'), 'w') as f:
         json.dump(dump, f)
+    # the determinant path (DiracDeterminant + DelayedUpdate + DiracMatrix
+    # over OpenBLAS) on a well-conditioned table, delay ranks 1 and 32
+    det = subprocess.check_output([os.path.join(REPO, 'oracle', '_ref', 'ref_det_harness')],
+                                  env=dict(os.environ, OPENBLAS_NUM_THREADS='1'))
+    with open(os.path.join(HERE, 'reference_det_dump.json'), 'w') as f:
+        json.dump(json.loads(det), f)
     with open(os.path.join(HERE, 'known_answers.json'), 'w') as f:
         json.dump(known_answers(args.reference), f, indent=1)
     print('wrote', os.path.join(HERE, 'reference_dump.json'), 'and known_answers.json')
