@@ -1,0 +1,89 @@
+"""The plain FP64 form on the two small configurations of the benchmark as
+they are written, against the FP64 oracle on identical random streams.
+
+Configuration 1: miniqmc VMC on the 4-atom NiO cell (48 electrons, 24
+orbitals per spin) on a 37x37x37 table of FP32-valued coefficients (uniform
+[-0.5, 0.5) from seed 11, held in FP64: QMC_FILL_UNIFORM_F32), the synthetic
+J1 / J2, rank-1 Sherman-Morrison updates, one walker, 5 steps x 100
+substeps (24,000 moves) with acceptance threshold 0.5, electrons from seed 7.
+
+Configuration 2: NiO 2x2x2 of the 4-atom cell (32 atoms, 384 electrons, 192
+orbitals per spin) on a 74x74x74 FP64 table, FP64 throughout, rank-1, 64
+walkers (seeds 7 + 7919 w), 10 steps.  The plain form runs one walker per
+launch; the batch runs all 64 in one launch, and walkers 0 and 1 are also
+run alone to show that both give the same walkers bit for bit.
+
+Both follow the reference driver's loop (miniqmc.cpp:406-468): the accept
+sequence must equal the oracle's exactly (it depends only on the uniforms),
+every ratio and log value must agree to FP64 round-off."""
+import numpy as np
+import pytest
+
+from miniqmc_b200 import api, capi
+from tests import gpu_helpers as H
+from tests.test_gpu_parity import elem_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(tiling, grid, fill, walkers, seeds):
+    out = []
+    for lib in (H.product(), H.oracle()):
+        spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=tiling, grid=grid, fill=fill, spo_seed=11,
+                              jastrow='synthetic')
+        system = api.System(lib, spec, capi.PREC_FP64)
+        w = api.Walkers(system, walkers, 1)
+        w.init_random(seeds)
+        out.append((spec, system, w))
+    return out
+
+
+def _compare(rg, ro, tag):
+    tg, to = rg['trace'], ro['trace']
+    assert np.array_equal(tg[..., 7], to[..., 7]), tag
+    assert np.array_equal(rg['accepted'], ro['accepted']), tag
+    e = elem_rel(tg[..., 0], to[..., 0]).ravel()
+    lp = elem_rel(rg['logpsi'], ro['logpsi']).max()
+    print('%s: %d moves, accepted %d, ratio rel median %.2e p99 %.2e max %.2e, log psi rel %.2e' % (
+        tag, e.size, int(rg['accepted'].sum()), np.median(e), np.percentile(e, 99), e.max(), lp))
+    return e, lp
+
+
+def test_configuration_1_as_written():
+    seeds = np.array([7], dtype=np.uint32)
+    (sg, _, wg), (so, _, wo) = _pair((1, 1, 1), (37, 37, 37), capi.FILL_UNIFORM_F32, 1, seeds)
+    assert sg.n_elec == 48 and sg.n_orb == 24
+    wg.evaluate_log()
+    wo.evaluate_log()
+    ur, de = H.host_streams(seeds, sg.n_elec, 5, 100)
+    rg = wg.sweep(5, 100, 0.5, ur=ur, delta=de, trace=True)
+    ro = wo.sweep(5, 100, 0.5, ur=ur, delta=de, trace=True)
+    assert rg['trace'][..., 7].size == 24000
+    e, lp = _compare(rg, ro, 'configuration 1')
+    assert np.median(e) < 1e-12 and np.percentile(e, 99) < 1e-10, (np.median(e), np.percentile(e, 99))
+    assert lp < 1e-10
+    assert np.max(np.abs(wg.positions() - wo.positions())) < 1e-10
+
+
+def test_configuration_2_as_written():
+    W = 64
+    seeds = (7 + 7919 * np.arange(W)).astype(np.uint32)
+    (sg, s_g, wg), (so, _, wo) = _pair((2, 2, 2), (74, 74, 74), capi.FILL_UNIFORM, W, seeds)
+    assert sg.n_elec == 384 and sg.n_orb == 192
+    wg.evaluate_log()
+    wo.evaluate_log()
+    ur, de = H.host_streams(seeds, sg.n_elec, 10, 1)
+    rg = wg.sweep(10, 1, 0.5, ur=ur, delta=de, trace=True)
+    ro = wo.sweep(10, 1, 0.5, ur=ur, delta=de, trace=True)
+    e, lp = _compare(rg, ro, 'configuration 2')
+    assert np.median(e) < 1e-12 and np.percentile(e, 99) < 1e-10, (np.median(e), np.percentile(e, 99))
+    assert lp < 1e-10
+    # the plain form proper: one walker per launch, walkers in sequence
+    for w in (0, 1):
+        one = api.Walkers(s_g, 1, 1)
+        one.init_random(seeds[w:w + 1])
+        one.evaluate_log()
+        r1 = one.sweep(10, 1, 0.5, ur=ur[:, w:w + 1], delta=de[:, w:w + 1], trace=True)
+        assert np.array_equal(r1['trace'][:, 0], rg['trace'][:, w])
+        assert np.array_equal(r1['logpsi'][0], rg['logpsi'][w])
+        one.close()
