@@ -26,6 +26,26 @@ int fail(int code, const std::string& msg)
 
 // set while walkers_footprint sizes a batch: dalloc only counts bytes
 static thread_local bool g_dry = false;
+// set while a request-loop job's walkers are allocated: dalloc takes the
+// memory stream-ordered from the server's pool on its stream (no device-wide
+// synchronisation, memory reused without returning it to the driver)
+static thread_local cudaStream_t g_alloc_stream = nullptr;
+static thread_local cudaMemPool_t g_alloc_pool  = nullptr;
+struct AllocScope
+{
+  cudaStream_t s0;
+  cudaMemPool_t p0;
+  AllocScope(cudaStream_t s, cudaMemPool_t p) : s0(g_alloc_stream), p0(g_alloc_pool)
+  {
+    g_alloc_stream = s;
+    g_alloc_pool   = p;
+  }
+  ~AllocScope()
+  {
+    g_alloc_stream = s0;
+    g_alloc_pool   = p0;
+  }
+};
 
 template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes, P** p, size_t count)
 {
@@ -37,10 +57,12 @@ template <typename P> static int dalloc(std::vector<void*>& list, size_t& bytes,
     bytes += count * sizeof(P);
     return QMC_OK;
   }
-  cudaError_t e = cudaMalloc((void**)p, count * sizeof(P));
+  cudaError_t e = g_alloc_stream
+      ? cudaMallocFromPoolAsync((void**)p, count * sizeof(P), g_alloc_pool, g_alloc_stream)
+      : cudaMalloc((void**)p, count * sizeof(P));
   if (e != cudaSuccess)
-    return fail(QMC_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
-  e = cudaMemset(*p, 0, count * sizeof(P));
+    return fail(QMC_ERR_OOM, std::string("device allocation failed: ") + cudaGetErrorString(e));
+  e = g_alloc_stream ? cudaMemsetAsync(*p, 0, count * sizeof(P), g_alloc_stream) : cudaMemset(*p, 0, count * sizeof(P));
   if (e != cudaSuccess)
     return fail(QMC_ERR_CUDA, cudaGetErrorString(e));
   list.push_back((void*)*p);
@@ -585,14 +607,16 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
     return QMC_ERR_OOM;
   if (g_dry)
     return QMC_OK;
-  if (d.j3_cnt)
+  // (dalloc has zeroed every array, stream-ordered for a pooled batch)
+  if (!g_alloc_stream && d.j3_cnt)
   {
     CK(cudaMemset(d.j3_cnt, 0, W * 2 * (size_t)d.I * sizeof(int)));
     CK(cudaMemset(d.j3_Uat, 0, W * N * es));
     CK(cudaMemset(d.j3_d2Uat, 0, W * N * es));
     CK(cudaMemset(d.j3_dUat, 0, W * 3 * N * es));
   }
-  CK(cudaMemset(d.j_log, 0, W * 3 * sizeof(double)));
+  if (!g_alloc_stream)
+    CK(cudaMemset(d.j_log, 0, W * 3 * sizeof(double)));
   std::vector<MoveState> ms(W);
   for (auto& m : ms)
   {
@@ -602,7 +626,10 @@ static int alloc_walkers(qmc_walkers* w, qmc_system* s, int W, int k)
     m.partial[0] = m.partial[1] = 1;
     m.j_partial                 = 1;
   }
-  CK(cudaMemcpy(d.ms, ms.data(), W * sizeof(MoveState), cudaMemcpyHostToDevice));
+  if (g_alloc_stream) // pageable source: staged before the call returns
+    CK(cudaMemcpyAsync(d.ms, ms.data(), W * sizeof(MoveState), cudaMemcpyHostToDevice, g_alloc_stream));
+  else
+    CK(cudaMemcpy(d.ms, ms.data(), W * sizeof(MoveState), cudaMemcpyHostToDevice));
   return QMC_OK;
 }
 
@@ -628,6 +655,16 @@ extern "C" {
 
 static void free_walkers(qmc_walkers* w)
 {
+  if (w->alloc_stream)
+  {
+    // a pooled batch: its memory returns to the pool behind its last work
+    // on the stream, without waiting for it
+    for (void* p : w->allocs)
+      cudaFreeAsync(p, w->alloc_stream);
+    w->allocs.clear();
+    if (!w->d_ur && !w->d_delta && !w->d_trace && !w->d_rows && !w->d_timers)
+      return;
+  }
   if (w->stream)
     cudaStreamSynchronize(w->stream);
   for (void* p : w->allocs)
@@ -682,6 +719,45 @@ int qmc_walkers_create(qmc_system* s, int n_walkers, int delay_rank, qmc_walkers
   *out          = w;
   return QMC_OK;
 }
+} // extern "C"
+
+// a request-loop job's batch: memory stream-ordered from `pool` on `st`
+// (which becomes the batch's stream); nothing here waits for the device
+int walkers_create_pooled(qmc_system* s, int n_walkers, int delay_rank, cudaStream_t st, cudaMemPool_t pool,
+                          qmc_walkers** out)
+{
+  if (!s || !out || n_walkers < 1 || delay_rank < 1 || delay_rank > 64 || delay_rank > s->h.norb || !st || !pool)
+    return fail(QMC_ERR_ARG, "bad walker batch arguments");
+  *out = nullptr;
+  AllocScope scope(st, pool);
+  auto* w         = new qmc_walkers_s;
+  w->sys          = s;
+  w->fp32         = s->fp32;
+  w->stream       = st;
+  w->own_stream   = false;
+  w->alloc_stream = st;
+  w->alloc_pool   = pool;
+  int rc          = alloc_walkers(w, s, n_walkers, delay_rank);
+  const int vw    = w->fp32 ? 4 : 2;
+  w->threads      = std::min(256, std::max(std::max(64, 2 * delay_rank), round_up(s->h.npad / vw, 32)));
+  w->tc_capable   = w->fp32 && w->threads >= 128 && delay_rank <= 32 && (s->h.comp & QMC_WF_DET);
+  if (!rc && w->tc_capable)
+  {
+    rc        = dalloc(w->allocs, w->bytes, &w->dw.tci, (size_t)n_walkers * tc_image_floats(w->dw.npad));
+    w->use_tc = rc == QMC_OK;
+  }
+  if (rc)
+  {
+    free_walkers(w);
+    delete w;
+    return rc;
+  }
+  *out = w;
+  return QMC_OK;
+}
+
+extern "C" {
+
 int qmc_walkers_destroy(qmc_walkers* w)
 {
   if (!w)
@@ -832,7 +908,13 @@ static int sync_rs(qmc_walkers* w)
   return QMC_OK;
 }
 
-int qmc_walkers_init_random(qmc_walkers* w, const uint32_t* seeds)
+int qmc_walkers_init_random(qmc_walkers* w, const uint32_t* seeds) { return walkers_init_random(w, seeds, true); }
+} // extern "C"
+
+// build_els on every walker's stream (host mt19937, then copied); sync =
+// false leaves the copies and the SoA kernel in flight (the sources are
+// pageable, so they are staged before each call returns)
+int walkers_init_random(qmc_walkers* w, const uint32_t* seeds, bool sync)
 {
   if (!w || !seeds)
     return fail(QMC_ERR_ARG, "null pointer");
@@ -862,9 +944,12 @@ int qmc_walkers_init_random(qmc_walkers* w, const uint32_t* seeds)
   int st = sync_rs(w);
   if (st)
     return st;
-  CK(cudaStreamSynchronize(w->stream));
+  if (sync)
+    CK(cudaStreamSynchronize(w->stream));
   return QMC_OK;
 }
+
+extern "C" {
 int qmc_walkers_set_positions(qmc_walkers* w, const double* R)
 {
   if (!w || !R)
@@ -983,6 +1068,7 @@ static int ensure_lu(qmc_walkers* w)
 {
   if (w->dw.lu)
     return QMC_OK;
+  AllocScope scope(w->alloc_stream, w->alloc_pool);
   return dalloc(w->allocs, w->bytes, &w->dw.lu, (size_t)w->dw.W * 2 * w->dw.n * w->dw.npad);
 }
 
@@ -1003,6 +1089,20 @@ int recompute_dets(qmc_walkers* w)
 extern "C" {
 
 int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi)
+{
+  int st = evaluate_log_launch(w);
+  if (st)
+    return st;
+  if (logpsi)
+    CK(cudaMemcpyAsync(logpsi, w->dw.logpsi, w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
+  return device_status(w);
+}
+} // extern "C"
+
+// evaluateLog's launches on the batch's stream, without waiting for them
+// (errors land in the batch's status word)
+int evaluate_log_launch(qmc_walkers* w)
 {
   if (!w)
     return fail(QMC_ERR_ARG, "null handle");
@@ -1034,11 +1134,10 @@ int qmc_wf_evaluate_log(qmc_walkers* w, double* logpsi)
     m.j_partial                 = 1;
   }
   CK(cudaMemcpyAsync(w->dw.ms, ms.data(), ms.size() * sizeof(MoveState), cudaMemcpyHostToDevice, w->stream));
-  if (logpsi)
-    CK(cudaMemcpyAsync(logpsi, w->dw.logpsi, w->dw.W * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
-  CK(cudaStreamSynchronize(w->stream));
-  return device_status(w);
+  return QMC_OK;
 }
+
+extern "C" {
 
 int qmc_wf_eval_grad(qmc_walkers* w, int iat, double* grad)
 {

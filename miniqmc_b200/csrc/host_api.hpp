@@ -58,6 +58,10 @@ struct qmc_walkers_s
   bool tc_capable = false; // FP32, >= 128 threads, k <= 32, determinant on
   bool use_tc     = false; // Woodbury flushes on the tensor cores
   int max_moves   = 1; // moves the fused sweep evaluates together (qmc_walkers_set_move_batching)
+  // a request-loop job's batch: device memory from the server's pool,
+  // allocated and freed stream-ordered on its stream (else both null)
+  cudaStream_t alloc_stream = nullptr;
+  cudaMemPool_t alloc_pool  = nullptr;
 };
 
 // the tensor-core flush keeps (Binv V)^T as 32-row hi/lo tiles of up to 32
@@ -74,3 +78,10 @@ int recompute_dets(qmc_walkers* w);
 size_t walkers_footprint(qmc_system* s, int W, int k);
 // the sweep's SweepTask of a batch (device RNG streams)
 qmc::SweepTask sweep_task(qmc_walkers* w, int first_block);
+// request-loop batches: device memory stream-ordered from `pool` on `st`
+// (freed the same way by qmc_walkers_destroy); initialisation and
+// evaluateLog enqueued on the batch's stream without waiting
+int walkers_create_pooled(qmc_system* s, int n_walkers, int delay_rank, cudaStream_t st, cudaMemPool_t pool,
+                          qmc_walkers** out);
+int walkers_init_random(qmc_walkers* w, const uint32_t* seeds, bool sync);
+int evaluate_log_launch(qmc_walkers* w);
