@@ -76,8 +76,14 @@ int device_status(qmc_walkers* w)
   CK(cudaMemcpyAsync(&st, w->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost, w->stream));
   CK(cudaStreamSynchronize(w->stream));
   if (st)
-  {
     CK(cudaMemsetAsync(w->dw.status, 0, sizeof(unsigned), w->stream));
+  return status_from_bits(st);
+}
+
+int status_from_bits(unsigned st)
+{
+  if (st)
+  {
     if (st & DEV_ERR_SINGULAR)
       return fail(QMC_ERR_SINGULAR, "zero pivot in the FP64 inverse of a Slater matrix");
     if (st & DEV_ERR_NONFINITE)

@@ -70,6 +70,8 @@ inline size_t tc_image_floats(int npad) { return (size_t)2 * 32 * npad; }
 
 // device error bits of a batch -> status (and message); synchronises
 int device_status(qmc_walkers* w);
+// device error bits -> status (and message)
+int status_from_bits(unsigned bits);
 // SPO matrices + FP64 inverse and log-det of every walker (evaluateLog's
 // determinant part, also the periodic refresh)
 int recompute_dets(qmc_walkers* w);

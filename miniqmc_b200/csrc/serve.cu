@@ -369,6 +369,16 @@ int qmc_autotune(qmc_system* sys, int n_walkers, const int* delays, int n_delays
 // --------------------------------------------------------------- server --
 namespace
 {
+// pinned host space a retiring job's results land in
+struct ResultSlot
+{
+  int cap            = 0;
+  long long* acc     = nullptr; // [cap]
+  double* lp         = nullptr; // [cap]
+  unsigned* status   = nullptr; // [1]
+  cudaEvent_t done   = nullptr; // recorded after the copies
+};
+
 struct Job
 {
   int64_t id;
@@ -383,6 +393,7 @@ struct Job
   int64_t accepted = 0;
   double logpsi_mean = 0;
   int status = QMC_OK;
+  ResultSlot slot;
 };
 } // namespace
 
@@ -391,11 +402,14 @@ struct qmc_server_s
   size_t budget = 0, used = 0;
   int threads = 128, recompute_every = 0;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool  = nullptr; // every job's device memory, stream-ordered on `stream`
   double t0 = 0;
   int64_t next_id = 1;
   std::map<int64_t, Job> jobs;
   std::deque<int64_t> waiting;
   std::vector<int64_t> running;
+  std::deque<int64_t> retiring; // swept to the end; results in flight to the host
+  std::vector<ResultSlot> free_slots;
   TaskList tasks;
   bool dirty = true;
   int64_t launches = 0, moves = 0;
@@ -403,48 +417,107 @@ struct qmc_server_s
 
 namespace
 {
+// admission: the batch's memory from the server's pool, its electrons and
+// evaluateLog enqueued on the server stream; nothing waits for the device
+// (an error of evaluateLog, e.g. a singular Slater matrix, lands in the
+// job's own status word and fails the job when it retires)
 int start_job(qmc_server_s* s, Job& j)
 {
-  int st = qmc_walkers_create(j.sys, j.W, j.delay, &j.w);
+  int st = walkers_create_pooled(j.sys, j.W, j.delay, s->stream, s->pool, &j.w);
   if (st)
-    return st;
-  if ((st = qmc_walkers_set_stream(j.w, s->stream)))
     return st;
   std::vector<uint32_t> seeds(j.W);
   for (int i = 0; i < j.W; ++i)
     seeds[i] = j.seed + 7919u * (uint32_t)i;
-  if ((st = qmc_walkers_init_random(j.w, seeds.data())))
+  if ((st = walkers_init_random(j.w, seeds.data(), false)))
     return st;
-  if ((st = qmc_wf_evaluate_log(j.w, nullptr)))
+  if ((st = evaluate_log_launch(j.w)))
     return st;
   CK(cudaMemsetAsync(j.w->dw.accepted, 0, j.W * sizeof(long long), s->stream));
   return QMC_OK;
 }
 
+int get_slot(qmc_server_s* s, int W, ResultSlot& out)
+{
+  for (size_t i = 0; i < s->free_slots.size(); ++i)
+    if (s->free_slots[i].cap >= W)
+    {
+      out = s->free_slots[i];
+      s->free_slots.erase(s->free_slots.begin() + (long)i);
+      return QMC_OK;
+    }
+  ResultSlot r;
+  r.cap = std::max(W, 256);
+  CK(cudaMallocHost(&r.acc, r.cap * sizeof(long long)));
+  CK(cudaMallocHost(&r.lp, r.cap * sizeof(double)));
+  CK(cudaMallocHost(&r.status, sizeof(unsigned)));
+  CK(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+  out = r;
+  return QMC_OK;
+}
+
+// the job has made its steps: its results and status word start towards
+// pinned host memory behind its last launch; the job retires when they land
+int begin_retire(qmc_server_s* s, Job& j)
+{
+  int st = get_slot(s, j.W, j.slot);
+  if (st)
+    return st;
+  CK(cudaMemcpyAsync(j.slot.acc, j.w->dw.accepted, j.W * sizeof(long long), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(j.slot.lp, j.w->dw.logpsi, j.W * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(j.slot.status, j.w->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaEventRecord(j.slot.done, s->stream));
+  s->retiring.push_back(j.id);
+  return QMC_OK;
+}
+
+// the job's walkers are gone (stream-ordered) and its memory is free for
+// admission; status QMC_OK with a clean status word means done
 void finish_job(qmc_server_s* s, Job& j, int status)
 {
   if (j.w)
   {
-    if (status == QMC_OK)
-    {
-      std::vector<int64_t> acc(j.W);
-      std::vector<double> lp(j.W);
-      status = qmc_sweep_results(j.w, acc.data(), lp.data());
-      j.accepted    = 0;
-      j.logpsi_mean = 0;
-      for (int i = 0; i < j.W; ++i)
-      {
-        j.accepted += acc[i];
-        j.logpsi_mean += lp[i] / j.W;
-      }
-    }
-    qmc_walkers_destroy(j.w);
+    qmc_walkers_destroy(j.w); // pooled: cudaFreeAsync on the server stream
     j.w = nullptr;
   }
   s->used -= j.bytes;
   j.status = status;
   j.state  = status == QMC_OK ? QMC_JOB_DONE : QMC_JOB_FAILED;
   j.t_done = now_s() - s->t0;
+  if (j.slot.done)
+  {
+    s->free_slots.push_back(j.slot);
+    j.slot = ResultSlot();
+  }
+}
+
+// retire every job whose results have landed (wait for the oldest if
+// `block`); returns how many retired
+int poll_retiring(qmc_server_s* s, bool block)
+{
+  int n = 0;
+  while (!s->retiring.empty())
+  {
+    Job& j = s->jobs[s->retiring.front()];
+    cudaError_t q = block && n == 0 ? cudaEventSynchronize(j.slot.done) : cudaEventQuery(j.slot.done);
+    if (q == cudaErrorNotReady)
+      break;
+    s->retiring.pop_front();
+    int status = q == cudaSuccess ? status_from_bits(*j.slot.status) : QMC_ERR_CUDA;
+    if (status == QMC_OK)
+    {
+      j.accepted    = 0;
+      j.logpsi_mean = 0;
+      for (int i = 0; i < j.W; ++i)
+      {
+        j.accepted += j.slot.acc[i];
+        j.logpsi_mean += j.slot.lp[i] / j.W;
+      }
+    }
+    finish_job(s, j, status);
+    ++n;
+  }
+  return n;
 }
 } // namespace
 
@@ -454,14 +527,32 @@ int qmc_server_create(size_t memory_budget, int threads, int recompute_every, qm
 {
   if (!out || memory_budget == 0 || threads % 32 || threads < 64 || threads > 256 || recompute_every < 0)
     return fail(QMC_ERR_ARG, "bad server arguments");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
   auto* s            = new qmc_server_s;
   s->budget          = memory_budget;
   s->threads         = threads;
   s->recompute_every = recompute_every;
   s->t0              = now_s();
   cudaError_t e      = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  cudaMemPoolProps props{};
+  props.allocType     = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id   = dev;
+  if (e == cudaSuccess)
+    e = cudaMemPoolCreate(&s->pool, &props);
+  if (e == cudaSuccess)
+  {
+    // keep freed job memory in the pool for the next admissions
+    uint64_t keep = ~0ull;
+    e             = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   if (e != cudaSuccess)
   {
+    if (s->stream)
+      cudaStreamDestroy(s->stream);
+    if (s->pool)
+      cudaMemPoolDestroy(s->pool);
     delete s;
     return fail(QMC_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -475,8 +566,21 @@ int qmc_server_destroy(qmc_server* s)
     return QMC_OK;
   cudaStreamSynchronize(s->stream);
   for (auto& kv : s->jobs)
+  {
     if (kv.second.w)
       qmc_walkers_destroy(kv.second.w);
+    if (kv.second.slot.done)
+      s->free_slots.push_back(kv.second.slot);
+  }
+  cudaStreamSynchronize(s->stream);
+  for (auto& r : s->free_slots)
+  {
+    cudaFreeHost(r.acc);
+    cudaFreeHost(r.lp);
+    cudaFreeHost(r.status);
+    cudaEventDestroy(r.done);
+  }
+  cudaMemPoolDestroy(s->pool);
   cudaStreamDestroy(s->stream);
   delete s;
   return QMC_OK;
@@ -507,6 +611,9 @@ int qmc_server_tick(qmc_server* s, int* n_running, int* n_waiting)
 {
   if (!s)
     return fail(QMC_ERR_ARG, "null handle");
+  // jobs whose results have landed free their memory first; with nothing
+  // left to launch, wait for the oldest instead of spinning
+  poll_retiring(s, s->running.empty() && !s->retiring.empty());
   // admit, in arrival order, every waiting job that fits the budget now
   for (auto it = s->waiting.begin(); it != s->waiting.end();)
   {
@@ -558,7 +665,8 @@ int qmc_server_tick(qmc_server* s, int* n_running, int* n_waiting)
       }
       if (++j.steps_done == j.steps)
       {
-        finish_job(s, j, QMC_OK); // reads the results (stream-ordered, synchronising)
+        if ((st = begin_retire(s, j)))
+          finish_job(s, j, st);
         s->dirty = true;
       }
       else
@@ -567,7 +675,7 @@ int qmc_server_tick(qmc_server* s, int* n_running, int* n_waiting)
     s->running.swap(still);
   }
   if (n_running)
-    *n_running = (int)s->running.size();
+    *n_running = (int)(s->running.size() + s->retiring.size());
   if (n_waiting)
     *n_waiting = (int)s->waiting.size();
   return QMC_OK;

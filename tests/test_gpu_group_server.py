@@ -155,3 +155,34 @@ def test_handles_are_reentrant_across_host_threads():
     for i in range(2):
         for a, b in zip(alone[i], together[i]):
             assert np.array_equal(a, b)
+
+
+def test_server_failed_job_leaves_the_others_unchanged():
+    """A job whose Slater matrices are singular (the reference's own rank-1
+    orbital fill, einspline_spo.hpp:145-155, on an FP64 table) fails inside
+    the request loop: its evaluateLog raises the zero-pivot bit in the job's
+    own status word, the job keeps its slot in the shared launches until it
+    retires, and it is reported QMC_JOB_FAILED with QMC_ERR_SINGULAR.  The
+    jobs admitted before and after it finish with exactly the results they
+    give alone (the reference has no counterpart: it aborts the process,
+    Configuration.h:35-39)."""
+    lib = H.product()
+    sa, sb = _system((1, 1, 1), capi.PREC_FP64), _system((2, 1, 1), capi.PREC_FP64)
+    bad_spec = api.SystemSpec(lib, cell=capi.NIO_PRIM4, tiling=(1, 1, 1), grid=(12, 12, 12),
+                              fill=capi.FILL_REFERENCE, spo_seed=11, jastrow='synthetic')
+    bad = api.System(lib, bad_spec, capi.PREC_FP64)
+    jobs = [(sa, 8, 5, 4, 3), (bad, 4, 4, 4, 7), (sb, 4, 3, 8, 5)]
+    srv = api.Server(lib, 8 << 30, threads=128, recompute_every=2)
+    ids = [srv.submit(*j) for j in jobs]
+    for _ in range(10000):
+        running, waiting = srv.tick()
+        if running == 0 and waiting == 0:
+            break
+    infos = [srv.job(i) for i in ids]
+    assert infos[1]['state'] == capi.JOB_FAILED
+    assert capi.STATUS[infos[1]['status']] == 'QMC_ERR_SINGULAR'
+    for k in (0, 2):
+        assert infos[k]['state'] == capi.JOB_DONE, infos[k]
+        alone, _ = _run_server(api.Server(lib, 8 << 30, threads=128, recompute_every=2), [jobs[k]])
+        assert alone[0]['n_accepted'] == infos[k]['n_accepted']
+        assert alone[0]['logpsi_mean'] == infos[k]['logpsi_mean']
