@@ -59,7 +59,7 @@ def parse():
                     help='nio128: the headline batch; uneven: three NiO systems in one autotuned, graph-replayed '
                          'launch; serve: Poisson-arrival request loop; nlpp: the NonLocalPP ratios')
     ap.add_argument('--nlpp-grid', default='148,148,148', help='nlpp: orbital grid of the NiO 2,2,1 cell')
-    ap.add_argument('--jobs', type=int, default=200, help='serve: number of jobs (the full configuration is 2000)')
+    ap.add_argument('--jobs', type=int, default=2000, help='serve: number of jobs (the configuration: 2000)')
     ap.add_argument('--rate', type=float, default=20.0, help='serve: arrivals per second')
     ap.add_argument('--budget-gb', type=float, default=100.0, help='serve: device memory budget of the server')
     ap.add_argument('--no-tune', action='store_true', help='uneven: skip the autotuner (default launch settings)')

@@ -540,6 +540,11 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
 // zero (numerically singular).  At the end A holds the exchanged matrix:
 // A^{-1}[a][b] = M[piv[a]][pinv[b]], so psiM[i][j] = M[piv[j]][pinv[i]];
 // the sign of det A is the pivots' sign times the parity of piv.
+// the panel's rank-32 update on the FP64 tensor cores (mma.sync .f64)
+// rather than as CUDA-core FMAs with a 4 x 4 register tile
+#ifndef GJB_DMMA
+#define GJB_DMMA 1
+#endif
 constexpr int GJB_B = 32;      // panel width
 constexpr int GJB_FS = GJB_B + 1; // padded panel row (conflict-free row-per-thread access)
 __host__ __device__ constexpr size_t gjb_smem_bytes(int n)
@@ -692,6 +697,68 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
         Rb[idx]     = (k < bw && jj < jw) ? M[(size_t)piv[c0 + k] * npad + j0 + jj] : 0.0;
       }
       __syncthreads();
+#if GJB_DMMA
+      // the rank-32 update on the FP64 tensor cores (mma.sync m8n8k4 .f64):
+      // each warp takes three 8-row groups at a time and the chunk's four
+      // 8-column tiles; fragments: A (8 x 4 of the panel) one element per
+      // lane at (lane / 4, lane % 4), B (4 x 8 of the pivot rows) at
+      // (lane % 4, lane / 4), C (8 x 8) two at (lane / 4, 2 (lane % 4) + e)
+      {
+        const int qr = lane >> 2, qc = lane & 3;
+        for (int gb = wid * 3; gb * 8 < n; gb += nw * 3)
+        {
+          double acc[3][4][2];
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+          {
+            const int i     = (gb + u) * 8 + qr;
+            const int c     = i < n ? pinv[i] : c0;
+            const bool zero = i >= n || (c >= c0 && c < c0 + bw);
+            const double* mi = M + (size_t)(i < n ? i : 0) * npad + j0;
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+              for (int e = 0; e < 2; ++e)
+              {
+                const int col = t * 8 + 2 * qc + e;
+                acc[u][t][e]  = (zero || col >= jw) ? 0.0 : mi[col];
+              }
+          }
+#pragma unroll 2
+          for (int k = 0; k < GJB_B; k += 4)
+          {
+            double b[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+              b[t] = Rb[(k + qc) * 32 + t * 8 + qr];
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+            {
+              const double a = F[min((gb + u) * 8 + qr, n - 1) * GJB_FS + k + qc];
+#pragma unroll
+              for (int t = 0; t < 4; ++t)
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                             : "+d"(acc[u][t][0]), "+d"(acc[u][t][1])
+                             : "d"(a), "d"(b[t]));
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+          {
+            const int i = (gb + u) * 8 + qr;
+            if (i >= n)
+              continue;
+            double* mi = M + (size_t)i * npad + j0;
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+              for (int e = 0; e < 2; ++e)
+                if (t * 8 + 2 * qc + e < jw)
+                  mi[t * 8 + 2 * qc + e] = acc[u][t][e];
+          }
+        }
+      }
+#else
       // each thread updates a 4-row x 4-column tile: columns j0 + 2 cg + {0, 1}
       // and j0 + 16 + 2 cg + {0, 1} (cg = lane % 8: a row's 32 columns are
       // two 128-byte runs over 8 lanes), rows ib..ib+3 (rg = lane / 8), so
@@ -749,6 +816,7 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
           }
         }
       }
+#endif
     }
     for (int idx = tid; idx < n * bw; idx += NT)
     {
