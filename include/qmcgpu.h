@@ -265,6 +265,13 @@ int qmc_wf_eval_grad(qmc_walkers* w, int iat, double* grad /* [W][3] */);
 int qmc_wf_ratio_grad(qmc_walkers* w, int iat, double* ratio, double* grad);
 /* ratio only (SPOSet values, no gradients). */
 int qmc_wf_ratio(qmc_walkers* w, int iat, double* ratio);
+/* evaluateRatios (WaveFunction::evaluateRatios over a VirtualParticleSet,
+ * WaveFunction.h:72, DiracDeterminant.cpp:216-224): ratios[k] =
+ * psi(R with electron iat at pos[k]) / psi(R) for ONE walker of the batch,
+ * at n_pos absolute positions pos[n_pos][3].  The batch's move state is
+ * untouched (no makeMove, and the determinants keep their update mode).
+ * Needs completeUpdates done (QMC_ERR_STATE with delayed rows pending). */
+int qmc_wf_evaluate_ratios(qmc_walkers* w, int walker, int iat, int n_pos, const double* pos, double* ratios);
 /* accept[i] != 0: acceptMove(iat); else restore(iat) (a no-op). */
 int qmc_wf_accept_restore(qmc_walkers* w, int iat, const int* accept);
 int qmc_wf_complete_updates(qmc_walkers* w);

@@ -314,6 +314,14 @@ class Walkers:
         self.lib.call('wf_ratio', self.h, iat, _pd(r))
         return r
 
+    def evaluate_ratios(self, walker, iat, pos):
+        """WaveFunction::evaluateRatios: one walker's ratios of electron iat
+        at absolute positions pos[n][3]."""
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        r = np.zeros(len(p))
+        self.lib.call('wf_evaluate_ratios', self.h, walker, iat, len(p), _pd(p), _pd(r))
+        return r
+
     def accept_restore(self, iat, accept):
         a = np.ascontiguousarray(accept, dtype=np.int32)
         self.lib.call('wf_accept_restore', self.h, iat, _pi(a))

@@ -97,6 +97,7 @@ SIGNATURES = {
     'wf_eval_grad': (I, [P, I, PD]),
     'wf_ratio_grad': (I, [P, I, PD, PD]),
     'wf_ratio': (I, [P, I, PD]),
+    'wf_evaluate_ratios': (I, [P, I, I, I, PD, PD]),
     'wf_accept_restore': (I, [P, I, PI]),
     'wf_complete_updates': (I, [P]),
     'wf_evaluate_gl': (I, [P, PD, PD, PD]),

@@ -44,6 +44,15 @@ struct NlppArgs
   long long* count;  // [W] points evaluated
   double* ratios;    // walker 0: every ratio in (electron, ion, knot) order, or null
   int max_ratios;
+  // the points form (WaveFunction::evaluateRatios): one CTA, walker
+  // `walker`, electron `pts_iat` (>= 0) at the n_pts positions `pts`
+  // ([n][3], absolute), ratios into pts_out ([n]); the ion search, wsum and
+  // count are not used
+  int walker;
+  int pts_iat;
+  int n_pts;
+  const double* pts;
+  double* pts_out;
 };
 
 template <typename T>
@@ -65,7 +74,8 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
   extern __shared__ int cand[];
   const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = NT >> 5;
   load_sys(sys, ss);
-  const int w    = blockIdx.x;
+  const bool PTS = a.pts_iat >= 0;
+  const int w    = PTS ? a.walker : blockIdx.x;
   const WV<T> wv = make_wv<T>(dw, w);
   const bool DET = ss.comp & QMC_WF_DET, J1 = ss.comp & QMC_WF_J1, J2 = ss.comp & QMC_WF_J2;
   const bool J3  = ss.comp & QMC_WF_J3;
@@ -84,7 +94,7 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
   long long cnt   = 0;
   int n_out       = 0;
   const double wk = 1.0 / NLPP_K;
-  for (int jel = 0; jel < N; ++jel)
+  for (int jel = PTS ? a.pts_iat : 0; jel < (PTS ? a.pts_iat + 1 : N); ++jel)
   {
     const int s = jel < ss.n_up ? 0 : 1, r = jel - (s ? ss.n_up : 0);
     const double ex = wv.R[3 * jel], ey = wv.R[3 * jel + 1], ez = wv.R[3 * jel + 2];
@@ -92,7 +102,7 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
     if (tid == 0)
       s_n = 0;
     __syncthreads();
-    for (int c0 = 0; c0 < I; c0 += NT)
+    for (int c0 = 0; c0 < (PTS ? 0 : I); c0 += NT)
     {
       const int c = c0 + tid;
       bool in     = false;
@@ -133,18 +143,29 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
       }
       __syncthreads();
     }
-    const int n_in = min(s_n, NLPP_MAXIN);
+    // the points form takes its positions in groups of 12 (the last group's
+    // unused slots repeat its last point and are not reported)
+    const int n_in = PTS ? (a.n_pts + NLPP_K - 1) / NLPP_K : min(s_n, NLPP_MAXIN);
     for (int li = 0; li < n_in; ++li)
     {
       // ---- the 12 virtual positions and their stencils
       if (tid < NLPP_K)
       {
-        const int k     = tid;
-        const double d  = in_d[li];
-        const double sg = a.form == 0 ? 1.0 : -1.0;
-        vpos[k][0]      = ex + sg * in_dx[li][0] + d * a.rot[k][0];
-        vpos[k][1]      = ey + sg * in_dx[li][1] + d * a.rot[k][1];
-        vpos[k][2]      = ez + sg * in_dx[li][2] + d * a.rot[k][2];
+        const int k = tid;
+        if (PTS)
+        {
+          const int q = min(li * NLPP_K + k, a.n_pts - 1);
+          for (int c = 0; c < 3; ++c)
+            vpos[k][c] = a.pts[3 * q + c];
+        }
+        else
+        {
+          const double d  = in_d[li];
+          const double sg = a.form == 0 ? 1.0 : -1.0;
+          vpos[k][0]      = ex + sg * in_dx[li][0] + d * a.rot[k][0];
+          vpos[k][1]      = ey + sg * in_dx[li][1] + d * a.rot[k][1];
+          vpos[k][2]      = ez + sg * in_dx[li][2] + d * a.rot[k][2];
+        }
         if (DET)
           spline_locate(sys, vpos[k], sk[k]);
       }
@@ -203,9 +224,29 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
       if (J2)
       {
         const int gi = jel < ss.n_up ? 0 : 1;
-        const double sg = a.form == 0 ? 1.0 : -1.0;
-        const T cx = (T)(ex + sg * in_dx[li][0]), cy = (T)(ey + sg * in_dx[li][1]), cz = (T)(ez + sg * in_dx[li][2]);
-        const T reach  = (T)in_d[li] + (ss.j2uu.cutoff > ss.j2ud.cutoff ? ss.j2uu.cutoff : ss.j2ud.cutoff);
+        // the sphere's centre and radius; for the points form the first
+        // point and the largest distance of the others from it
+        double gc[3], grad = 0.0;
+        if (PTS)
+        {
+          for (int c = 0; c < 3; ++c)
+            gc[c] = vpos[0][c];
+          for (int k = 1; k < NLPP_K; ++k)
+          {
+            const double qx = vpos[k][0] - gc[0], qy = vpos[k][1] - gc[1], qz = vpos[k][2] - gc[2];
+            grad = fmax(grad, sqrt(qx * qx + qy * qy + qz * qz));
+          }
+          grad *= 1.0 + 1e-6; // covers the rounding of the test below
+        }
+        else
+        {
+          const double sg = a.form == 0 ? 1.0 : -1.0;
+          for (int c = 0; c < 3; ++c)
+            gc[c] = (c == 0 ? ex : c == 1 ? ey : ez) + sg * in_dx[li][c];
+          grad = in_d[li];
+        }
+        const T cx = (T)gc[0], cy = (T)gc[1], cz = (T)gc[2];
+        const T reach  = (T)grad + (ss.j2uu.cutoff > ss.j2ud.cutoff ? ss.j2uu.cutoff : ss.j2ud.cutoff);
         const int per  = ((((N + 31) >> 5) + nw - 1) / nw) << 5;
         int* lst       = cand + wid * per;
         int cnt        = 0;
@@ -327,13 +368,22 @@ __global__ void __launch_bounds__(256, 3) nlpp_kernel(const DevSystem* __restric
             ratio *= exp(u3 - sums[3 * NLPP_K + k]);
           wsum += wk * ratio;
           ++cnt;
-          if (w == 0 && a.ratios && n_out < a.max_ratios)
+          if (PTS)
+          {
+            if (li * NLPP_K + k < a.n_pts)
+              a.pts_out[li * NLPP_K + k] = ratio;
+          }
+          else if (w == 0 && a.ratios && n_out < a.max_ratios)
             a.ratios[n_out++] = ratio;
         }
       }
       __syncthreads();
     }
   }
+  // DiracDeterminant::evaluateRatios leaves the update mode as it was
+  // (DiracDeterminant.cpp:216-224)
+  if (PTS)
+    return;
   if (tid == 0)
   {
     a.wsum[w]  = wsum;
@@ -356,12 +406,12 @@ cudaError_t launch_nlpp(bool fp32, const DevSystem* sys, const DevWalkers& dw, c
   if (fp32)
   {
     cudaFuncSetAttribute(nlpp_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    nlpp_kernel<float><<<dw.W, threads, bytes, st>>>(sys, dw, a);
+    nlpp_kernel<float><<<a.pts_iat >= 0 ? 1 : dw.W, threads, bytes, st>>>(sys, dw, a);
   }
   else
   {
     cudaFuncSetAttribute(nlpp_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    nlpp_kernel<double><<<dw.W, threads, bytes, st>>>(sys, dw, a);
+    nlpp_kernel<double><<<a.pts_iat >= 0 ? 1 : dw.W, threads, bytes, st>>>(sys, dw, a);
   }
   return cudaGetLastError();
 }
@@ -424,6 +474,7 @@ int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, 
     return fail(QMC_ERR_ARG, "bad NLPP arguments");
   const size_t W = w->dw.W;
   NlppArgs a{};
+  a.pts_iat = -1;
   nlpp_sphere((int)w->nlpp_calls, a.rot);
   a.rmax       = rmax;
   a.form       = form;
@@ -454,6 +505,30 @@ int qmc_nlpp_evaluate(qmc_walkers* w, double rmax, int form, int64_t* n_points, 
     if (n_points)
       n_points[i] = hc[i];
   }
+  return device_status(w);
+}
+
+int qmc_wf_evaluate_ratios(qmc_walkers* w, int walker, int iat, int n_pos, const double* pos, double* ratios)
+{
+  if (!w || walker < 0 || walker >= w->dw.W || iat < 0 || iat >= w->dw.N || n_pos < 0 || (n_pos && (!pos || !ratios)))
+    return fail(QMC_ERR_ARG, "bad evaluateRatios arguments");
+  if (n_pos == 0)
+    return QMC_OK;
+  NlppArgs a{};
+  a.walker   = walker;
+  a.pts_iat  = iat;
+  a.n_pts    = n_pos;
+  double* d  = nullptr;
+  CK(cudaMallocAsync(&d, (size_t)n_pos * 4 * sizeof(double), w->stream));
+  CK(cudaMemcpyAsync(d, pos, (size_t)n_pos * 3 * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  a.pts     = d;
+  a.pts_out = d + (size_t)n_pos * 3;
+  int threads = std::max(64, std::min(256, w->threads));
+  CK(launch_nlpp(w->fp32, w->sys->d, w->dw, a, threads, w->stream));
+  w->launches++;
+  CK(cudaMemcpyAsync(ratios, a.pts_out, (size_t)n_pos * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CK(cudaFreeAsync(d, w->stream));
+  CK(cudaStreamSynchronize(w->stream));
   return device_status(w);
 }
 

@@ -463,6 +463,13 @@ int oracle_wf_ratio(oracle_walkers* o, int iat, double* ratio)
     ratio[i] = o->w[i].ratio(iat);
   return 0;
 }
+int oracle_wf_evaluate_ratios(oracle_walkers* o, int walker, int iat, int n_pos, const double* pos, double* ratios)
+{
+  if (!o || walker < 0 || walker >= o->W || iat < 0 || iat >= o->w[walker].sys->n_elec || n_pos < 0)
+    return 1;
+  o->w[walker].evaluateRatios(iat, n_pos, pos, ratios);
+  return 0;
+}
 int oracle_wf_accept_restore(oracle_walkers* o, int iat, const int* accept)
 {
   for (int i = 0; i < o->W; ++i)

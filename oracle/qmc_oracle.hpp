@@ -2243,6 +2243,28 @@ struct Walker
     return sum;
   }
 
+  // ---- WaveFunction::evaluateRatios over a VirtualParticleSet
+  // (NonLocalPP.hpp:115-134, DiracDeterminant.cpp:216-224): the ratio of
+  // electron jel at each absolute position, the determinants' update mode
+  // left as it was ----
+  void evaluateRatios(int jel, int n, const double* p, double* out)
+  {
+    const int s     = jel < sys->n_up ? 0 : 1;
+    const bool keep = det[s].partial;
+    for (int k = 0; k < n; ++k)
+    {
+      activePtcl = jel;
+      for (int c = 0; c < 3; ++c)
+        activePos[c] = p[3 * k + c];
+      sys->lattice.computeDistances(activePos, R.data(), aa_r.data(), aa_dx.data(), aa_dy.data(), aa_dz.data(), 0,
+                                    sys->n_elec, jel);
+      ab_row(activePos, ab_r.data(), ab_dx.data(), ab_dy.data(), ab_dz.data());
+      out[k] = ratio(jel);
+      rejectMove_pset(jel);
+    }
+    det[s].partial = keep;
+  }
+
   // ---- WaveFunction (WaveFunction.cpp:178-279) ----
   bool evaluateLog()
   {
