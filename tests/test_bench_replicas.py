@@ -31,7 +31,7 @@ def _rank(rank, world, port, out):
 def test_job_rate_takes_the_slowest_rank():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context('spawn').Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
