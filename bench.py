@@ -527,7 +527,7 @@ def reference_binary(mixed=False):
     return path if os.access(path, os.X_OK) else None
 
 
-def reference_miniqmc(args, n_threads, steps, mixed=False):
+def reference_miniqmc(args, n_threads, steps, mixed=False, delay=None):
     """Time the reference's own miniqmc on the host cores: one walker per
     OpenMP thread (-w = threads), its Release build, OPENBLAS_NUM_THREADS=1.
     The bench's NiO tiling (n1,n2,n3) of the 4-atom cell is the reference's
@@ -547,7 +547,8 @@ def reference_miniqmc(args, n_threads, steps, mixed=False):
         raise RuntimeError('tiling %s has no reference equivalent (odd factor)' % args.tiling)
     g = '%d %d %d' % (t[0] // 2, t[1] // 2, t[2] // 2)
     env = dict(os.environ, OMP_NUM_THREADS=str(n_threads), OPENBLAS_NUM_THREADS='1')
-    cmd = [exe, '-g', g, '-m', '2', '-n', str(steps), '-N', '1', '-r', '0.5', '-k', str(args.delay),
+    k = args.delay if delay is None else delay
+    cmd = [exe, '-g', g, '-m', '2', '-n', str(steps), '-N', '1', '-r', '0.5', '-k', str(k),
            '-w', str(n_threads), '-x', '0']
     with tempfile.TemporaryDirectory() as d:  # the driver writes info_*.xml into its working directory
         r = subprocess.run(cmd, cwd=d, env=env, capture_output=True, text=True, timeout=900)
@@ -560,14 +561,15 @@ def reference_miniqmc(args, n_threads, steps, mixed=False):
     rate = float(m.group(1)) * steps / float(n_elec) ** 2
     desc = ('reference miniqmc %s (%s build, -ffast-math -O3, OpenBLAS): -g "%s" -m 2 -k %d -w %d -n %d -x 0, '
             'one walker per thread' % (os.path.basename(exe), 'mixed-precision' if mixed else 'FP64', g,
-                                       args.delay, n_threads, steps))
+                                       k, n_threads, steps))
     return rate, desc
 
 
 def run_reference(args, rank, world):
     """The reference arm: the reference's own miniqmc Release build on all
     host cores (rank 0 only), each timed step one MC step of its walkers; its
-    mixed-precision build and the FP64 oracle port are reported beside it."""
+    mixed-precision build and its rank-1 form (-k 1) are reported beside
+    it."""
     if rank != 0:
         return
     ncpu = os.cpu_count() or 1
@@ -583,6 +585,12 @@ def run_reference(args, rank, world):
         extra['reference_mixed'] = {'value': mv, 'unit': 'electron-moves/s', 'sample': mdesc}
     except Exception as ex:
         extra['reference_mixed'] = {'value': None, 'note': str(ex)}
+    try:
+        # the reference's rank-1 (Sherman-Morrison) form, -k 1
+        kv, kdesc = reference_miniqmc(args, ncpu, args.steps, delay=1)
+        extra['reference_k1'] = {'value': kv, 'unit': 'electron-moves/s', 'sample': kdesc}
+    except Exception as ex:
+        extra['reference_k1'] = {'value': None, 'note': str(ex)}
     tiling = args.tiling
     print(json.dumps({
         'impl': 'reference', 'metric': 'electron-moves/s', 'value': v, 'unit': 'electron-moves/s',
