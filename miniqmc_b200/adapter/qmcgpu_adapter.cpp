@@ -316,6 +316,7 @@ int WaveFunctionComponentGpu::note(int status, const char* what)
 
 Batch& WaveFunctionComponentGpu::batch_of(const std::vector<WaveFunctionComponent*>& list) const
 {
+  ensure_device(); // the drivers call from any OpenMP thread
   Batch* b = batch_.get();
   bool ok  = b && (int)list.size() == b->W;
   for (size_t i = 0; ok && i < list.size(); ++i)
@@ -327,6 +328,7 @@ Batch& WaveFunctionComponentGpu::batch_of(const std::vector<WaveFunctionComponen
 
 Batch& WaveFunctionComponentGpu::single(const char* verb)
 {
+  ensure_device(); // the drivers call from any OpenMP thread
   if (!batch_)
     fail("evaluateLog must come first");
   if (batch_->W != 1)
@@ -411,6 +413,7 @@ void WaveFunctionComponentGpu::restore(int iat)
 
 WaveFunctionComponentGpu::ValueType WaveFunctionComponentGpu::ratio(ParticleSet& P, int iat)
 {
+  ensure_device();
   if (!batch_)
     fail("evaluateLog must come first");
   double q = 0.0;
@@ -456,6 +459,7 @@ void WaveFunctionComponentGpu::completeUpdates()
 
 void WaveFunctionComponentGpu::evaluateRatios(VirtualParticleSet& VP, std::vector<ValueType>& ratios)
 {
+  ensure_device();
   if (!batch_)
     fail("evaluateLog must come first");
   const int n = VP.getTotalNum();
