@@ -340,9 +340,11 @@ int qmc_walkers_enable_timers(qmc_walkers* w, int enable);
 /* Woodbury flush on the tensor cores (tcgen05, 3xTF32 with FP32
  * accumulation) or on the CUDA cores (FP32 FMA).  The tensor-core flush is
  * on by default wherever it applies: FP32 walkers with the determinant,
- * delay rank <= 32 and >= 128 threads per walker (480 or more orbitals per
- * spin).  QMC_ERR_ARG when asked for where it does not apply.  Both compute
- * DelayedUpdate::updateInvMat (DelayedUpdate.h:184-191). */
+ * delay rank <= 64 and >= 128 threads per walker (480 or more orbitals per
+ * spin).  Its tiles take 48 KB of shared memory per walker up to delay 32
+ * and 96 KB above (two walkers per SM).  QMC_ERR_ARG when asked for where
+ * it does not apply.  Both compute DelayedUpdate::updateInvMat
+ * (DelayedUpdate.h:184-191). */
 int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable);
 /* Limit, in SM cycles, of every bounded wait of the tensor-core flush on the
  * MMAs it issued (no reference counterpart: the reference has no device
@@ -377,6 +379,10 @@ int qmc_walkers_set_threads(qmc_walkers* w, int threads);
 enum { QMC_PREFETCH_AUTO = 0, QMC_PREFETCH_OFF = 1, QMC_PREFETCH_ON = 2 };
 int qmc_walkers_set_prefetch(qmc_walkers* w, int mode);
 int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* tensor_cores);
+/* Walkers (CTAs) of this batch's fused sweep that one SM holds at once with
+ * its present settings (registers, shared memory, block size): with W
+ * walkers a launch runs in ceil(W / (walkers_per_sm x SMs)) waves. */
+int qmc_walkers_occupancy(const qmc_walkers* w, int* walkers_per_sm);
 
 /* Batch groups (no reference counterpart: the reference's flex_ batch,
  * miniqmc_sync_move.cpp:432-521, holds movers of one system).  A group
@@ -468,7 +474,7 @@ int qmc_detengine_accept_row(qmc_detengine* e, int row, const double* psiv);
 int qmc_detengine_update_inv_mat(qmc_detengine* e);
 int qmc_detengine_get_ainv(qmc_detengine* e, double* ainv);
 /* The engine's flushes on the tensor cores (FP32 engines with delay rank
- * <= 32; on by default there) or on the CUDA cores. */
+ * <= 64; on by default there) or on the CUDA cores. */
 int qmc_detengine_set_tensor_cores(qmc_detengine* e, int enable);
 
 /* Local kinetic energy of every walker, -1/2 sum_i (L_i + |G_i|^2), from

@@ -138,6 +138,7 @@ PRODUCT_ONLY = {
     'walkers_checkpoint': (I, [P, P, C.c_size_t]),
     'walkers_restore': (I, [P, P, C.c_size_t]),
     'walkers_get_config': (I, [P, PI, PI, PI]),
+    'walkers_occupancy': (I, [P, PI]),
     'group_create': (I, [C.POINTER(P), I, C.POINTER(P)]),
     'group_destroy': (I, [P]),
     'group_set_threads': (I, [P, I]),

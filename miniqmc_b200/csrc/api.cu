@@ -652,8 +652,8 @@ size_t walkers_footprint(qmc_system* s, int W, int k)
   const int nvec    = s->h.npad / (s->fp32 ? 4 : 2);
   const int threads = std::min(256, std::max(std::max(64, 2 * k), round_up(nvec, 32)));
   size_t b          = t.bytes + (size_t)W * 2 * s->h.norb * s->h.npad * sizeof(double); // FP64 inverse scratch
-  if (s->fp32 && threads >= 128 && k <= 32 && (s->h.comp & QMC_WF_DET))
-    b += (size_t)W * tc_image_floats(s->h.npad) * sizeof(float);
+  if (s->fp32 && threads >= 128 && k <= TC_KD && (s->h.comp & QMC_WF_DET))
+    b += (size_t)W * tc_image_floats(s->h.npad, k) * sizeof(float);
   return b;
 }
 
@@ -703,10 +703,10 @@ int qmc_walkers_create(qmc_system* s, int n_walkers, int delay_rank, qmc_walkers
   const int vw   = w->fp32 ? 4 : 2;
   const int nvec = s->h.npad / vw;
   w->threads     = std::min(256, std::max(std::max(64, 2 * delay_rank), round_up(nvec, 32)));
-  w->tc_capable  = w->fp32 && w->threads >= 128 && delay_rank <= 32 && (s->h.comp & QMC_WF_DET);
+  w->tc_capable  = w->fp32 && w->threads >= 128 && delay_rank <= TC_KD && (s->h.comp & QMC_WF_DET);
   if (w->tc_capable)
   {
-    if (dalloc(w->allocs, w->bytes, &w->dw.tci, (size_t)n_walkers * tc_image_floats(w->dw.npad)))
+    if (dalloc(w->allocs, w->bytes, &w->dw.tci, (size_t)n_walkers * tc_image_floats(w->dw.npad, delay_rank)))
     {
       free_walkers(w);
       delete w;
@@ -746,10 +746,10 @@ int walkers_create_pooled(qmc_system* s, int n_walkers, int delay_rank, cudaStre
   int rc          = alloc_walkers(w, s, n_walkers, delay_rank);
   const int vw    = w->fp32 ? 4 : 2;
   w->threads      = std::min(256, std::max(std::max(64, 2 * delay_rank), round_up(s->h.npad / vw, 32)));
-  w->tc_capable   = w->fp32 && w->threads >= 128 && delay_rank <= 32 && (s->h.comp & QMC_WF_DET);
+  w->tc_capable   = w->fp32 && w->threads >= 128 && delay_rank <= TC_KD && (s->h.comp & QMC_WF_DET);
   if (!rc && w->tc_capable)
   {
-    rc        = dalloc(w->allocs, w->bytes, &w->dw.tci, (size_t)n_walkers * tc_image_floats(w->dw.npad));
+    rc        = dalloc(w->allocs, w->bytes, &w->dw.tci, (size_t)n_walkers * tc_image_floats(w->dw.npad, delay_rank));
     w->use_tc = rc == QMC_OK;
   }
   if (rc)
@@ -834,12 +834,23 @@ int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* 
     *tensor_cores = w->use_tc ? 1 : 0;
   return QMC_OK;
 }
+int qmc_walkers_occupancy(const qmc_walkers* w, int* walkers_per_sm)
+{
+  if (!w || !walkers_per_sm)
+    return fail(QMC_ERR_ARG, "null pointer");
+  const int n = sweep_occupancy(w->fp32, w->threads, w->dw.k, w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0,
+                                w->max_moves > 1);
+  if (n < 0)
+    return fail(QMC_ERR_CUDA, "occupancy query failed");
+  *walkers_per_sm = n;
+  return QMC_OK;
+}
 int qmc_walkers_set_tensor_cores(qmc_walkers* w, int enable)
 {
   if (!w)
     return fail(QMC_ERR_ARG, "null handle");
   if (enable && (!w->tc_capable || w->threads < 128))
-    return fail(QMC_ERR_ARG, "tensor-core flush needs FP32 walkers, the determinant, delay rank <= 32 and >= 128 "
+    return fail(QMC_ERR_ARG, "tensor-core flush needs FP32 walkers, the determinant, delay rank <= 64 and >= 128 "
                              "threads per walker (480 or more orbitals per spin in FP32 give that)");
   w->use_tc = enable != 0;
   return QMC_OK;
@@ -1522,10 +1533,10 @@ int qmc_detengine_create_prec(int n, int delay, int precision, qmc_detengine_s**
   st |= dalloc(L, B, &d.lu, 2 * n * np);
   st |= dalloc(L, B, &d.status, 1);
   st |= dalloc(L, B, &d.ms, 1);
-  w->tc_capable = w->fp32 && delay <= 32;
+  w->tc_capable = w->fp32 && delay <= TC_KD;
   if (w->tc_capable)
   {
-    st |= dalloc(L, B, &d.tci, tc_image_floats(d.npad));
+    st |= dalloc(L, B, &d.tci, tc_image_floats(d.npad, delay));
     w->use_tc = true;
   }
   if (st)
@@ -1548,7 +1559,7 @@ int qmc_detengine_set_tensor_cores(qmc_detengine_s* e, int enable)
   if (!e)
     return fail(QMC_ERR_ARG, "null handle");
   if (enable && !e->w.tc_capable)
-    return fail(QMC_ERR_ARG, "tensor-core flush needs an FP32 engine with delay rank <= 32");
+    return fail(QMC_ERR_ARG, "tensor-core flush needs an FP32 engine with delay rank <= 64");
   e->w.use_tc = enable != 0;
   return QMC_OK;
 }

@@ -66,7 +66,9 @@ struct qmc_walkers_s
 
 // the tensor-core flush keeps (Binv V)^T as 32-row hi/lo tiles of up to 32
 // delays: 2 x 32 floats per padded orbital and walker
-inline size_t tc_image_floats(int npad) { return (size_t)2 * 32 * npad; }
+// the tensor-core flush's image of (Binv V)^T hi / lo tiles for delay ranks
+// up to k: npad / 32 tiles of 2 x 32 x Kd floats
+inline size_t tc_image_floats(int npad, int k) { return (size_t)2 * (k <= 32 ? 32 : 64) * npad; }
 
 // device error bits of a batch -> status (and message); synchronises
 int device_status(qmc_walkers* w);

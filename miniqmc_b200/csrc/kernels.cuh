@@ -59,6 +59,8 @@ struct LaunchCfg
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
                          double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3,
                          bool epoch);
+// CTAs (walkers) of one sweep launch that an SM holds at once, or -1
+int sweep_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool epoch);
 
 // evaluateLog pieces
 // ratio_mode_only: only the derivative rows of the determinants whose last

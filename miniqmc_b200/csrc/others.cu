@@ -1318,8 +1318,8 @@ cudaError_t launch_det_engine(bool fp32, int op, const DevWalkers& dw, int row, 
     return cudaErrorInvalidValue;
   if (fp32)
   {
-    const size_t bytes = tc && tc_flush_smem_bytes() > flush_smem_bytes<float>() ? tc_flush_smem_bytes()
-                                                                                 : flush_smem_bytes<float>();
+    const size_t bytes = tc && tc_flush_smem_bytes(max_k) > flush_smem_bytes<float>() ? tc_flush_smem_bytes(max_k)
+                                                                                      : flush_smem_bytes<float>();
     allow_smem(det_engine_kernel<float>, bytes);
     det_engine_kernel<float><<<1, 256, bytes, st>>>(dw, op, row, tc ? 1 : 0);
   }

@@ -244,36 +244,71 @@ static void launch_sweep_t(bool j3, bool epoch, size_t bytes, const SweepTask* d
   }
 }
 
+// dynamic shared memory of a sweep launch: the active spin's Binv, then the
+// flush scratch or, between flushes, the J2 candidate lists and the epoch's
+// stencil weights (or the J3 move scratch); the tensor-core flush tiles
+// overlay the cached Binv
+template <typename T> static size_t sweep_smem_bytes(int threads, int max_k, bool tc, bool j3, bool epoch)
+{
+  const size_t moves = j2_list_bytes() + (epoch ? epoch_smem_bytes<T>() : 0);
+  size_t bytes       = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<T>(threads, max_k), moves);
+  if (tc && tc_flush_smem_bytes(max_k) > bytes)
+    bytes = tc_flush_smem_bytes(max_k);
+  if (j3)
+    bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<T>));
+  return bytes;
+}
+
 cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int total_blocks, int n_substeps,
                          double accept, int threads, int max_npad, int max_k, cudaStream_t st, bool tc, bool j3,
                          bool epoch)
 {
   (void)max_npad;
-  if (max_k > MAXK || (tc && (!fp32 || threads < 128))) // a task flushes on the tensor cores only if its k <= 32
+  if (max_k > MAXK || (tc && (!fp32 || threads < 128)))
     return cudaErrorInvalidValue;
   epoch = epoch && !j3;
-  // dynamic shared memory between flushes: the J2 candidate lists, then the
-  // epoch's stencil weights
+  if (fp32)
+    launch_sweep_t<float>(j3, epoch, sweep_smem_bytes<float>(threads, max_k, tc, j3, epoch), d_tasks, n_tasks,
+                          total_blocks, n_substeps, accept, threads, st, tc ? 1 : 0);
+  else
+    launch_sweep_t<double>(j3, epoch, sweep_smem_bytes<double>(threads, max_k, false, j3, epoch), d_tasks, n_tasks,
+                           total_blocks, n_substeps, accept, threads, st, 0);
+  return cudaGetLastError();
+}
+
+// CTAs per SM from the kernel's registers and static shared memory and the
+// launch's block size and dynamic shared memory (registers are allocated
+// per warp in units of 256; every CTA also reserves 1 KB of shared memory)
+template <typename T, bool HAS_J3, bool EPOCH> static int occupancy_t(int threads, size_t bytes)
+{
+  set_smem_attr<T, HAS_J3, EPOCH>(bytes);
+  cudaFuncAttributes fa;
+  cudaDeviceProp p;
+  int dev = 0;
+  if (cudaFuncGetAttributes(&fa, sweep_kernel<T, HAS_J3, EPOCH>) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaGetDeviceProperties(&p, dev) != cudaSuccess)
+    return -1;
+  const int warps     = (threads + 31) / 32;
+  const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;
+  const int by_regs   = regs_warp ? p.regsPerMultiprocessor / (warps * regs_warp) : p.maxBlocksPerMultiProcessor;
+  const size_t cta    = fa.sharedSizeBytes + bytes + p.reservedSharedMemPerBlock;
+  const int by_smem   = (int)(p.sharedMemPerMultiprocessor / cta);
+  const int by_warps  = p.maxThreadsPerMultiProcessor / (warps * 32);
+  return std::min(std::min(by_regs, by_smem), std::min(by_warps, p.maxBlocksPerMultiProcessor));
+}
+
+int sweep_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool epoch)
+{
+  epoch = epoch && !j3;
   if (fp32)
   {
-    const size_t moves = j2_list_bytes() + (epoch ? epoch_smem_bytes<float>() : 0);
-    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<float>(threads, max_k), moves);
-    if (tc && tc_flush_smem_bytes() > bytes)
-      bytes = tc_flush_smem_bytes(); // the tiles overlay the cached Binv
-    if (j3)
-      bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<float>));
-    launch_sweep_t<float>(j3, epoch, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st,
-                          tc ? 1 : 0);
+    const size_t b = sweep_smem_bytes<float>(threads, max_k, tc, j3, epoch);
+    return j3 ? occupancy_t<float, true, false>(threads, b)
+              : epoch ? occupancy_t<float, false, true>(threads, b) : occupancy_t<float, false, false>(threads, b);
   }
-  else
-  {
-    const size_t moves = j2_list_bytes() + (epoch ? epoch_smem_bytes<double>() : 0);
-    size_t bytes = bsm_bytes(max_k) + std::max(flush_smem_bytes_for<double>(threads, max_k), moves);
-    if (j3)
-      bytes = std::max(bytes, bsm_bytes(max_k) + sizeof(J3Smem<double>));
-    launch_sweep_t<double>(j3, epoch, bytes, d_tasks, n_tasks, total_blocks, n_substeps, accept, threads, st, 0);
-  }
-  return cudaGetLastError();
+  const size_t b = sweep_smem_bytes<double>(threads, max_k, false, j3, epoch);
+  return j3 ? occupancy_t<double, true, false>(threads, b)
+            : epoch ? occupancy_t<double, false, true>(threads, b) : occupancy_t<double, false, false>(threads, b);
 }
 
 } // namespace qmc

@@ -10,6 +10,8 @@ namespace qmc
 // default limit of a bounded wait, in SM cycles (about one second); a batch
 // may set its own (qmc_walkers_set_wait_limit)
 constexpr long long kTcWaitCycles = 2000000000LL;
+// largest padded delay rank of the tensor-core Woodbury flush
+constexpr int TC_KD = 64;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {

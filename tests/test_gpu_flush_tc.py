@@ -34,11 +34,11 @@ def _engines(n, delay, rng):
 
 
 @pytest.mark.parametrize('n,delay,dc', [(256, 32, 32), (200, 32, 20), (300, 16, 11), (768, 32, 32),
-                                        (130, 16, 16)])
+                                        (130, 16, 16), (768, 64, 64), (300, 64, 37), (200, 48, 48)])
 def test_engine_flush(n, delay, dc):
     """dc = delay: the flush inside acceptRow; dc < delay: updateInvMat of a
-    partial delay (Kd = 16 or 32 with zero-padded delays); n not a multiple
-    of 128: masked rows of the last 128-row block."""
+    partial delay (Kd = dc rounded up to 16, zero-padded delays, 16 to 64);
+    n not a multiple of 128: masked rows of the last 128-row block."""
     rng = np.random.default_rng(n + dc)
     tc, simt, o = _engines(n, delay, rng)
     for r in rng.choice(n, size=dc, replace=False):
@@ -63,11 +63,11 @@ def test_engine_flush_rejects_where_not_applicable():
         H.product().call('detengine_set_tensor_cores', e.h, 1)
 
 
-def _nio128_pair(precision, tensor_cores=None):
+def _nio128_pair(precision, tensor_cores=None, delay=32):
     """NiO 4x4x2 (768 orbitals per spin: 192 threads per walker), delay 32,
     on a 24x24x12 grid: the periodic spline space (nx ny nz functions) must
     be well above 768 for the Slater matrices to be regular."""
-    gw, ow = H.make_pair(precision=precision, walkers=1, delay=32, tiling=(4, 4, 2), grid=(24, 24, 12),
+    gw, ow = H.make_pair(precision=precision, walkers=1, delay=delay, tiling=(4, 4, 2), grid=(24, 24, 12),
                          jastrow='synthetic')
     if tensor_cores is not None:
         H.product().call('walkers_set_tensor_cores', gw.h, 1 if tensor_cores else 0)
@@ -179,6 +179,31 @@ def _phase_times(gw):
     H.product().call('walkers_phase_times', gw.h, ms.ctypes.data_as(capi.PD), C.byref(n))
     return n.value, ms[:n.value]
 
+
+
+def test_sweep_nio128_tensor_core_flush_delay64():
+    """Delay rank 64 (the largest of the configuration's {16, 32, 64}) with
+    its flushes on the tensor cores: GEMM1 with N = 64, GEMM2 with K = 64,
+    96 KB of tiles.  Same case and checks as delay 32: the accept sequence
+    exact, the log-ratio errors against the oracle bounded and within 4x of
+    the CUDA-core flush on the same streams."""
+    seeds = H.oracle_primes(1)
+    g_tc, ow = _nio128_pair(capi.PREC_MIXED, True, delay=64)
+    g_simt, _ = _nio128_pair(capi.PREC_MIXED, False, delay=64)
+    for w in (g_tc, g_simt, ow):
+        w.evaluate_log()
+    ur, de = H.host_streams(seeds, g_tc.N, 1, 1)
+    r_tc = g_tc.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    r_simt = g_simt.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    r_o = ow.sweep(1, 1, 0.5, ur=ur, delta=de, trace=True)
+    assert np.array_equal(r_tc['trace'][..., 7], r_o['trace'][..., 7])
+    lt, ls = _logratio_err(r_tc, r_o), _logratio_err(r_simt, r_o)
+    print('NiO-128 24x24x12 delay 64: tc median %.3e p99 %.3e logpsi %.3e; simt median %.3e p99 %.3e' % (
+        np.median(lt), np.percentile(lt, 99), elem_rel(r_tc['logpsi'], r_o['logpsi']).max(), np.median(ls),
+        np.percentile(ls, 99)))
+    assert np.median(lt) < 3e-3, np.median(lt)
+    assert np.median(lt) < 4 * max(np.median(ls), 1e-7), (np.median(lt), np.median(ls))
+    assert elem_rel(r_tc['logpsi'], r_o['logpsi']).max() < 1e-4
 
 @pytest.mark.parametrize('tensor_cores', [True, False])
 def test_phase_timers(tensor_cores):
