@@ -67,9 +67,10 @@ struct MoveSmem
   int accept, dc, ok;
   int eG; // moves in the current epoch (do_epoch)
   // tensor-core flush state: commit barriers (GEMM1 stages 0/1, GEMM2
-  // accumulators 0/1, and the drain barrier of an aborted CTA), their phase
-  // bits, the TMEM base, the abort flag and the limit of each bounded wait
-  unsigned long long tc_bar[5];
+  // accumulators 0/1, and the drain barrier of an aborted CTA), the GEMM2 B
+  // stages' bulk-copy barriers (5, 6), their phase bits, the TMEM base, the
+  // abort flag and the limit of each bounded wait
+  unsigned long long tc_bar[7];
   unsigned tc_phase, tc_tmem;
   int tc_on, tc_abort;
   long long tc_limit;
@@ -187,7 +188,7 @@ template <typename T> __device__ WV<T> make_wv(const DevWalkers& d, int w)
   v.d2psiV    = (T*)d.d2psiV + (size_t)w * d.npad;
   v.U2        = (T*)d.U2 + (size_t)w * kn;
   v.tm        = (T*)d.tm + (size_t)w * d.n * d.k;
-  v.tci       = d.tci ? d.tci + (size_t)w * 2 * 32 * d.npad : nullptr;
+  v.tci       = d.tci ? d.tci + (size_t)w * 2 * (d.k <= 32 ? 32 : 64) * d.npad : nullptr; // tc_image_floats
   v.lu        = d.lu ? d.lu + (size_t)w * 2 * nn : nullptr;
   v.ms        = d.ms + w;
   v.G         = d.G + (size_t)w * d.N * 3;

@@ -125,7 +125,7 @@ struct DevWalkers
   void* d2psiV;    // [W][npad]
   void* U2;        // [W][k][npad] flush scratch (Binv V)
   void* tm;        // [W][n][k] flush scratch (Ainv U^T - E)
-  float* tci;      // [W][npad/32][2][32][32] tensor-core flush: (Binv V)^T hi/lo tiles, or null
+  float* tci;      // [W][npad/32][2][32][32 or 64 (k > 32)] tensor-core flush: (Binv V)^T hi/lo tiles, or null
   double* lu;      // [W][2][n][npad] FP64 Slater matrices for the LU (lazily)
   MoveState* ms;   // [W]
   double* G;       // [W][N][3]

@@ -63,12 +63,12 @@ def test_engine_flush_rejects_where_not_applicable():
         H.product().call('detengine_set_tensor_cores', e.h, 1)
 
 
-def _nio128_pair(precision, tensor_cores=None, delay=32):
+def _nio128_pair(precision, tensor_cores=None, delay=32, walkers=1):
     """NiO 4x4x2 (768 orbitals per spin: 192 threads per walker), delay 32,
     on a 24x24x12 grid: the periodic spline space (nx ny nz functions) must
     be well above 768 for the Slater matrices to be regular."""
-    gw, ow = H.make_pair(precision=precision, walkers=1, delay=delay, tiling=(4, 4, 2), grid=(24, 24, 12),
-                         jastrow='synthetic')
+    gw, ow = H.make_pair(precision=precision, walkers=walkers, delay=delay, tiling=(4, 4, 2), grid=(24, 24, 12),
+                         jastrow='synthetic', seeds=H.oracle_primes(walkers))
     if tensor_cores is not None:
         H.product().call('walkers_set_tensor_cores', gw.h, 1 if tensor_cores else 0)
     return gw, ow
@@ -184,12 +184,13 @@ def _phase_times(gw):
 def test_sweep_nio128_tensor_core_flush_delay64():
     """Delay rank 64 (the largest of the configuration's {16, 32, 64}) with
     its flushes on the tensor cores: GEMM1 with N = 64, GEMM2 with K = 64,
-    96 KB of tiles.  Same case and checks as delay 32: the accept sequence
-    exact, the log-ratio errors against the oracle bounded and within 4x of
-    the CUDA-core flush on the same streams."""
-    seeds = H.oracle_primes(1)
-    g_tc, ow = _nio128_pair(capi.PREC_MIXED, True, delay=64)
-    g_simt, _ = _nio128_pair(capi.PREC_MIXED, False, delay=64)
+    96 KB of tiles, a 64-wide image per walker.  Same case and checks as
+    delay 32, on three walkers: the accept sequence exact, the log-ratio
+    errors against the oracle bounded and within 4x of the CUDA-core flush
+    on the same streams."""
+    seeds = H.oracle_primes(3)
+    g_tc, ow = _nio128_pair(capi.PREC_MIXED, True, delay=64, walkers=3)
+    g_simt, _ = _nio128_pair(capi.PREC_MIXED, False, delay=64, walkers=3)
     for w in (g_tc, g_simt, ow):
         w.evaluate_log()
     ur, de = H.host_streams(seeds, g_tc.N, 1, 1)
