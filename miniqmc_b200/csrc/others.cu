@@ -547,9 +547,12 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
 #endif
 constexpr int GJB_B = 32;      // panel width
 constexpr int GJB_FS = GJB_B + 1; // padded panel row (conflict-free row-per-thread access)
+// padded row of a chunk's pivot rows: the update's B fragments (row k + lane % 4,
+// column lane / 4 + 8 t) then fall in distinct banks across each half-warp
+constexpr int GJB_RS = 36;
 __host__ __device__ constexpr size_t gjb_smem_bytes(int n)
 {
-  return (((size_t)n * GJB_FS + 1) & ~(size_t)1) * sizeof(double) + (size_t)2 * GJB_B * 32 * sizeof(double) +
+  return (((size_t)n * GJB_FS + 1) & ~(size_t)1) * sizeof(double) + (size_t)2 * GJB_B * GJB_RS * sizeof(double) +
       (size_t)2 * n * sizeof(int);
 }
 constexpr size_t GJB_MAX_SMEM = 226 * 1024;
@@ -559,8 +562,8 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
   extern __shared__ __align__(16) unsigned char dyn[];
   const int n = dw.n, npad = dw.npad;
   double* F = reinterpret_cast<double*>(dyn);   // [n][GJB_FS] panel
-  double* R = F + (((size_t)n * GJB_FS + 1) & ~(size_t)1); // [2][GJB_B][32] pivot rows of a column chunk (16-byte aligned)
-  int* piv  = reinterpret_cast<int*>(R + 2 * GJB_B * 32); // [n] pivot row of each column
+  double* R = F + (((size_t)n * GJB_FS + 1) & ~(size_t)1); // [2][GJB_B][GJB_RS] pivot rows of a column chunk (16-byte aligned)
+  int* piv  = reinterpret_cast<int*>(R + 2 * GJB_B * GJB_RS); // [n] pivot row of each column
   int* pinv = piv + n;                                 // [n] column pivoted by each row, -1 while free
   __shared__ double s_val[32];
   __shared__ int s_idx[32];
@@ -689,12 +692,12 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
       if (j0 == c0)
         continue;
       const int jw = min(32, n - j0);
-      double* Rb   = R + rbuf * GJB_B * 32;
+      double* Rb   = R + rbuf * GJB_B * GJB_RS;
       rbuf ^= 1;
       for (int idx = tid; idx < GJB_B * 32; idx += NT)
       {
         const int k = idx >> 5, jj = idx & 31;
-        Rb[idx]     = (k < bw && jj < jw) ? M[(size_t)piv[c0 + k] * npad + j0 + jj] : 0.0;
+        Rb[k * GJB_RS + jj] = (k < bw && jj < jw) ? M[(size_t)piv[c0 + k] * npad + j0 + jj] : 0.0;
       }
       __syncthreads();
 #if GJB_DMMA
@@ -702,16 +705,22 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
       // each warp takes three 8-row groups at a time and the chunk's four
       // 8-column tiles; fragments: A (8 x 4 of the panel) one element per
       // lane at (lane / 4, lane % 4), B (4 x 8 of the pivot rows) at
-      // (lane % 4, lane / 4), C (8 x 8) two at (lane / 4, 2 (lane % 4) + e)
+      // (lane % 4, lane / 4), C (8 x 8) two at (lane / 4, 2 (lane % 4) + e).
+      // Group g holds rows 32 (g / 4) + g % 4 + 4 r (r = 0..7): with the
+      // panel's row stride of 33 doubles the A fragments of a half-warp then
+      // fall in distinct banks (consecutive rows put lane % 4 and lane / 4 on
+      // the same banks)
       {
         const int qr = lane >> 2, qc = lane & 3;
-        for (int gb = wid * 3; gb * 8 < n; gb += nw * 3)
+        const int ngroups = (n + 31) / 32 * 4;
+        auto grow = [&](int g) { return (g >> 2) * 32 + (g & 3) + 4 * qr; };
+        for (int gb = wid * 3; gb < ngroups; gb += nw * 3)
         {
           double acc[3][4][2];
 #pragma unroll
           for (int u = 0; u < 3; ++u)
           {
-            const int i     = (gb + u) * 8 + qr;
+            const int i     = gb + u < ngroups ? grow(gb + u) : n;
             const int c     = i < n ? pinv[i] : c0;
             const bool zero = i >= n || (c >= c0 && c < c0 + bw);
             const double* mi = M + (size_t)(i < n ? i : 0) * npad + j0;
@@ -730,11 +739,11 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
             double b[4];
 #pragma unroll
             for (int t = 0; t < 4; ++t)
-              b[t] = Rb[(k + qc) * 32 + t * 8 + qr];
+              b[t] = Rb[(k + qc) * GJB_RS + t * 8 + qr];
 #pragma unroll
             for (int u = 0; u < 3; ++u)
             {
-              const double a = F[min((gb + u) * 8 + qr, n - 1) * GJB_FS + k + qc];
+              const double a = F[min(grow(gb + u), n - 1) * GJB_FS + k + qc];
 #pragma unroll
               for (int t = 0; t < 4; ++t)
                 asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -745,7 +754,7 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
 #pragma unroll
           for (int u = 0; u < 3; ++u)
           {
-            const int i = (gb + u) * 8 + qr;
+            const int i = gb + u < ngroups ? grow(gb + u) : n;
             if (i >= n)
               continue;
             double* mi = M + (size_t)i * npad + j0;
@@ -787,8 +796,8 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
 #pragma unroll 4
         for (int k = 0; k < GJB_B; ++k)
         {
-          const double2 ra = *reinterpret_cast<const double2*>(Rb + k * 32 + ja);
-          const double2 rb = *reinterpret_cast<const double2*>(Rb + k * 32 + jb);
+          const double2 ra = *reinterpret_cast<const double2*>(Rb + k * GJB_RS + ja);
+          const double2 rb = *reinterpret_cast<const double2*>(Rb + k * GJB_RS + jb);
 #pragma unroll
           for (int u = 0; u < 4; ++u)
           {

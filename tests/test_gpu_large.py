@@ -1,5 +1,5 @@
 """The largest system the tests run: NiO 4x4x4 of the 4-atom cell (256 atoms,
-3072 electrons, 1536 orbitals per spin).  Past 790 orbitals the FP64
+3072 electrons, 1536 orbitals per spin).  Past 782 orbitals the FP64
 inverse's panel no longer fits one SM's shared memory, so evaluateLog and
 the refresh take the one-pivot-per-pass Gauss-Jordan kernel; the
 tensor-core flush runs twelve 128-row blocks; each thread of a 256-thread
