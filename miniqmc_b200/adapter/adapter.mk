@@ -2,6 +2,7 @@
 # the adapter classes (qmcgpu_adapter.hpp):
 #   ../bin/ref_miniqmc            Drivers/miniqmc.cpp
 #   ../bin/ref_miniqmc_sync_move  Drivers/miniqmc_sync_move.cpp
+#   ../bin/check_spo_gpu          the reference's SPO set against SPOSetGpu
 # Each binary is the driver's source and the reference's particle, SPO
 # builder and utility sources (the qmcutil / qmcbase source lists of
 # src/CMakeLists.txt), compiled with the reference's GNU Release flags
@@ -36,7 +37,7 @@ REF_SRCS := Particle/VirtualParticleSet.cpp Particle/ParticleSet.cpp Particle/Pa
 REF_OBJS := $(addprefix $(OBJ)/ref/,$(REF_SRCS:.cpp=.o))
 ADAPTER_OBJS := $(OBJ)/qmcgpu_adapter.o $(OBJ)/qmcgpu_wavefunction.o
 LIBS := -L$(PKG) -lqmcgpu -Wl,-rpath,'$$ORIGIN/..' -fopenmp -lm
-BINS := $(BIN)/ref_miniqmc $(BIN)/ref_miniqmc_sync_move
+BINS := $(BIN)/ref_miniqmc $(BIN)/ref_miniqmc_sync_move $(BIN)/check_spo_gpu
 
 ifeq ($(wildcard $(REF)/Drivers/miniqmc.cpp),)
 all:
@@ -56,6 +57,10 @@ $(OBJ)/drivers/%.o: $(REF)/Drivers/%.cpp
 $(OBJ)/%.o: $(HERE)%.cpp $(HERE)qmcgpu_adapter.hpp $(ROOT)/include/qmcgpu.h
 	@mkdir -p $(dir $@)
 	$(REF_CXX) $(ADAPTER_FLAGS) -c -o $@ $<
+
+$(BIN)/check_spo_gpu: $(OBJ)/check_spo_gpu.o $(REF_OBJS) $(ADAPTER_OBJS) $(PKG)/libqmcgpu.so
+	@mkdir -p $(BIN)
+	$(REF_CXX) -o $@ $< $(REF_OBJS) $(ADAPTER_OBJS) $(LIBS)
 
 $(BIN)/ref_%: $(OBJ)/drivers/%.o $(REF_OBJS) $(ADAPTER_OBJS) $(PKG)/libqmcgpu.so
 	@mkdir -p $(BIN)

@@ -60,3 +60,8 @@ def test_driver_without_a_device_stops(tmp_path):
     r = subprocess.run([R.MINIQMC, '-g', '1 1 1', '-m', '0.5', '-w', '1', '-n', '1'], capture_output=True, text=True,
                        timeout=300, cwd=str(tmp_path), env=dict(os.environ, OMP_NUM_THREADS='1'))
     assert r.returncode == 1 and 'QMC_ERR_NODEVICE' in r.stderr
+
+
+@R.needs_binaries
+def test_reference_sposet_over_oracle(tmp_path, shim_env):
+    R.check_sposet(tmp_path, ['-g', '1 1 1', '-m', '0.5', '-a', '48', '-n', '8'], shim_env)

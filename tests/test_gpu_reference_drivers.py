@@ -2,7 +2,8 @@
 classes (miniqmc_b200/adapter/): Drivers/miniqmc.cpp (one walker per mover,
 the per-walker WaveFunction verbs, NLPP through WaveFunction::ratio) and
 Drivers/miniqmc_sync_move.cpp (flex_ verbs over a batch of movers, NLPP
-through WaveFunction::evaluateRatios).  Each walker's counters and last log
+through WaveFunction::evaluateRatios); and the reference's SPO set against
+the SPOSet adapter (check_spo_gpu).  Each walker's counters and last log
 value (QMCGPU_ADAPTER_REPORT) are compared with the oracle driven through
 the C ABI over the same system, random streams and NLPP spheres.
 
@@ -22,10 +23,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, 'miniqmc_b200', 'bin')
 MINIQMC = os.path.join(BIN, 'ref_miniqmc')
 SYNC = os.path.join(BIN, 'ref_miniqmc_sync_move')
+CHECK_SPO = os.path.join(BIN, 'check_spo_gpu')
 PRIMES = [3, 5, 7, 11]  # PrimeNumberSet<uint32_t> from 3
 QUIRKS = 3  # the reference's 32-atom cell at -g "1 1 1": ions in lattice units, one species group
 
-needs_binaries = pytest.mark.skipif(not (os.path.exists(MINIQMC) and os.path.exists(SYNC)),
+needs_binaries = pytest.mark.skipif(not all(os.path.exists(b) for b in (MINIQMC, SYNC, CHECK_SPO)),
                                     reason='reference drivers on the device not built (no reference tree)')
 
 
@@ -202,3 +204,23 @@ def check_reference_table(tmp_path, extra_env=None):
 @pytest.mark.gpu
 def test_reference_table_is_singular_and_the_run_goes_on(tmp_path):
     check_reference_table(tmp_path)
+
+
+def check_sposet(tmp_path, args, extra_env=None):
+    """The reference's own SPO set (its builder, fill and tiles) against the
+    SPOSet adapter on the device copy of its table (check_spo_gpu)."""
+    env = dict(os.environ, OMP_NUM_THREADS='1', **(extra_env or {}))
+    env.pop('QMCGPU_SPO_FILL', None)
+    r = subprocess.run([CHECK_SPO, *args], capture_output=True, text=True, timeout=600, env=env, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert 'All checks passed for spo on the device' in r.stdout
+    return r.stdout
+
+
+@needs_binaries
+@pytest.mark.gpu
+@pytest.mark.parametrize('args,precision', [(['-g', '1 1 1', '-m', '0.5', '-a', '48'], 'fp64'),
+                                            (['-g', '1 1 1', '-m', '0.5'], 'fp64'),
+                                            (['-g', '2 1 1', '-m', '0.5', '-a', '96'], 'mixed')])
+def test_reference_sposet_on_the_device(tmp_path, args, precision):
+    print(check_sposet(tmp_path, args + ['-n', '24'], {'QMCGPU_PRECISION': precision}))
