@@ -67,10 +67,9 @@ struct MoveSmem
   int accept, dc, ok;
   int eG; // moves in the current epoch (do_epoch)
   // tensor-core flush state: commit barriers (GEMM1 stages 0/1, GEMM2
-  // accumulators 0/1, and the drain barrier of an aborted CTA), the GEMM2 B
-  // stages' bulk-copy barriers (5, 6), their phase bits, the TMEM base, the
-  // abort flag and the limit of each bounded wait
-  unsigned long long tc_bar[7];
+  // accumulators 0/1, and the drain barrier of an aborted CTA), their phase
+  // bits, the TMEM base, the abort flag and the limit of each bounded wait
+  unsigned long long tc_bar[5];
   unsigned tc_phase, tc_tmem;
   int tc_on, tc_abort;
   long long tc_limit;

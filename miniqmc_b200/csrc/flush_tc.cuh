@@ -79,7 +79,7 @@ __device__ __forceinline__ void tc_begin(MoveSmem& m, int on, long long limit)
       tc_alloc(&m.tc_tmem, TC_COLS);
     if (threadIdx.x == 0)
     {
-      for (int b = 0; b < 7; ++b)
+      for (int b = 0; b < 5; ++b)
         mbar_init(&m.tc_bar[b], 1);
       mbar_fence_init();
     }
@@ -202,7 +202,6 @@ static __device__ __noinline__ void flush_tc_body(const WV<float>& wv, MoveSmem&
   }
   // the tiles overlay the cached Binv: keep the other spin's copy if cached
   double* keep = (wv.bsm && wv.bsm_spin != s) ? wv.Binv + (size_t)wv.bsm_spin * k * k : nullptr;
-  fence_async_global(); // the image is read by bulk copies (the async proxy)
   __syncthreads();
   phase_mark(m, PH_FLUSH_U2);
   if (keep)
@@ -322,29 +321,14 @@ static __device__ __noinline__ void flush_tc_body(const WV<float>& wv, MoveSmem&
     tc_fence_before();
 
     // ------------------------------------------ GEMM2 and the Ainv update
-    // B tile t (U2^T hi/lo, 8 KB of the per-walker image at Kd = 32) into
-    // stage st: one bulk copy (the TMA engine, untiled) issued by thread 0 on
-    // the stage's barrier (tc_bar[5 + st]); `pend` (thread 0) marks the
-    // stages whose copy has not been waited for yet
-    const uint32_t b2bytes = (uint32_t)(2 * TC_BN2 * Kd * sizeof(float));
-    uint32_t pend          = 0;
+    // B tile t (U2^T hi/lo, 8 KB of the per-walker image) into stage st:
+    // 16-byte cp.async copies, no registers held while they land
     auto load2 = [&](int t, int st) {
-      mbar_arrive_expect_tx(&m.tc_bar[5 + st], b2bytes);
-      bulk_g2s(b2 + st * 2 * TC_BN2 * Kd, img + (size_t)t * 2 * 32 * Kd, b2bytes, &m.tc_bar[5 + st]);
-      pend |= 1u << st;
-    };
-    // thread 0: stage st's tile has landed (bounded; false after a timeout,
-    // the copy then stays pending for the drain below)
-    auto landed = [&](int st) {
-      if (mbar_wait(&m.tc_bar[5 + st], (ph >> (5 + st)) & 1u, m.tc_limit))
-      {
-        ph ^= 1u << (5 + st);
-        pend &= ~(1u << st);
-        return true;
-      }
-      m.tc_abort = 1;
-      atomicOr(wv.status, DEV_ERR_TIMEOUT);
-      return false;
+      const uint4* src = reinterpret_cast<const uint4*>(img + (size_t)t * 2 * 32 * Kd);
+      uint4* dst       = reinterpret_cast<uint4*>(b2 + st * 2 * TC_BN2 * Kd);
+      for (int i = tid; i < 2 * TC_BN2 * Kd / 4; i += NT)
+        tc_cp_async16(dst + i, src + i);
+      tc_cp_async_commit();
     };
     auto mma2 = [&](int t) {
       float* Bs = b2 + (t & 1) * 2 * TC_BN2 * Kd;
@@ -362,32 +346,30 @@ static __device__ __noinline__ void flush_tc_body(const WV<float>& wv, MoveSmem&
       }
       tc_commit(&m.tc_bar[2 + (t & 1)]);
     };
-    // Per column block t: the MMAs of block t+1 are issued first (once its
-    // tile has landed), then those of block t are waited for, block t+2's B
-    // tile starts into the stage they have just released, and the Ainv
-    // update of block t runs while block t+1 multiplies.  B tiles are thus
-    // copied two blocks ahead.
-    if (tid == 0)
-    {
-      load2(0, 0);
-      if (T2 > 1)
-        load2(1, 1);
-    }
+    // Per column block t: the MMAs of block t+1 are issued first, then those
+    // of block t are waited for, block t+2's B tile starts into the stage
+    // they have just released, and the Ainv update of block t runs while
+    // block t+1 multiplies.  B tiles are thus copied two blocks ahead.
+    load2(0, 0);
+    if (T2 > 1)
+      load2(1, 1);
     for (int t = 0; t < T2; ++t)
     {
-      __syncthreads(); // the update of block t-1 has read its accumulator
+      tc_cp_async_wait_all(); // this thread's copies of block t+1's tile (and block 0's)
+      fence_async_smem();
+      __syncthreads();
       if (m.tc_abort)
         break;
       if (tid == 0)
       {
-        if (t == 0 && landed(0))
+        if (t == 0)
           mma2(0);
-        if (t + 1 < T2 && !m.tc_abort && landed((t + 1) & 1))
+        if (t + 1 < T2)
           mma2(t + 1);
       }
       tc_wait(m, 2 + (t & 1), ph, wv);
       tc_fence_after();
-      if (tid == 0 && t + 2 < T2 && !m.tc_abort)
+      if (t + 2 < T2)
         load2(t + 2, t & 1); // its stage was read by the MMAs of block t, now complete
       if (warp < 4)
       {
@@ -417,16 +399,7 @@ static __device__ __noinline__ void flush_tc_body(const WV<float>& wv, MoveSmem&
       }
       tc_fence_before();
     }
-    // a copy still in flight after an abort lands before its stage is reused
-    // (bounded by the default limit, not the batch's, which may be tiny)
-    if (tid == 0)
-      for (int st = 0; st < 2; ++st)
-        if (pend & (1u << st))
-        {
-          mbar_wait(&m.tc_bar[5 + st], (ph >> (5 + st)) & 1u, kTcWaitCycles);
-          ph ^= 1u << (5 + st);
-          pend &= ~(1u << st);
-        }
+    tc_cp_async_wait_all(); // nothing in flight if the loop was left early
     __syncthreads();
     phase_mark(m, PH_FLUSH);
   }
@@ -513,7 +486,6 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
   }
   // the tiles overlay the cached Binv: keep the other spin's copy if cached
   double* keep = (wv.bsm && wv.bsm_spin != s) ? wv.Binv + (size_t)wv.bsm_spin * k * k : nullptr;
-  fence_async_global(); // the image is read by bulk copies (the async proxy)
   __syncthreads();
   phase_mark(m, PH_FLUSH_U2);
   if (keep)
@@ -624,29 +596,14 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
     tc_fence_before();
 
     // ------------------------------------------ GEMM2 and the Ainv update
-    // B tile t (U2^T hi/lo, 8 KB of the per-walker image at Kd = 32) into
-    // stage st: one bulk copy (the TMA engine, untiled) issued by thread 0 on
-    // the stage's barrier (tc_bar[5 + st]); `pend` (thread 0) marks the
-    // stages whose copy has not been waited for yet
-    const uint32_t b2bytes = (uint32_t)(2 * TC_BN2 * Kd * sizeof(float));
-    uint32_t pend          = 0;
+    // B tile t (U2^T hi/lo, 8 KB of the per-walker image) into stage st:
+    // 16-byte cp.async copies, no registers held while they land
     auto load2 = [&](int t, int st) {
-      mbar_arrive_expect_tx(&m.tc_bar[5 + st], b2bytes);
-      bulk_g2s(b2 + st * 2 * TC_BN2 * Kd, img + (size_t)t * 2 * 32 * Kd, b2bytes, &m.tc_bar[5 + st]);
-      pend |= 1u << st;
-    };
-    // thread 0: stage st's tile has landed (bounded; false after a timeout,
-    // the copy then stays pending for the drain below)
-    auto landed = [&](int st) {
-      if (mbar_wait(&m.tc_bar[5 + st], (ph >> (5 + st)) & 1u, m.tc_limit))
-      {
-        ph ^= 1u << (5 + st);
-        pend &= ~(1u << st);
-        return true;
-      }
-      m.tc_abort = 1;
-      atomicOr(wv.status, DEV_ERR_TIMEOUT);
-      return false;
+      const uint4* src = reinterpret_cast<const uint4*>(img + (size_t)t * 2 * 32 * Kd);
+      uint4* dst       = reinterpret_cast<uint4*>(b2 + st * 2 * TC_BN2 * Kd);
+      for (int i = tid; i < 2 * TC_BN2 * Kd / 4; i += NT)
+        tc_cp_async16(dst + i, src + i);
+      tc_cp_async_commit();
     };
     auto mma2 = [&](int t) {
       float* Bs = b2 + (t & 1) * 2 * TC_BN2 * Kd;
@@ -664,32 +621,30 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
       }
       tc_commit(&m.tc_bar[2 + (t & 1)]);
     };
-    // Per column block t: the MMAs of block t+1 are issued first (once its
-    // tile has landed), then those of block t are waited for, block t+2's B
-    // tile starts into the stage they have just released, and the Ainv
-    // update of block t runs while block t+1 multiplies.  B tiles are thus
-    // copied two blocks ahead.
-    if (tid == 0)
-    {
-      load2(0, 0);
-      if (T2 > 1)
-        load2(1, 1);
-    }
+    // Per column block t: the MMAs of block t+1 are issued first, then those
+    // of block t are waited for, block t+2's B tile starts into the stage
+    // they have just released, and the Ainv update of block t runs while
+    // block t+1 multiplies.  B tiles are thus copied two blocks ahead.
+    load2(0, 0);
+    if (T2 > 1)
+      load2(1, 1);
     for (int t = 0; t < T2; ++t)
     {
-      __syncthreads(); // the update of block t-1 has read its accumulator
+      tc_cp_async_wait_all(); // this thread's copies of block t+1's tile (and block 0's)
+      fence_async_smem();
+      __syncthreads();
       if (m.tc_abort)
         break;
       if (tid == 0)
       {
-        if (t == 0 && landed(0))
+        if (t == 0)
           mma2(0);
-        if (t + 1 < T2 && !m.tc_abort && landed((t + 1) & 1))
+        if (t + 1 < T2)
           mma2(t + 1);
       }
       tc_wait(m, 2 + (t & 1), ph, wv);
       tc_fence_after();
-      if (tid == 0 && t + 2 < T2 && !m.tc_abort)
+      if (t + 2 < T2)
         load2(t + 2, t & 1); // its stage was read by the MMAs of block t, now complete
       if (warp < 4)
       {
@@ -719,16 +674,7 @@ static __device__ __noinline__ void flush_tc(const WV<float>& wv, MoveSmem& m, i
       }
       tc_fence_before();
     }
-    // a copy still in flight after an abort lands before its stage is reused
-    // (bounded by the default limit, not the batch's, which may be tiny)
-    if (tid == 0)
-      for (int st = 0; st < 2; ++st)
-        if (pend & (1u << st))
-        {
-          mbar_wait(&m.tc_bar[5 + st], (ph >> (5 + st)) & 1u, kTcWaitCycles);
-          ph ^= 1u << (5 + st);
-          pend &= ~(1u << st);
-        }
+    tc_cp_async_wait_all(); // nothing in flight if the loop was left early
     __syncthreads();
     phase_mark(m, PH_FLUSH);
   }

@@ -52,26 +52,6 @@ __device__ __forceinline__ void tc_cp_async16(void* dst_smem, const void* src)
 __device__ __forceinline__ void tc_cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void tc_cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// one thread: arrive once on `bar` and expect `bytes` of bulk-copy data
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes)
-{
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-// one thread: bulk copy of `bytes` (a multiple of 16; both addresses 16-byte
-// aligned) from global to this CTA's shared memory through the TMA engine,
-// completing on `bar` (no tensor map, no multicast)
-__device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src, uint32_t bytes, unsigned long long* bar)
-{
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst_smem)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-// order this thread's generic-proxy global writes before later async-proxy
-// (bulk copy) reads of them
-__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count)
 {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
