@@ -36,8 +36,9 @@ def test_miniqmc_driver_over_oracle(tmp_path, shim_env, j3):
 
 
 @R.needs_binaries
-def test_sync_move_driver_over_oracle(tmp_path, shim_env):
-    R.check_sync_move_driver(tmp_path, R.EXACT, shim_env)
+@pytest.mark.parametrize('j3', [False, True])
+def test_sync_move_driver_over_oracle(tmp_path, shim_env, j3):
+    R.check_sync_move_driver(tmp_path, R.EXACT, shim_env, j3=j3)
 
 
 @R.needs_binaries

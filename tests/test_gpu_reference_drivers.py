@@ -132,15 +132,16 @@ def test_reference_miniqmc_driver(tmp_path, j3):
     check_miniqmc_driver(tmp_path, j3, DEVICE)
 
 
-def check_sync_move_driver(tmp_path, tol, extra_env=None):
+def check_sync_move_driver(tmp_path, tol, extra_env=None, j3=False):
     """Drivers/miniqmc_sync_move.cpp, 4 movers in 2 batches of 2 (one device
     batch each, one launch per verb), 2 steps, delay 8, NLPP through
-    NonLocalPP::evaluate's virtual particle sets."""
+    NonLocalPP::evaluate's virtual particle sets; with -j the three-body
+    Jastrow in every verb and virtual ratio."""
     steps, k, nw = 2, 8, 2
-    reports, out = run(SYNC, ['-g', '1 1 1', '-m', '0.5', '-w', '4', '-c', str(nw), '-n', str(steps), '-k', str(k)],
-                       str(tmp_path / 'report.jsonl'), 1, extra_env)
+    reports, out = run(SYNC, ['-g', '1 1 1', '-m', '0.5', '-w', '4', '-c', str(nw), '-n', str(steps), '-k', str(k),
+                              *(['-j'] if j3 else [])], str(tmp_path / 'report.jsonl'), 1, extra_env)
     assert 'Diffusion throughput' in out.stdout
-    lib, spec, system = oracle_system((18, 18, 18))
+    lib, spec, system = oracle_system((18, 18, 18), j3)
     N = spec.n_elec
     per = nw + 2 * ((3 * nw + 1) // 2)
     for first in (0, 2):
@@ -179,8 +180,9 @@ def check_sync_move_driver(tmp_path, tol, extra_env=None):
 
 @needs_binaries
 @pytest.mark.gpu
-def test_reference_sync_move_driver(tmp_path):
-    check_sync_move_driver(tmp_path, DEVICE)
+@pytest.mark.parametrize('j3', [False, True])
+def test_reference_sync_move_driver(tmp_path, j3):
+    check_sync_move_driver(tmp_path, DEVICE, j3=j3)
 
 
 def check_reference_table(tmp_path, extra_env=None):
