@@ -724,14 +724,22 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
             const int c     = i < n ? pinv[i] : c0;
             const bool zero = i >= n || (c >= c0 && c < c0 + bw);
             const double* mi = M + (size_t)(i < n ? i : 0) * npad + j0;
+            // a lane's two columns of a tile are adjacent: one 16-byte load
 #pragma unroll
             for (int t = 0; t < 4; ++t)
-#pragma unroll
-              for (int e = 0; e < 2; ++e)
+            {
+              const int col = t * 8 + 2 * qc;
+              if (!zero && col + 1 < jw)
               {
-                const int col = t * 8 + 2 * qc + e;
-                acc[u][t][e]  = (zero || col >= jw) ? 0.0 : mi[col];
+                const double2 v = *reinterpret_cast<const double2*>(mi + col);
+                acc[u][t][0] = v.x, acc[u][t][1] = v.y;
               }
+              else
+              {
+                acc[u][t][0] = (zero || col >= jw) ? 0.0 : mi[col];
+                acc[u][t][1] = 0.0;
+              }
+            }
           }
 #pragma unroll 2
           for (int k = 0; k < GJB_B; k += 4)
@@ -760,10 +768,13 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
             double* mi = M + (size_t)i * npad + j0;
 #pragma unroll
             for (int t = 0; t < 4; ++t)
-#pragma unroll
-              for (int e = 0; e < 2; ++e)
-                if (t * 8 + 2 * qc + e < jw)
-                  mi[t * 8 + 2 * qc + e] = acc[u][t][e];
+            {
+              const int col = t * 8 + 2 * qc;
+              if (col + 1 < jw)
+                *reinterpret_cast<double2*>(mi + col) = make_double2(acc[u][t][0], acc[u][t][1]);
+              else if (col < jw)
+                mi[col] = acc[u][t][0];
+            }
           }
         }
       }
