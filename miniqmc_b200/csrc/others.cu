@@ -428,7 +428,8 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
     int bi    = n;
     for (int i = k + tid; i < n; i += NT)
     {
-      const double v = fabs(M[(size_t)i * npad + k]);
+      // a NaN entry competes as 0: the pivot is then always a row < n
+      const double v = fmax(fabs(M[(size_t)i * npad + k]), 0.0);
       if (v > bv)
         bv = v, bi = i;
     }
@@ -463,11 +464,12 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
       }
     __syncthreads();
     const double piv = M[(size_t)k * npad + k];
+    const bool zero  = !(fabs(piv) > 0.0); // a NaN pivot counts as zero
     if (tid == 0)
     {
       if (p != k)
         s_sign = -s_sign;
-      if (piv == 0.0)
+      if (zero)
         s_sing = 1;
       else
       {
@@ -476,7 +478,7 @@ template <typename T> __global__ void __launch_bounds__(512) gj_inverse_kernel(D
           s_sign = -s_sign;
       }
     }
-    if (piv == 0.0)
+    if (zero)
     {
       __syncthreads();
       continue;
@@ -629,7 +631,9 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
       for (int i = tid; i < n; i += NT)
         if (pinv[i] < 0)
         {
-          const double v = fabs(F[i * GJB_FS + kk]);
+          // a NaN entry competes as 0: some free row is always taken, so
+          // piv and pinv end as full permutations of 0..n-1
+          const double v = fmax(fabs(F[i * GJB_FS + kk]), 0.0);
           if (v > bv)
             bv = v, bi = i;
         }
@@ -845,15 +849,31 @@ template <typename T> __global__ void __launch_bounds__(512, 1) gj_blocked_kerne
     }
     __syncthreads();
   }
-  // psiM[i][j] = A^{-1}[j][i] = M[piv[j]][pinv[i]]
-  T* out = wv.ainv(s);
-  for (int i = wid; i < n; i += nw)
+  // psiM[i][j] = A^{-1}[j][i] = M[piv[j]][pinv[i]], through the panel's
+  // shared memory (free now): 32 rows M[piv[j]] at a time are read whole
+  // and coalesced, then every row i of psiM takes its 32 columns from
+  // column pinv[i] of them (an odd row stride keeps those reads on distinct
+  // banks), so that neither side gathers single doubles from global memory
+  T* out       = wv.ainv(s);
+  double* S    = F;     // [32][SS] over the panel and the chunk buffers: 32 (n + 1) <= 33 n + 2304 doubles
+  const int SS = n | 1; // >= n, odd
+  for (int jb = 0; jb < n; jb += 32)
   {
-    const int ci = pinv[i];
-    for (int j = lane; j < n; j += 32)
-      out[(size_t)i * npad + j] = (T)M[(size_t)piv[j] * npad + ci];
+    const int jw = min(32, n - jb);
+    for (int idx = tid; idx < jw * n; idx += NT)
+    {
+      const int jj = idx / n, c = idx - jj * n;
+      S[jj * SS + c] = M[(size_t)piv[jb + jj] * npad + c];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < n * 32; idx += NT)
+    {
+      const int i = idx >> 5, jj = idx & 31;
+      if (jj < jw)
+        out[(size_t)i * npad + jb + jj] = (T)S[jj * SS + pinv[i]];
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (tid == 0)
   {
     // parity of the permutation c -> piv[c] from its cycles

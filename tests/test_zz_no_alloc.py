@@ -77,3 +77,30 @@ def test_noalloc_singular_then_regular():
     psim, lg, ph = _noalloc(lib, a)
     ref_psim, ref_lg, ref_ph = _engine(lib, a)
     assert np.array_equal(psim, ref_psim) and lg == ref_lg and ph == ref_ph
+
+
+@pytest.mark.parametrize('n', [64, 900])
+def test_nan_entries_are_singular_then_regular(n):
+    """A NaN in the matrix competes as 0 in every pivot search, so the
+    pivots stay rows of the matrix and the inverse reports a zero pivot:
+    QMC_ERR_SINGULAR from the engine (and from the allocation-free entry
+    point within its size), after which a regular matrix inverts as before.
+    n = 900 takes the column-at-a-time kernel (the blocked one's panel no
+    longer fits in shared memory)."""
+    lib = product()
+    rng = np.random.default_rng(11)
+    a = _matrix(rng, n)
+    for bad in ('entry', 'column'):
+        s = a.copy()
+        if bad == 'entry':
+            s[3, 7] = np.nan
+        else:
+            s[:, 5] = np.nan
+        calls = [_engine] + ([_noalloc] if n <= capi.NOALLOC_MAX_N else [])
+        for f in calls:
+            with pytest.raises(api.QMCError) as ei:
+                f(lib, s)
+            assert capi.STATUS[ei.value.status] == 'QMC_ERR_SINGULAR', (bad, f.__name__)
+    psim, lg, _ = _engine(lib, a)
+    assert np.abs(psim.T @ a - np.eye(n)).max() < 1e-8
+    assert abs(lg - np.linalg.slogdet(a)[1]) < 1e-9 * n
