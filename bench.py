@@ -63,6 +63,9 @@ def parse():
     ap.add_argument('--rate', type=float, default=20.0, help='serve: arrivals per second')
     ap.add_argument('--budget-gb', type=float, default=100.0, help='serve: device memory budget of the server')
     ap.add_argument('--no-tune', action='store_true', help='uneven: skip the autotuner (default launch settings)')
+    ap.add_argument('--schedule', default='auto', choices=['auto', 'static', 'queue'],
+                    help='the sweep CTAs\' schedule (qmc_walkers_set_schedule)')
+    ap.add_argument('--unit', type=int, default=0, help='moves per unit of the work-queue schedule (0: default)')
     ap.add_argument('--flush', default='tc', choices=['tc', 'simt'],
                     help='Woodbury flush on the tensor cores (tcgen05 3xTF32) or the CUDA cores (FP32 FMA)')
     ap.add_argument('--plain-steps', type=int, default=4,
@@ -160,6 +163,24 @@ def build_workload(lib, args, capi, api, device_rng_seeds):
 # tensor-core flush); the bench's traffic figure scales it by the moves of
 # one launch
 MEASURED_TRAFFIC_PER_MOVE = (24.772e9 + 5.215e9) / (64 * 1536)
+
+
+def schedule_of(lib, walkers, args):
+    """The sweep form qmc_walkers_set_schedule selects for this batch (AUTO:
+    the work queue once the walkers outnumber the SMs), its kernel and a
+    line for the config."""
+    import torch
+    from miniqmc_b200 import capi
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    queue = args.schedule == 'queue' or (args.schedule == 'auto' and args.walkers > sms)
+    per_sm = C.c_int()
+    lib.call('walkers_occupancy', walkers.h, C.byref(per_sm))
+    if not queue:
+        return {'kernel': 'sweep_kernel', 'text': 'static: one CTA per walker, %d per SM' % per_sm.value}
+    ctas = per_sm.value * sms
+    unit = args.unit or capi.SCHED_UNIT_DEFAULT
+    return {'kernel': 'sweep_queue_kernel',
+            'text': 'work queue: %d CTAs (%d per SM) take units of %d moves' % (ctas, per_sm.value, unit)}
 
 
 def plain_fp64_form(lib, args, api, capi, stream_cls):
@@ -634,6 +655,9 @@ def main():
     lib.call('walkers_set_stream', walkers.h, C.c_void_p(stream.cuda_stream))
     if args.precision == 'mixed':
         lib.call('walkers_set_tensor_cores', walkers.h, 1 if args.flush == 'tc' else 0)
+    mode = {'auto': capi.SCHED_AUTO, 'static': capi.SCHED_STATIC, 'queue': capi.SCHED_QUEUE}[args.schedule]
+    lib.call('walkers_set_schedule', walkers.h, mode, args.unit, 0)
+    sched = schedule_of(lib, walkers, args)
     walkers.evaluate_log()
     W, N = args.walkers, spec.n_elec
     count = C.c_int64()
@@ -739,7 +763,7 @@ def main():
                             if (args.precision == 'mixed' and args.delay == 32) else None),
                 'traffic_source': 'ncu dram bytes per move (64 walkers, grid 74x74x37) x moves per launch',
                 'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm,
-                'kernel': 'sweep_kernel<%s>' % ('float' if s == 4 else 'double'), 'launch_ms': avg_launch_ms}
+                'kernel': '%s<%s>' % (sched['kernel'], 'float' if s == 4 else 'double'), 'launch_ms': avg_launch_ms}
     # the Woodbury GEMMs on the tensor cores (tcgen05 kind::tf32, 3xTF32):
     # per flush GEMM1 (n x npad by npad x k) and GEMM2 (n x k by k x npad),
     # three TF32 products each, i.e. 12 n npad flops per accepted move.
@@ -803,7 +827,8 @@ def main():
                              % (system_bytes(lib, system) / 1e9, walkers_bytes(lib, walkers) / 1e9),
                        'acceptance': a, 'parallelism': 'replicas x%d' % world,
                        'flush': args.flush if args.precision == 'mixed' else 'simt',
-                       'recompute_every': args.recompute_every, 'recompute_ms': recompute_ms},
+                       'recompute_every': args.recompute_every, 'recompute_ms': recompute_ms,
+                       'schedule': sched['text']},
             'roofline': roofline, 'tensor': tensor, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clk,
             'plain_fp64': plain, 'batched_fp64': batched, 'error': error,
             'operating_points': operating_points(value, refresh1, args.recompute_every, error),

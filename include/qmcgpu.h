@@ -378,10 +378,27 @@ int qmc_walkers_set_threads(qmc_walkers* w, int threads);
  * 32 MB of the 126 MB L2. */
 enum { QMC_PREFETCH_AUTO = 0, QMC_PREFETCH_OFF = 1, QMC_PREFETCH_ON = 2 };
 int qmc_walkers_set_prefetch(qmc_walkers* w, int mode);
+/* Schedule of the fused sweep's CTAs (no reference counterpart: the
+ * reference moves each walker on one host thread).  STATIC: one CTA per
+ * walker for the whole step.  QUEUE: `ctas` resident CTAs (0: walkers per SM
+ * x SMs, every slot of the device) take each walker's step in units of at most
+ * unit_moves consecutive moves of one spin (0: QMC_SCHED_UNIT_DEFAULT), in
+ * the order unit j of every walker before unit j + 1 of any, each unit after
+ * its walker's previous one; a walker's state passes between units through
+ * device memory, so the results are those of STATIC bit for bit.  With more
+ * walkers than SMs the static form leaves the SMs that hold one walker more
+ * setting the step (512 walkers on 148 SMs: 68 SMs with four, 80 with three)
+ * while the queue spreads every walker over busy and quiet SMs alike.  AUTO
+ * (the default): QUEUE when the walkers outnumber the SMs, else STATIC.
+ * Batch groups always launch STATIC. */
+enum { QMC_SCHED_AUTO = 0, QMC_SCHED_STATIC = 1, QMC_SCHED_QUEUE = 2 };
+#define QMC_SCHED_UNIT_DEFAULT 16
+int qmc_walkers_set_schedule(qmc_walkers* w, int mode, int unit_moves, int ctas);
 int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* tensor_cores);
 /* Walkers (CTAs) of this batch's fused sweep that one SM holds at once with
- * its present settings (registers, shared memory, block size): with W
- * walkers a launch runs in ceil(W / (walkers_per_sm x SMs)) waves. */
+ * its present settings (registers, shared memory, block size, and the form
+ * its schedule selects): with W walkers a static launch runs in
+ * ceil(W / (walkers_per_sm x SMs)) waves. */
 int qmc_walkers_occupancy(const qmc_walkers* w, int* walkers_per_sm);
 
 /* Batch groups (no reference counterpart: the reference's flex_ batch,

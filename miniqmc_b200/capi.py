@@ -19,6 +19,8 @@ WF_DET, WF_J1, WF_J2, WF_ALL, WF_J3 = 1, 2, 4, 7, 8
 J3_PARAMS = 26
 RNG_DEVICE, RNG_HOST = 0, 1
 PREFETCH_AUTO, PREFETCH_OFF, PREFETCH_ON = 0, 1, 2
+SCHED_AUTO, SCHED_STATIC, SCHED_QUEUE = 0, 1, 2
+SCHED_UNIT_DEFAULT = 16
 NIO_REF32, NIO_PRIM4 = 0, 1
 NIO_QUIRK_UNIT_IONS, NIO_QUIRK_ONE_GROUP = 1, 2
 MAX_FUNCTOR_COEFS = 32
@@ -133,6 +135,7 @@ PRODUCT_ONLY = {
     'walkers_set_move_batching': (I, [P, I]),
     'walkers_set_threads': (I, [P, I]),
     'walkers_set_prefetch': (I, [P, I]),
+    'walkers_set_schedule': (I, [P, I, I, I]),
     'local_kinetic': (I, [P, PD]),
     'walkers_checkpoint_bytes': (I, [P, C.POINTER(C.c_size_t)]),
     'walkers_checkpoint': (I, [P, P, C.c_size_t]),

@@ -668,7 +668,7 @@ static void free_walkers(qmc_walkers* w)
     for (void* p : w->allocs)
       cudaFreeAsync(p, w->alloc_stream);
     w->allocs.clear();
-    if (!w->d_ur && !w->d_delta && !w->d_trace && !w->d_rows && !w->d_timers)
+    if (!w->d_ur && !w->d_delta && !w->d_trace && !w->d_rows && !w->d_timers && !w->d_sched)
       return;
   }
   if (w->stream)
@@ -681,6 +681,7 @@ static void free_walkers(qmc_walkers* w)
   cudaFree(w->d_trace);
   cudaFree(w->d_rows);
   cudaFree(w->d_timers);
+  cudaFree(w->d_sched);
   if (w->own_stream && w->stream)
     cudaStreamDestroy(w->stream);
 }
@@ -810,6 +811,16 @@ int qmc_walkers_set_prefetch(qmc_walkers* w, int mode)
   return QMC_OK;
 }
 
+int qmc_walkers_set_schedule(qmc_walkers* w, int mode, int unit_moves, int ctas)
+{
+  if (!w || mode < QMC_SCHED_AUTO || mode > QMC_SCHED_QUEUE || unit_moves < 0 || ctas < 0)
+    return fail(QMC_ERR_ARG, "bad schedule");
+  w->sched_mode = mode;
+  w->sched_unit = unit_moves ? unit_moves : QMC_SCHED_UNIT_DEFAULT;
+  w->sched_ctas = ctas;
+  return QMC_OK;
+}
+
 int qmc_walkers_set_threads(qmc_walkers* w, int threads)
 {
   if (!w)
@@ -834,12 +845,15 @@ int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* 
     *tensor_cores = w->use_tc ? 1 : 0;
   return QMC_OK;
 }
+static int sweep_queue_ctas(const qmc_walkers* w);
 int qmc_walkers_occupancy(const qmc_walkers* w, int* walkers_per_sm)
 {
   if (!w || !walkers_per_sm)
     return fail(QMC_ERR_ARG, "null pointer");
-  const int n = sweep_occupancy(w->fp32, w->threads, w->dw.k, w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0,
-                                w->max_moves > 1);
+  const int q = sweep_queue_ctas(w);
+  const int n = q < 0 ? -1
+                      : sweep_occupancy(w->fp32, w->threads, w->dw.k, w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0,
+                                        w->max_moves > 1, q > 0);
   if (n < 0)
     return fail(QMC_ERR_CUDA, "occupancy query failed");
   *walkers_per_sm = n;
@@ -1347,6 +1361,30 @@ int qmc_wf_get_inverse(qmc_walkers* w, int walker, int spin, double* psiM)
 }
 
 // ------------------------------------------------------------ sweep -----
+// CTAs of a work-queue sweep launch for this batch, 0 for the static form
+// (one CTA per walker), -1 if the occupancy query failed.  AUTO takes the
+// queue once the walkers outnumber the SMs, with every resident CTA slot
+// (walkers per SM x SMs) taking units: the slots beyond the walkers hold
+// the units whose walker is still busy, so no walker waits for a CTA.
+static int sweep_queue_ctas(const qmc_walkers* w)
+{
+  const int W = w->dw.W;
+  if (w->sched_mode == QMC_SCHED_STATIC)
+    return 0;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
+    return -1;
+  if (w->sched_mode == QMC_SCHED_AUTO && W <= sms)
+    return 0;
+  if (w->sched_ctas > 0)
+    return w->sched_ctas;
+  const int per_sm = sweep_occupancy(w->fp32, w->threads, w->dw.k, w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0,
+                                     w->max_moves > 1, true);
+  if (per_sm < 1)
+    return -1;
+  return per_sm * sms;
+}
+
 static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accept, int rng_mode, const double* ur,
                        const double* delta, int recompute_every, double* trace, bool async)
 {
@@ -1379,6 +1417,22 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
   task.delta     = w->d_delta;
   task.trace     = trace ? w->d_trace : nullptr;
   CK(cudaMemcpyAsync(w->d_task, &task, sizeof(task), cudaMemcpyHostToDevice, w->stream));
+  const int queue_ctas = sweep_queue_ctas(w);
+  if (queue_ctas < 0)
+    return fail(QMC_ERR_CUDA, "occupancy query failed");
+  const size_t n_sched =
+      queue_ctas ? sweep_queue_words((int)W, queue_ctas,
+                                     sweep_queue_units((int)N, w->sys->h.n_up, n_substeps, w->sched_unit))
+                 : 0;
+  if (n_sched > (size_t)INT32_MAX)
+    return fail(QMC_ERR_ARG, "too many work-queue units in one launch: take longer units");
+  if (w->cap_sched < n_sched)
+  {
+    cudaFree(w->d_sched);
+    w->d_sched = nullptr;
+    CK(cudaMalloc(&w->d_sched, n_sched * sizeof(int)));
+    w->cap_sched = n_sched;
+  }
   for (int step = 0; step < n_steps; ++step)
   {
     if (rng_mode == QMC_RNG_HOST)
@@ -1388,8 +1442,16 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
       CK(cudaMemcpyAsync(w->d_delta, delta + step * blk * 3, 3 * blk * sizeof(double), cudaMemcpyHostToDevice,
                          w->stream));
     }
-    CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k, w->stream,
-                    w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0, w->max_moves > 1));
+    const bool j3 = (w->sys->h.comp & QMC_WF_J3) != 0;
+    if (queue_ctas > 0)
+    {
+      CK(cudaMemsetAsync(w->d_sched, 0, n_sched * sizeof(int), w->stream));
+      CK(launch_sweep_queue(w->fp32, w->d_task, queue_ctas, n_substeps, accept, w->threads, w->dw.k, w->stream,
+                            w->use_tc, j3, w->max_moves > 1, w->sched_unit, w->d_sched));
+    }
+    else
+      CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k,
+                      w->stream, w->use_tc, j3, w->max_moves > 1));
     w->launches++;
     if (trace)
       CK(cudaMemcpyAsync(trace + (size_t)step * W * n_substeps * N * 8, w->d_trace,

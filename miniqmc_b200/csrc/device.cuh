@@ -779,9 +779,12 @@ constexpr int J2_SCAN = 8;
 __host__ __device__ constexpr size_t j2_list_bytes() { return (size_t)8 * 32 * J2_SCAN * sizeof(int); }
 
 // partial J2 sums over the electrons for electron iel moved to pos:
-// sum u, sum du*dr (TwoBodyJastrow::ratioGrad with the move row, flip = iel)
+// sum u, sum du*dr (TwoBodyJastrow::ratioGrad with the move row, flip = iel).
+// Rs is not __restrict__: accepted moves rewrite it during a launch (on
+// another SM, between units of the work-queue sweep), so its loads must stay
+// on the coherent path rather than the read-only one
 template <typename T, typename A>
-__device__ void j2_partials(const SysSmem<T>& ss, const T* __restrict__ Rs, int Npad, int iel, const double* pos,
+__device__ void j2_partials(const SysSmem<T>& ss, const T* Rs, int Npad, int iel, const double* pos,
                             A* part, bool grads, int* wlist)
 {
   const T px = (T)pos[0], py = (T)pos[1], pz = (T)pos[2];

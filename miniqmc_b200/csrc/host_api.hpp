@@ -58,6 +58,13 @@ struct qmc_walkers_s
   bool tc_capable = false; // FP32, >= 128 threads, k <= 32, determinant on
   bool use_tc     = false; // Woodbury flushes on the tensor cores
   int max_moves   = 1; // moves the fused sweep evaluates together (qmc_walkers_set_move_batching)
+  // the sweep's schedule (qmc_walkers_set_schedule) and the work-queue
+  // form's counters and hand-over ring (launch_sweep_queue)
+  int sched_mode   = QMC_SCHED_AUTO;
+  int sched_unit   = QMC_SCHED_UNIT_DEFAULT;
+  int sched_ctas   = 0;
+  int* d_sched     = nullptr;
+  size_t cap_sched = 0;
   // a request-loop job's batch: device memory from the server's pool,
   // allocated and freed stream-ordered on its stream (else both null)
   cudaStream_t alloc_stream = nullptr;
