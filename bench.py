@@ -775,7 +775,7 @@ def main():
         tflop = 12.0 * n * npad * a * W * N / 1e12
         tf32_peak = pk['bf16_tflops'] / 2
         ach = tflop / (avg_launch_ms / 1e3)
-        tensor = {'kernel': 'sweep_kernel Woodbury flush (tcgen05 kind::tf32, 3xTF32)', 'tflop_per_launch': tflop,
+        tensor = {'kernel': '%s Woodbury flush (tcgen05 kind::tf32, 3xTF32)' % sched['kernel'], 'tflop_per_launch': tflop,
                   'achieved': ach, 'peak': tf32_peak, 'unit': 'TFLOP/s', 'frac': ach / tf32_peak,
                   'peak_kind': pk_kind + ' bf16 / 2',
                   'ncu_pipe_tensor_cycles_active_pct': 0.75}

@@ -846,6 +846,7 @@ int qmc_walkers_get_config(const qmc_walkers* w, int* threads, int* delay, int* 
   return QMC_OK;
 }
 static int sweep_queue_ctas(const qmc_walkers* w);
+static int sweep_queue_ctas_query(const qmc_walkers* w);
 int qmc_walkers_occupancy(const qmc_walkers* w, int* walkers_per_sm)
 {
   if (!w || !walkers_per_sm)
@@ -1364,13 +1365,28 @@ int qmc_wf_get_inverse(qmc_walkers* w, int walker, int spin, double* psiM)
 // CTAs of a work-queue sweep launch for this batch, 0 for the static form
 // (one CTA per walker), -1 if the occupancy query failed.  AUTO takes the
 // queue once the walkers outnumber the SMs, with every resident CTA slot
-// (walkers per SM x SMs) taking units: the slots beyond the walkers hold
-// the units whose walker is still busy, so no walker waits for a CTA.
+// (walkers per SM x SMs) taking units: the slots beyond the walkers are the
+// CTAs that wait for a walker, so no walker waits for a CTA.
 static int sweep_queue_ctas(const qmc_walkers* w)
 {
-  const int W = w->dw.W;
   if (w->sched_mode == QMC_SCHED_STATIC)
     return 0;
+  // the answer for the present settings, kept from the last call
+  const int key[6] = {w->sched_mode, w->sched_ctas, w->threads, (int)w->use_tc, w->max_moves, 1};
+  if (std::equal(key, key + 6, w->sched_key))
+    return w->sched_cached;
+  const int n = sweep_queue_ctas_query(w);
+  if (n >= 0)
+  {
+    std::copy(key, key + 6, w->sched_key);
+    w->sched_cached = n;
+  }
+  return n;
+}
+
+static int sweep_queue_ctas_query(const qmc_walkers* w)
+{
+  const int W = w->dw.W;
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
     return -1;

@@ -65,6 +65,10 @@ struct qmc_walkers_s
   int sched_ctas   = 0;
   int* d_sched     = nullptr;
   size_t cap_sched = 0;
+  // CTAs of the work-queue launch for the settings in sched_key (the
+  // occupancy query runs once per change of settings, not per sweep call)
+  mutable int sched_key[6] = {0, 0, 0, 0, 0, 0};
+  mutable int sched_cached = 0;
   // a request-loop job's batch: device memory from the server's pool,
   // allocated and freed stream-ordered on its stream (else both null)
   cudaStream_t alloc_stream = nullptr;

@@ -586,21 +586,26 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
 // CTAs per SM from the kernel's registers and static shared memory and the
 // launch's block size and dynamic shared memory (registers are allocated
 // per warp in units of 256; every CTA also reserves 1 KB of shared memory)
+// (the device figures by cudaDeviceGetAttribute: cudaGetDeviceProperties
+// takes milliseconds, and a sweep call asks this on every call)
 template <typename K> static int occupancy_of(K kernel, int threads, size_t bytes)
 {
   cudaFuncAttributes fa;
-  cudaDeviceProp p;
-  int dev = 0;
+  int dev = 0, regs = 0, smem = 0, reserved = 0, max_threads = 0, max_blocks = 0;
   if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
-      cudaGetDeviceProperties(&p, dev) != cudaSuccess)
+      cudaDeviceGetAttribute(&regs, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_blocks, cudaDevAttrMaxBlocksPerMultiprocessor, dev) != cudaSuccess)
     return -1;
   const int warps     = (threads + 31) / 32;
   const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;
-  const int by_regs   = regs_warp ? p.regsPerMultiprocessor / (warps * regs_warp) : p.maxBlocksPerMultiProcessor;
-  const size_t cta    = fa.sharedSizeBytes + bytes + p.reservedSharedMemPerBlock;
-  const int by_smem   = (int)(p.sharedMemPerMultiprocessor / cta);
-  const int by_warps  = p.maxThreadsPerMultiProcessor / (warps * 32);
-  return std::min(std::min(by_regs, by_smem), std::min(by_warps, p.maxBlocksPerMultiProcessor));
+  const int by_regs   = regs_warp ? regs / (warps * regs_warp) : max_blocks;
+  const size_t cta    = fa.sharedSizeBytes + bytes + (size_t)reserved;
+  const int by_smem   = (int)((size_t)smem / cta);
+  const int by_warps  = max_threads / (warps * 32);
+  return std::min(std::min(by_regs, by_smem), std::min(by_warps, max_blocks));
 }
 template <typename T, bool HAS_J3, bool EPOCH> static int occupancy_t(int threads, size_t bytes, bool queue)
 {
