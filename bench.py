@@ -167,12 +167,11 @@ MEASURED_TRAFFIC_PER_MOVE = (24.772e9 + 5.215e9) / (64 * 1536)
 
 def schedule_of(lib, walkers, args):
     """The sweep form qmc_walkers_set_schedule selects for this batch (AUTO:
-    the work queue once the walkers outnumber the SMs), its kernel and a
-    line for the config."""
+    the work queue), its kernel and a line for the config."""
     import torch
     from miniqmc_b200 import capi
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    queue = args.schedule == 'queue' or (args.schedule == 'auto' and args.walkers > sms)
+    queue = args.schedule in ('queue', 'auto')
     per_sm = C.c_int()
     lib.call('walkers_occupancy', walkers.h, C.byref(per_sm))
     if not queue:

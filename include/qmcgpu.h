@@ -380,17 +380,19 @@ enum { QMC_PREFETCH_AUTO = 0, QMC_PREFETCH_OFF = 1, QMC_PREFETCH_ON = 2 };
 int qmc_walkers_set_prefetch(qmc_walkers* w, int mode);
 /* Schedule of the fused sweep's CTAs (no reference counterpart: the
  * reference moves each walker on one host thread).  STATIC: one CTA per
- * walker for the whole step.  QUEUE: `ctas` resident CTAs (0: walkers per SM
- * x SMs, every slot of the device) take each walker's step in units of at most
- * unit_moves consecutive moves of one spin (0: QMC_SCHED_UNIT_DEFAULT), in
- * the order unit j of every walker before unit j + 1 of any, each unit after
- * its walker's previous one; a walker's state passes between units through
- * device memory, so the results are those of STATIC bit for bit.  With more
- * walkers than SMs the static form leaves the SMs that hold one walker more
- * setting the step (512 walkers on 148 SMs: 68 SMs with four, 80 with three)
- * while the queue spreads every walker over busy and quiet SMs alike.  AUTO
- * (the default): QUEUE when the walkers outnumber the SMs, else STATIC.
- * Batch groups always launch STATIC. */
+ * walker for the whole step (four per SM at NiO-128, 80 registers a
+ * thread).  QUEUE: `ctas` resident CTAs (0: walkers per SM x SMs, every slot
+ * of the device) take each walker's step in units of at most unit_moves
+ * consecutive moves of one spin (0: QMC_SCHED_UNIT_DEFAULT).  A unit that
+ * ends on an SM with no spare CTA hands its walker to the CTA that has
+ * waited longest; where a CTA waits already, the walker goes on in place.
+ * A walker's state passes between units through device memory, so the
+ * results are those of STATIC bit for bit.  Up to 192 threads a walker the
+ * queue runs three CTAs per SM at up to 112 registers a thread, and the
+ * walkers take turns where they outnumber the slots.  At NiO-128 it measured
+ * 141 ms per 512-walker launch against 173 ms static, 80 against 101 ms at
+ * 148 walkers.  AUTO (the default) is QUEUE.  Batch groups always launch
+ * STATIC. */
 enum { QMC_SCHED_AUTO = 0, QMC_SCHED_STATIC = 1, QMC_SCHED_QUEUE = 2 };
 #define QMC_SCHED_UNIT_DEFAULT 16
 int qmc_walkers_set_schedule(qmc_walkers* w, int mode, int unit_moves, int ctas);

@@ -1363,10 +1363,11 @@ int qmc_wf_get_inverse(qmc_walkers* w, int walker, int spin, double* psiM)
 
 // ------------------------------------------------------------ sweep -----
 // CTAs of a work-queue sweep launch for this batch, 0 for the static form
-// (one CTA per walker), -1 if the occupancy query failed.  AUTO takes the
-// queue once the walkers outnumber the SMs, with every resident CTA slot
-// (walkers per SM x SMs) taking units: the slots beyond the walkers are the
-// CTAs that wait for a walker, so no walker waits for a CTA.
+// (one CTA per walker), -1 if the occupancy query failed.  AUTO is the
+// queue, with every resident CTA slot (walkers per SM x SMs) taking units:
+// the slots beyond the walkers are the CTAs that wait for a walker, so no
+// walker waits for a CTA, and where the walkers outnumber the slots they
+// take turns on them.
 static int sweep_queue_ctas(const qmc_walkers* w)
 {
   if (w->sched_mode == QMC_SCHED_STATIC)
@@ -1386,12 +1387,9 @@ static int sweep_queue_ctas(const qmc_walkers* w)
 
 static int sweep_queue_ctas_query(const qmc_walkers* w)
 {
-  const int W = w->dw.W;
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
     return -1;
-  if (w->sched_mode == QMC_SCHED_AUTO && W <= sms)
-    return 0;
   if (w->sched_ctas > 0)
     return w->sched_ctas;
   const int per_sm = sweep_occupancy(w->fp32, w->threads, w->dw.k, w->use_tc, (w->sys->h.comp & QMC_WF_J3) != 0,

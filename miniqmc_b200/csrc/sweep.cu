@@ -212,9 +212,14 @@ __device__ __forceinline__ int sm_id()
 // this runs)
 constexpr unsigned long long kQueueWaitNs = 10ull * 1000 * 1000 * 1000;
 
-template <typename T, bool HAS_J3, bool EPOCH>
-__global__ void __launch_bounds__(256, 3) sweep_queue_kernel(const SweepTask* __restrict__ tasks, int n_substeps,
-                                                          double accept_thr, int tc, int unit, int* sched)
+// MAXT: the largest block the instantiation takes.  Three CTAs per SM
+// either way: at up to 192 threads that leaves 112 registers a thread (the
+// kernel takes 96 and spills a third of what it spills at 80), which at 512
+// NiO-128 walkers measured 141 ms per launch against 161.5 ms for four CTAs
+// per SM at 80 registers (and 154 ms for two CTAs per SM at 168 registers).
+template <typename T, bool HAS_J3, bool EPOCH, int MAXT>
+__global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* __restrict__ tasks, int n_substeps,
+                                                           double accept_thr, int tc, int unit, int* sched)
 {
   __shared__ SysSmem<T> ss;
   __shared__ MoveSmem m;
@@ -520,12 +525,12 @@ template <typename T, bool HAS_J3, bool EPOCH> static void set_smem_attr(size_t 
     done = bytes;
   }
 }
-template <typename T, bool HAS_J3, bool EPOCH> static void set_queue_smem_attr(size_t bytes)
+template <typename T, bool HAS_J3, bool EPOCH, int MAXT> static void set_queue_smem_attr(size_t bytes)
 {
   static size_t done = 0;
   if (bytes > done)
   {
-    cudaFuncSetAttribute(sweep_queue_kernel<T, HAS_J3, EPOCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(sweep_queue_kernel<T, HAS_J3, EPOCH, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)bytes);
     done = bytes;
   }
@@ -607,13 +612,16 @@ template <typename K> static int occupancy_of(K kernel, int threads, size_t byte
   const int by_warps  = max_threads / (warps * 32);
   return std::min(std::min(by_regs, by_smem), std::min(by_warps, max_blocks));
 }
+template <typename T, bool HAS_J3, bool EPOCH, int MAXT> static int queue_occupancy_t(int threads, size_t bytes)
+{
+  set_queue_smem_attr<T, HAS_J3, EPOCH, MAXT>(bytes);
+  return occupancy_of(sweep_queue_kernel<T, HAS_J3, EPOCH, MAXT>, threads, bytes);
+}
 template <typename T, bool HAS_J3, bool EPOCH> static int occupancy_t(int threads, size_t bytes, bool queue)
 {
   if (queue)
-  {
-    set_queue_smem_attr<T, HAS_J3, EPOCH>(bytes);
-    return occupancy_of(sweep_queue_kernel<T, HAS_J3, EPOCH>, threads, bytes);
-  }
+    return threads <= 192 ? queue_occupancy_t<T, HAS_J3, EPOCH, 192>(threads, bytes)
+                          : queue_occupancy_t<T, HAS_J3, EPOCH, 256>(threads, bytes);
   set_smem_attr<T, HAS_J3, EPOCH>(bytes);
   return occupancy_of(sweep_kernel<T, HAS_J3, EPOCH>, threads, bytes);
 }
@@ -634,25 +642,33 @@ int sweep_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool ep
                  : occupancy_t<double, false, false>(threads, b, queue);
 }
 
+template <typename T, bool HAS_J3, bool EPOCH, int MAXT>
+static void queue_launch_tt(size_t bytes, const SweepTask* d_task, int ctas, int n_substeps, double accept,
+                            int threads, cudaStream_t st, int tc, int unit, int* sched)
+{
+  set_queue_smem_attr<T, HAS_J3, EPOCH, MAXT>(bytes);
+  sweep_queue_kernel<T, HAS_J3, EPOCH, MAXT>
+      <<<ctas, threads, bytes, st>>>(d_task, n_substeps, accept, tc, unit, sched);
+}
+template <typename T, bool HAS_J3, bool EPOCH>
+static void queue_launch_t(size_t bytes, const SweepTask* d_task, int ctas, int n_substeps, double accept,
+                           int threads, cudaStream_t st, int tc, int unit, int* sched)
+{
+  if (threads <= 192)
+    queue_launch_tt<T, HAS_J3, EPOCH, 192>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+  else
+    queue_launch_tt<T, HAS_J3, EPOCH, 256>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+}
 template <typename T>
 static void launch_queue_t(bool j3, bool epoch, size_t bytes, const SweepTask* d_task, int ctas, int n_substeps,
                            double accept, int threads, cudaStream_t st, int tc, int unit, int* sched)
 {
   if (j3)
-  {
-    set_queue_smem_attr<T, true, false>(bytes);
-    sweep_queue_kernel<T, true, false><<<ctas, threads, bytes, st>>>(d_task, n_substeps, accept, tc, unit, sched);
-  }
+    queue_launch_t<T, true, false>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
   else if (epoch)
-  {
-    set_queue_smem_attr<T, false, true>(bytes);
-    sweep_queue_kernel<T, false, true><<<ctas, threads, bytes, st>>>(d_task, n_substeps, accept, tc, unit, sched);
-  }
+    queue_launch_t<T, false, true>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
   else
-  {
-    set_queue_smem_attr<T, false, false>(bytes);
-    sweep_queue_kernel<T, false, false><<<ctas, threads, bytes, st>>>(d_task, n_substeps, accept, tc, unit, sched);
-  }
+    queue_launch_t<T, false, false>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
 }
 
 cudaError_t launch_sweep_queue(bool fp32, const SweepTask* d_task, int ctas, int n_substeps, double accept,

@@ -23,10 +23,12 @@ SMALL = dict(tiling=(1, 1, 2), grid=(12, 12, 12))
 NIO128 = dict(tiling=(4, 4, 2), grid=(24, 24, 12), jastrow='synthetic')
 
 
-def _batch(spec, precision, W, delay, seeds, mode, unit=0, ctas=0, moves=1, tc=None):
+def _batch(spec, precision, W, delay, seeds, mode, unit=0, ctas=0, moves=1, tc=None, threads=0):
     lib = H.product()
     w = api.Walkers(api.System(lib, spec, precision), W, delay)
     w.init_random(seeds)
+    if threads:
+        lib.call('walkers_set_threads', w.h, threads)
     lib.call('walkers_set_schedule', w.h, mode, unit, ctas)
     if moves > 1:
         lib.call('walkers_set_move_batching', w.h, moves)
@@ -36,11 +38,11 @@ def _batch(spec, precision, W, delay, seeds, mode, unit=0, ctas=0, moves=1, tc=N
 
 
 def _compare(kw, precision, W, delay, unit, ctas, steps=2, substeps=1, host_rng=False, moves=1, tc=None,
-             components=capi.WF_ALL):
+             components=capi.WF_ALL, threads=0):
     sp, _ = H.spec_pair(components=components, **kw)
     seeds = H.oracle_primes(W)
-    a = _batch(sp, precision, W, delay, seeds, capi.SCHED_STATIC, moves=moves, tc=tc)
-    b = _batch(sp, precision, W, delay, seeds, capi.SCHED_QUEUE, unit, ctas, moves=moves, tc=tc)
+    a = _batch(sp, precision, W, delay, seeds, capi.SCHED_STATIC, moves=moves, tc=tc, threads=threads)
+    b = _batch(sp, precision, W, delay, seeds, capi.SCHED_QUEUE, unit, ctas, moves=moves, tc=tc, threads=threads)
     assert np.array_equal(a.evaluate_log(), b.evaluate_log())
     ur = de = None
     if host_rng:
@@ -64,9 +66,12 @@ def _compare(kw, precision, W, delay, unit, ctas, steps=2, substeps=1, host_rng=
 
 
 @pytest.mark.parametrize('precision', [capi.PREC_FP64, capi.PREC_MIXED])
-def test_queue_equals_static_small(precision):
-    # 5 walkers on 2 CTAs, units of 3 moves, 2 substeps, device streams
-    _compare(SMALL, precision, 5, 4, unit=3, ctas=2, substeps=2)
+@pytest.mark.parametrize('threads', [0, 256])
+def test_queue_equals_static_small(precision, threads):
+    # 5 walkers on 2 CTAs, units of 3 moves, 2 substeps, device streams;
+    # the default block and a 256-thread one (the queue kernel's two
+    # register budgets)
+    _compare(SMALL, precision, 5, 4, unit=3, ctas=2, substeps=2, threads=threads)
 
 
 def test_queue_units_of_one_move_host_streams():
