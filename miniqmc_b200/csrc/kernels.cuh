@@ -62,6 +62,7 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
 // CTAs (walkers) of one sweep launch that an SM holds at once, or -1
 // queue: of the work-queue form (launch_sweep_queue)
 int sweep_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool epoch, bool queue = false);
+int sweep_queue_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool epoch);
 // the sweep of one batch in the work-queue form: `ctas` resident CTAs take
 // units of at most `unit` moves of one spin of a walker, a walker passing
 // from CTA to CTA between its units; sched: device ints, zero,
