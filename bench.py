@@ -66,6 +66,7 @@ def parse():
     ap.add_argument('--schedule', default='auto', choices=['auto', 'static', 'queue'],
                     help='the sweep CTAs\' schedule (qmc_walkers_set_schedule)')
     ap.add_argument('--unit', type=int, default=0, help='moves per unit of the work-queue schedule (0: default)')
+    ap.add_argument('--threads', type=int, default=0, help='threads per walker (0: the library default)')
     ap.add_argument('--flush', default='tc', choices=['tc', 'simt'],
                     help='Woodbury flush on the tensor cores (tcgen05 3xTF32) or the CUDA cores (FP32 FMA)')
     ap.add_argument('--plain-steps', type=int, default=4,
@@ -654,6 +655,8 @@ def main():
     lib.call('walkers_set_stream', walkers.h, C.c_void_p(stream.cuda_stream))
     if args.precision == 'mixed':
         lib.call('walkers_set_tensor_cores', walkers.h, 1 if args.flush == 'tc' else 0)
+    if args.threads:
+        lib.call('walkers_set_threads', walkers.h, args.threads)
     mode = {'auto': capi.SCHED_AUTO, 'static': capi.SCHED_STATIC, 'queue': capi.SCHED_QUEUE}[args.schedule]
     lib.call('walkers_set_schedule', walkers.h, mode, args.unit, 0)
     sched = schedule_of(lib, walkers, args)
