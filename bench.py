@@ -449,6 +449,8 @@ def run_uneven(args, lib, api, capi, torch):
         batches.append((spec, W, w))
         chosen.append({'tiling': list(tiling), 'walkers': W, 'electrons': spec.n_elec, **best})
     g = api.Group(lib, [b[2] for b in batches])
+    mode = {'auto': capi.SCHED_AUTO, 'static': capi.SCHED_STATIC, 'queue': capi.SCHED_QUEUE}[args.schedule]
+    lib.call('group_set_schedule', g.h, mode, args.unit, 0)
     g.use_graph(True)
     g.sweep(args.warmup, 1, 0.5, args.recompute_every)
     g.sync()
@@ -478,7 +480,9 @@ def run_uneven(args, lib, api, capi, torch):
             'ms_per_step': ms / args.steps, 'higher_is_better': True, 'dtype': 'f32', 'data': 'synthetic',
             'config': {'workload': 'uneven', 'batches': chosen, 'launch_threads': st['threads'],
                        'graph_launches': st['graph_launches'], 'recompute_every': args.recompute_every,
-                       'autotune_s': t_tune},
+                       'autotune_s': t_tune,
+                       'schedule': 'static: one CTA per walker' if args.schedule == 'static'
+                                   else 'work queue, units of %d moves' % (args.unit or capi.SCHED_UNIT_DEFAULT)},
             'separate_launches': {'value': moves / (t_sep / 1e3), 'ms_per_step': t_sep / args.steps}}
 
 

@@ -391,8 +391,8 @@ int qmc_walkers_set_prefetch(qmc_walkers* w, int mode);
  * queue runs three CTAs per SM at up to 112 registers a thread, and the
  * walkers take turns where they outnumber the slots.  At NiO-128 it measured
  * 141 ms per 512-walker launch against 173 ms static, 80 against 101 ms at
- * 148 walkers.  AUTO (the default) is QUEUE.  Batch groups always launch
- * STATIC. */
+ * 148 walkers.  AUTO (the default) is QUEUE.  Batch groups choose theirs
+ * with qmc_group_set_schedule. */
 enum { QMC_SCHED_AUTO = 0, QMC_SCHED_STATIC = 1, QMC_SCHED_QUEUE = 2 };
 #define QMC_SCHED_UNIT_DEFAULT 16
 int qmc_walkers_set_schedule(qmc_walkers* w, int mode, int unit_moves, int ctas);
@@ -418,6 +418,12 @@ int qmc_group_destroy(qmc_group* g);
 /* launch block size: at least every batch's own threads per walker */
 int qmc_group_set_threads(qmc_group* g, int threads);
 int qmc_group_use_graph(qmc_group* g, int enable);
+/* The group's shared launches in the work-queue form or one CTA per walker
+ * (QMC_SCHED_*, as qmc_walkers_set_schedule; unit_moves 0 = the default,
+ * ctas 0 = every resident CTA slot): the queue takes units of any batch's
+ * walkers.  AUTO (the default) is the queue.  The request loop's shared
+ * launches take the queue too. */
+int qmc_group_set_schedule(qmc_group* g, int mode, int unit_moves, int ctas);
 /* n_steps MC steps (device RNG streams) of every batch; asynchronous.
  * recompute_every: FP64 refresh of a batch's inverses after every
  * recompute_every-th step of that batch (0 = never). */

@@ -136,6 +136,7 @@ PRODUCT_ONLY = {
     'walkers_set_threads': (I, [P, I]),
     'walkers_set_prefetch': (I, [P, I]),
     'walkers_set_schedule': (I, [P, I, I, I]),
+    'group_set_schedule': (I, [P, I, I, I]),
     'local_kinetic': (I, [P, PD]),
     'walkers_checkpoint_bytes': (I, [P, C.POINTER(C.c_size_t)]),
     'walkers_checkpoint': (I, [P, P, C.c_size_t]),

@@ -1434,10 +1434,8 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
   const int queue_ctas = sweep_queue_ctas(w);
   if (queue_ctas < 0)
     return fail(QMC_ERR_CUDA, "occupancy query failed");
-  const size_t n_sched =
-      queue_ctas ? sweep_queue_words((int)W, queue_ctas,
-                                     sweep_queue_units((int)N, w->sys->h.n_up, n_substeps, w->sched_unit))
-                 : 0;
+  const size_t total_units = W * (size_t)sweep_queue_units((int)N, w->sys->h.n_up, n_substeps, w->sched_unit);
+  const size_t n_sched     = queue_ctas ? sweep_queue_words((int)W, queue_ctas, total_units) : 0;
   if (n_sched > (size_t)INT32_MAX)
     return fail(QMC_ERR_ARG, "too many work-queue units in one launch: take longer units");
   if (w->cap_sched < n_sched)
@@ -1460,8 +1458,9 @@ static int sweep_steps(qmc_walkers* w, int n_steps, int n_substeps, double accep
     if (queue_ctas > 0)
     {
       CK(cudaMemsetAsync(w->d_sched, 0, n_sched * sizeof(int), w->stream));
-      CK(launch_sweep_queue(w->fp32, w->d_task, queue_ctas, n_substeps, accept, w->threads, w->dw.k, w->stream,
-                            w->use_tc, j3, w->max_moves > 1, w->sched_unit, w->d_sched));
+      const QueueLaunch q{w->d_task,    1,          (int)W, (int)total_units, n_substeps, w->sched_unit,
+                          queue_ctas, w->threads, accept, w->use_tc,      w->d_sched};
+      CK(launch_sweep_queue(w->fp32, q, w->dw.k, j3, w->max_moves > 1, w->stream));
     }
     else
       CK(launch_sweep(w->fp32, w->d_task, 1, (int)W, n_substeps, accept, w->threads, w->dw.npad, w->dw.k,

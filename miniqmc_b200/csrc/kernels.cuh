@@ -63,10 +63,10 @@ cudaError_t launch_sweep(bool fp32, const SweepTask* d_tasks, int n_tasks, int t
 // queue: of the work-queue form (launch_sweep_queue)
 int sweep_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool epoch, bool queue = false);
 int sweep_queue_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, bool epoch);
-// the sweep of one batch in the work-queue form: `ctas` resident CTAs take
-// units of at most `unit` moves of one spin of a walker, a walker passing
-// from CTA to CTA between its units; sched: device ints, zero,
-// sweep_queue_words of them
+// the fused sweep in the work-queue form over a list of tasks (one batch,
+// or a batch group): `ctas` resident CTAs take units of at most `unit`
+// moves of one spin of a walker, a walker passing from CTA to CTA between
+// its units.  sched: device ints, zero, sweep_queue_words of them.
 constexpr int QUEUE_HDR = 4;   // counters of the work-queue launch
 constexpr int QUEUE_SMS = 256; // per-SM words (SM ids above share the last)
 // units of one walker's step in the work-queue form
@@ -74,14 +74,21 @@ inline int sweep_queue_units(int n_elec, int n_up, int n_substeps, int unit)
 {
   return n_substeps * ((n_up + unit - 1) / unit + (n_elec - n_up + unit - 1) / unit);
 }
-// schedule words of a work-queue launch of W walkers on `ctas` CTAs
-inline size_t sweep_queue_words(int W, int ctas, int units_per_walker)
+// schedule words of a work-queue launch over n_walkers walkers (all tasks)
+// on `ctas` CTAs with total_units units in all
+inline size_t sweep_queue_words(int n_walkers, int ctas, size_t total_units)
 {
-  return (size_t)QUEUE_HDR + QUEUE_SMS + W + ctas + (size_t)W * units_per_walker;
+  return (size_t)QUEUE_HDR + QUEUE_SMS + n_walkers + ctas + total_units;
 }
-cudaError_t launch_sweep_queue(bool fp32, const SweepTask* d_task, int ctas, int n_substeps, double accept,
-                               int threads, int max_k, cudaStream_t st, bool tc, bool j3, bool epoch, int unit,
-                               int* sched);
+struct QueueLaunch
+{
+  const SweepTask* tasks; // device; first_block = the task's first walker over all tasks
+  int n_tasks, n_walkers, total_units, n_substeps, unit, ctas, threads;
+  double accept;
+  bool tc;     // some task's flushes run on the tensor cores (CTAs allocate TMEM)
+  int* sched;  // device, sweep_queue_words(...) ints, zero
+};
+cudaError_t launch_sweep_queue(bool fp32, const QueueLaunch& q, int max_k, bool j3, bool epoch, cudaStream_t st);
 
 // evaluateLog pieces
 // ratio_mode_only: only the derivative rows of the determinants whose last

@@ -2,11 +2,13 @@
 // the launch-configuration autotuner (qmc_autotune) and the request loop
 // that admits VMC jobs as they arrive (qmc_server).
 //
-// The fused sweep kernel already runs one CTA per walker over a list of
-// SweepTasks, each with its own system (spline table, lattice, Jastrows),
-// electron count and walker state.  A group fills that list once with its
-// batches, so one launch per MC step moves every walker of every system;
-// the launch can be captured once as a CUDA graph and replayed per step.
+// The fused sweep runs over a list of SweepTasks, each with its own system
+// (spline table, lattice, Jastrows), electron count and walker state: in
+// the work-queue form (the default) every resident CTA slot takes units of
+// any task's walkers, in the static form one CTA per walker.  A group fills
+// that list once with its batches, so one launch per MC step moves every
+// walker of every system; the launch can be captured once as a CUDA graph
+// (with the zeroing of its schedule words) and replayed per step.
 // The server keeps a group of the running jobs and rebuilds the list only
 // when a job starts or ends.
 #include "host_api.hpp"
@@ -35,8 +37,20 @@ struct TaskList
   SweepTask* d = nullptr;
   int cap = 0, n = 0, blocks = 0, threads = 64, max_npad = 0, max_k = 0;
   bool fp32 = true, tc = false, j3 = false, epoch = false;
+  // the work-queue form (QMC_SCHED_AUTO / QUEUE; STATIC launches one CTA
+  // per walker): per task its walkers, electrons and up electrons, the CTAs
+  // of a launch, and the schedule words prepared for n_substeps
+  int sched_mode = QMC_SCHED_AUTO, sched_unit = QMC_SCHED_UNIT_DEFAULT, sched_ctas = 0;
+  std::vector<int> task_W, task_N, task_nup;
+  int queue_ctas = 0, prepared_substeps = -1;
+  size_t total_units = 0, n_words = 0, cap_sched = 0;
+  int* sched = nullptr;
 
-  ~TaskList() { cudaFree(d); }
+  ~TaskList()
+  {
+    cudaFree(d);
+    cudaFree(sched);
+  }
 
   // fill the device task list for `batches` (stream-ordered copy)
   int build(const std::vector<qmc_walkers*>& batches, int launch_threads, cudaStream_t st)
@@ -53,9 +67,15 @@ struct TaskList
     std::vector<SweepTask> h;
     blocks = 0, max_npad = 0, max_k = 0, tc = false, j3 = false, epoch = false;
     threads = launch_threads;
+    task_W.clear();
+    task_N.clear();
+    task_nup.clear();
     double inflight = 0;
     for (auto* w : batches)
     {
+      task_W.push_back(w->dw.W);
+      task_N.push_back(w->dw.N);
+      task_nup.push_back(w->sys->h.n_up);
       SweepTask t = sweep_task(w, blocks);
       t.tc        = (w->use_tc && threads >= 128) ? 1 : 0;
       tc          = tc || t.tc;
@@ -76,12 +96,62 @@ struct TaskList
     }
     if (n)
       CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(SweepTask), cudaMemcpyHostToDevice, st));
+    queue_ctas        = 0;
+    prepared_substeps = -1;
+    if (n && sched_mode != QMC_SCHED_STATIC)
+    {
+      int dev = 0, sms = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      const int per_sm = sweep_occupancy(fp32, threads, max_k, tc, j3, epoch, true);
+      if (per_sm < 1)
+        return fail(QMC_ERR_CUDA, "occupancy query failed");
+      queue_ctas = sched_ctas > 0 ? sched_ctas : per_sm * sms;
+    }
+    return QMC_OK;
+  }
+
+  // the schedule words of a work-queue launch of n_substeps, allocated here
+  // (outside any stream capture); *moved: the buffer changed, so a graph
+  // that captured the old one must go
+  int prepare(int n_substeps, cudaStream_t st, bool* moved)
+  {
+    *moved = false;
+    if (!queue_ctas || prepared_substeps == n_substeps)
+      return QMC_OK;
+    size_t units = 0;
+    for (size_t i = 0; i < task_W.size(); ++i)
+      units += (size_t)task_W[i] * sweep_queue_units(task_N[i], task_nup[i], n_substeps, sched_unit);
+    const size_t words = sweep_queue_words(blocks, queue_ctas, units);
+    if (words > (size_t)INT32_MAX)
+      return fail(QMC_ERR_ARG, "too many work-queue units in one launch: take longer units");
+    if (cap_sched < words)
+    {
+      CK(cudaStreamSynchronize(st));
+      cudaFree(sched);
+      sched = nullptr;
+      CK(cudaMalloc(&sched, words * sizeof(int)));
+      cap_sched = words;
+      *moved    = true;
+    }
+    total_units       = units;
+    n_words           = words;
+    prepared_substeps = n_substeps;
     return QMC_OK;
   }
 
   cudaError_t launch(int n_substeps, double accept, cudaStream_t st) const
   {
-    return launch_sweep(fp32, d, n, blocks, n_substeps, accept, threads, max_npad, max_k, st, tc, j3, epoch);
+    if (!queue_ctas)
+      return launch_sweep(fp32, d, n, blocks, n_substeps, accept, threads, max_npad, max_k, st, tc, j3, epoch);
+    if (prepared_substeps != n_substeps)
+      return cudaErrorInvalidValue; // prepare() first
+    cudaError_t e = cudaMemsetAsync(sched, 0, n_words * sizeof(int), st);
+    if (e != cudaSuccess)
+      return e;
+    const QueueLaunch q{d,          n,       blocks, (int)total_units, n_substeps, sched_unit,
+                        queue_ctas, threads, accept, tc,               sched};
+    return launch_sweep_queue(fp32, q, max_k, j3, epoch, st);
   }
 };
 
@@ -211,6 +281,18 @@ int qmc_group_set_threads(qmc_group* g, int threads)
   return g->tasks.build(g->batches, g->threads, g->stream);
 }
 
+int qmc_group_set_schedule(qmc_group* g, int mode, int unit_moves, int ctas)
+{
+  if (!g || mode < QMC_SCHED_AUTO || mode > QMC_SCHED_QUEUE || unit_moves < 0 || ctas < 0)
+    return fail(QMC_ERR_ARG, "bad schedule");
+  CK(cudaStreamSynchronize(g->stream));
+  g->drop_graph();
+  g->tasks.sched_mode = mode;
+  g->tasks.sched_unit = unit_moves ? unit_moves : QMC_SCHED_UNIT_DEFAULT;
+  g->tasks.sched_ctas = ctas;
+  return g->tasks.build(g->batches, g->threads, g->stream);
+}
+
 int qmc_group_use_graph(qmc_group* g, int enable)
 {
   if (!g)
@@ -228,6 +310,11 @@ int qmc_group_sweep(qmc_group* g, int n_steps, int n_substeps, double accept, in
     return fail(QMC_ERR_ARG, "bad sweep options");
   for (int step = 0; step < n_steps; ++step)
   {
+    bool moved = false;
+    if (int st = g->tasks.prepare(n_substeps, g->stream, &moved))
+      return st;
+    if (moved)
+      g->drop_graph();
     if (g->use_graph && g->launched)
     {
       if (!g->exec || g->graph_substeps != n_substeps || g->graph_accept != accept)
@@ -648,6 +735,9 @@ int qmc_server_tick(qmc_server* s, int* n_running, int* n_waiting)
       s->dirty = false;
     }
     // one shared launch moves every walker of every running job by one step
+    bool moved = false;
+    if (int st = s->tasks.prepare(1, s->stream, &moved))
+      return st;
     CK(s->tasks.launch(1, 0.5, s->stream));
     s->launches++;
     std::vector<int64_t> still;

@@ -75,59 +75,55 @@ constexpr unsigned long long kQueueWaitNs = 10ull * 1000 * 1000 * 1000;
 // NiO-128 walkers measured 141 ms per launch against 161.5 ms for four CTAs
 // per SM at 80 registers (and 154 ms for two CTAs per SM at 168 registers).
 template <typename T, bool HAS_J3, bool EPOCH, int MAXT>
-__global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* __restrict__ tasks, int n_substeps,
-                                                           double accept_thr, int tc, int unit, int* sched)
+__global__ void __launch_bounds__(MAXT, 3)
+    sweep_queue_kernel(const SweepTask* __restrict__ tasks, int n_tasks, int n_walkers, int total, int n_substeps,
+                       double accept_thr, int tc, int unit, int* sched)
 {
   __shared__ SysSmem<T> ss;
   __shared__ MoveSmem m;
   __shared__ SplineSmem<T> sp;
   __shared__ WV<T> wv;
-  // the unit in hand: walker, substep, spin, first and end move, index j
-  __shared__ int q_w, q_l, q_spin, q_i0, q_i1, q_j, q_last;
-  // thread 0's hand-over state: the walker this CTA goes on with (or -1),
-  // and whether it is already counted among its SM's waiting CTAs
-  __shared__ int q_keep, q_waiting;
+  // the unit in hand: task, walker (in its task), substep, spin, first and
+  // end move, index j, and its task's electrons and up electrons
+  __shared__ int q_task, q_w, q_l, q_spin, q_i0, q_i1, q_j, q_last, q_N, q_nup;
+  // thread 0's hand-over state: the walker (over all tasks) this CTA goes on
+  // with (or -1), and whether it is already counted among its SM's waiting
+  // CTAs; the task whose system is in `ss`; whether this CTA holds tensor
+  // memory
+  __shared__ int q_keep, q_waiting, q_loaded, q_tc_alloc;
   extern __shared__ __align__(16) unsigned char dyn[];
-  const SweepTask& task = tasks[0];
-  const DevSystem* sys  = task.sys;
-  load_sys(sys, ss); // ends with a barrier
-  const int W = task.dw.W, N = task.dw.N, nup = ss.n_up;
-  const int nu0 = (nup + unit - 1) / unit, nus = nu0 + (N - nup + unit - 1) / unit;
-  const int total = W * n_substeps * nus;
-  int* waiting    = sched + QUEUE_HDR;              // [QUEUE_SMS] CTAs waiting per SM
-  int* units_done = waiting + QUEUE_SMS;            // [W]
-  int* ring       = units_done + W;                 // [CTAs + units]
+  int* waiting    = sched + QUEUE_HDR;   // [QUEUE_SMS] CTAs waiting per SM
+  int* units_done = waiting + QUEUE_SMS; // [n_walkers]
+  int* ring       = units_done + n_walkers; // [CTAs + units]
   const int sm    = min(sm_id(), QUEUE_SMS - 1);
-  const T* ions   = (const T*)sys->ion_soa;
-  const bool DET  = ss.comp & QMC_WF_DET;
-  const int k     = task.dw.k;
-  T* smem         = reinterpret_cast<T*>(dyn + bsm_bytes(k));
   if (threadIdx.x == 0)
   {
-    m.timing = task.timers != nullptr;
     for (int p = 0; p < NPHASE; ++p)
       m.tacc[p] = 0;
     q_keep    = -1;
     q_waiting = 0;
+    q_loaded  = -1;
   }
   if constexpr (sizeof(T) == 4)
-    tc_begin(m, tc && task.tc && DET, task.dw.wait_cycles);
+    tc_begin(m, tc, tasks[0].dw.wait_cycles);
   else
     tc_none(m);
+  if (threadIdx.x == 0)
+    q_tc_alloc = m.tc_on;
   for (;;)
   {
     if (threadIdx.x == 0)
     {
-      int w = q_keep;
-      if (w < 0)
+      int g = q_keep;
+      if (g < 0)
       {
-        // a ticket: the first W are the walkers' first units, each later
-        // one waits for the walker handed over in ring slot `ticket`
+        // a ticket: the first n_walkers are the walkers' first units, each
+        // later one waits for the walker handed over in ring slot `ticket`
         int t = total + (int)gridDim.x;
         if (!m.tc_abort && !ld_relaxed_gpu(sched + 2))
           t = atomicAdd(sched + 1, 1);
-        if (t < W)
-          w = t;
+        if (t < n_walkers)
+          g = t;
         else if (t < total + (int)gridDim.x)
         {
           if (!q_waiting)
@@ -148,7 +144,8 @@ __global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* _
             }
             else if (global_ns() - t0 > kQueueWaitNs)
             {
-              atomicOr(task.dw.status, DEV_ERR_TIMEOUT);
+              for (int i = 0; i < n_tasks; ++i)
+                atomicOr(tasks[i].dw.status, DEV_ERR_TIMEOUT);
               atomicExch(sched + 2, 1);
               break;
             }
@@ -161,31 +158,55 @@ __global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* _
           // before it handed its walker on (that walker is not moved on)
           fence_acquire_gpu();
           if (v && !ld_relaxed_gpu(sched + 2))
-            w = v - 1;
+            g = v - 1;
         }
       }
       q_waiting = 0;
       q_keep    = -1;
       q_j       = -1;
-      if (w >= 0)
+      if (g >= 0)
       {
-        const int j = units_done[w]; // published with the hand-over
+        int ti = 0;
+        while (ti + 1 < n_tasks && g >= tasks[ti + 1].first_block)
+          ++ti;
+        const SweepTask& tk = tasks[ti];
+        const int w = g - tk.first_block, N = tk.dw.N, nup = tk.sys->n_up;
+        const int nu0 = (nup + unit - 1) / unit, nus = nu0 + (N - nup + unit - 1) / unit;
+        const int j = units_done[g]; // published with the hand-over
         const int l = j / nus, r = j - l * nus;
+        q_task = ti;
         q_w    = w;
         q_j    = j;
         q_l    = l;
+        q_N    = N;
+        q_nup  = nup;
         q_spin = r < nu0 ? 0 : 1;
         q_i0   = r < nu0 ? r * unit : nup + (r - nu0) * unit;
         q_i1   = r < nu0 ? min(q_i0 + unit, nup) : min(q_i0 + unit, N);
         q_last = (l == n_substeps - 1 && r == nus - 1) ? 1 : 0;
-        wv       = make_wv<T>(task.dw, w);
-        m.tstamp = clock64();
+        wv     = make_wv<T>(tk.dw, w);
+        // the unit's flushes on the tensor cores where its task asks
+        m.tc_on    = q_tc_alloc && tk.tc && (tk.sys->comp & QMC_WF_DET);
+        m.tc_limit = tk.dw.wait_cycles;
+        m.timing   = tk.timers != nullptr;
+        m.tstamp   = clock64();
       }
     }
     __syncthreads();
     if (q_j < 0)
       break;
-    const int w = q_w, l = q_l, spin = q_spin;
+    if (q_task != q_loaded)
+    {
+      load_sys(tasks[q_task].sys, ss); // ends with a barrier
+      if (threadIdx.x == 0)
+        q_loaded = q_task;
+    }
+    const SweepTask& task = tasks[q_task];
+    const DevSystem* sys  = task.sys;
+    const int w = q_w, l = q_l, spin = q_spin, N = q_N, k = task.dw.k;
+    const T* ions  = (const T*)sys->ion_soa;
+    const bool DET = ss.comp & QMC_WF_DET;
+    T* smem        = reinterpret_cast<T*>(dyn + bsm_bytes(k));
     const double* urp;
     const double* dp;
     if (task.rng_mode == QMC_RNG_DEVICE)
@@ -243,7 +264,7 @@ __global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* _
     if (DET)
     {
       phase_mark(m, PH_REDUCE);
-      if (q_i1 == N || (spin == 0 && q_i1 == nup))
+      if (q_i1 == N || (spin == 0 && q_i1 == q_nup))
       {
         // the spin's last unit: completeUpdates of its determinant (and of
         // both at the end of the substep, as the static form does)
@@ -271,6 +292,7 @@ __global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* _
     __syncthreads();
     if (threadIdx.x == 0)
     {
+      const int g = task.first_block + w;
       if (q_last)
       {
         wv.ms->partial[0] = wv.ms->partial[1] = 1;
@@ -283,19 +305,19 @@ __global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* _
           task.timers[(size_t)w * NPHASE + p] += m.tacc[p];
           m.tacc[p] = 0;
         }
-      units_done[w] = q_j + 1;
+      units_done[g] = q_j + 1;
       if (m.tc_abort)
         atomicExch(sched + 2, 1);
       if (!q_last)
       {
         if (!m.tc_abort && atomicCAS(waiting + sm, 0, 1) != 0)
-          q_keep = w; // another CTA of this SM waits already: go on here
+          q_keep = g; // another CTA of this SM waits already: go on here
         else
         {
           // no CTA of this SM waits: hand the walker to the one that has
           // waited longest (on a quieter SM) and wait here in its place
           __threadfence();
-          st_release_gpu(ring + W + atomicAdd(sched, 1), w + 1);
+          st_release_gpu(ring + n_walkers + atomicAdd(sched, 1), g + 1);
           q_waiting = !m.tc_abort;
         }
       }
@@ -304,7 +326,11 @@ __global__ void __launch_bounds__(MAXT, 3) sweep_queue_kernel(const SweepTask* _
     }
   }
   if constexpr (sizeof(T) == 4)
+  {
+    if (threadIdx.x == 0)
+      m.tc_on = q_tc_alloc; // tc_end frees what tc_begin took
     tc_end(m);
+  }
 }
 
 template <typename T, bool HAS_J3, bool EPOCH, int MAXT> static void set_queue_smem_attr(size_t bytes)
@@ -345,47 +371,44 @@ int sweep_queue_occupancy(bool fp32, int threads, int max_k, bool tc, bool j3, b
 }
 
 template <typename T, bool HAS_J3, bool EPOCH, int MAXT>
-static void queue_launch_tt(size_t bytes, const SweepTask* d_task, int ctas, int n_substeps, double accept,
-                            int threads, cudaStream_t st, int tc, int unit, int* sched)
+static void queue_launch_tt(size_t bytes, const QueueLaunch& q, cudaStream_t st)
 {
   set_queue_smem_attr<T, HAS_J3, EPOCH, MAXT>(bytes);
-  sweep_queue_kernel<T, HAS_J3, EPOCH, MAXT>
-      <<<ctas, threads, bytes, st>>>(d_task, n_substeps, accept, tc, unit, sched);
+  sweep_queue_kernel<T, HAS_J3, EPOCH, MAXT><<<q.ctas, q.threads, bytes, st>>>(
+      q.tasks, q.n_tasks, q.n_walkers, q.total_units, q.n_substeps, q.accept, q.tc ? 1 : 0, q.unit, q.sched);
 }
 template <typename T, bool HAS_J3, bool EPOCH>
-static void queue_launch_t(size_t bytes, const SweepTask* d_task, int ctas, int n_substeps, double accept,
-                           int threads, cudaStream_t st, int tc, int unit, int* sched)
+static void queue_launch_t(size_t bytes, const QueueLaunch& q, cudaStream_t st)
 {
-  if (threads <= 192)
-    queue_launch_tt<T, HAS_J3, EPOCH, 192>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+  if (q.threads <= 192)
+    queue_launch_tt<T, HAS_J3, EPOCH, 192>(bytes, q, st);
   else
-    queue_launch_tt<T, HAS_J3, EPOCH, 256>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+    queue_launch_tt<T, HAS_J3, EPOCH, 256>(bytes, q, st);
 }
-template <typename T>
-static void launch_queue_t(bool j3, bool epoch, size_t bytes, const SweepTask* d_task, int ctas, int n_substeps,
-                           double accept, int threads, cudaStream_t st, int tc, int unit, int* sched)
+template <typename T> static void launch_queue_t(bool j3, bool epoch, size_t bytes, const QueueLaunch& q, cudaStream_t st)
 {
   if (j3)
-    queue_launch_t<T, true, false>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+    queue_launch_t<T, true, false>(bytes, q, st);
   else if (epoch)
-    queue_launch_t<T, false, true>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+    queue_launch_t<T, false, true>(bytes, q, st);
   else
-    queue_launch_t<T, false, false>(bytes, d_task, ctas, n_substeps, accept, threads, st, tc, unit, sched);
+    queue_launch_t<T, false, false>(bytes, q, st);
 }
 
-cudaError_t launch_sweep_queue(bool fp32, const SweepTask* d_task, int ctas, int n_substeps, double accept,
-                               int threads, int max_k, cudaStream_t st, bool tc, bool j3, bool epoch, int unit,
-                               int* sched)
+cudaError_t launch_sweep_queue(bool fp32, const QueueLaunch& q, int max_k, bool j3, bool epoch, cudaStream_t st)
 {
-  if (max_k > MAXK || (tc && (!fp32 || threads < 128)) || ctas < 1 || unit < 1 || !sched)
+  if (max_k > MAXK || (q.tc && (!fp32 || q.threads < 128)) || q.ctas < 1 || q.unit < 1 || !q.sched ||
+      q.n_tasks < 1 || q.n_walkers < 1)
     return cudaErrorInvalidValue;
   epoch = epoch && !j3;
   if (fp32)
-    launch_queue_t<float>(j3, epoch, sweep_smem_bytes<float>(threads, max_k, tc, j3, epoch), d_task, ctas,
-                          n_substeps, accept, threads, st, tc ? 1 : 0, unit, sched);
+    launch_queue_t<float>(j3, epoch, sweep_smem_bytes<float>(q.threads, max_k, q.tc, j3, epoch), q, st);
   else
-    launch_queue_t<double>(j3, epoch, sweep_smem_bytes<double>(threads, max_k, false, j3, epoch), d_task, ctas,
-                           n_substeps, accept, threads, st, 0, unit, sched);
+  {
+    QueueLaunch q64 = q;
+    q64.tc          = false;
+    launch_queue_t<double>(j3, epoch, sweep_smem_bytes<double>(q.threads, max_k, false, j3, epoch), q64, st);
+  }
   return cudaGetLastError();
 }
 

@@ -74,6 +74,30 @@ def test_group_graph_replay_equals_eager():
             assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize('graph', [False, True])
+def test_group_queue_equals_static(graph):
+    """Three systems (48, 96 and 192 electrons) in one launch per step, with
+    the periodic FP64 refresh: the work-queue form on 3 CTAs in units of 5
+    moves (walkers of every system handed between the CTAs, each CTA loading
+    the system of the walker it takes) gives the static form's walkers bit
+    for bit, eagerly and replayed from a graph."""
+    systems = [_system(t) for t in ((1, 1, 1), (2, 1, 1), (2, 2, 1))]
+    out = []
+    for mode, unit, ctas in ((capi.SCHED_STATIC, 0, 0), (capi.SCHED_QUEUE, 5, 3)):
+        ws = [_batch(s, W, k, seed) for s, W, k, seed in zip(systems, (4, 3, 2), (4, 8, 8), (5, 17, 29))]
+        g = api.Group(H.product(), ws)
+        H.product().call('group_set_schedule', g.h, mode, unit, ctas)
+        g.use_graph(graph)
+        g.sweep(3, 1, 0.5, recompute_every=2)
+        g.sync()
+        out.append([_results(w) for w in ws])
+        g.close()
+    for a, b in zip(out[0], out[1]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    assert any(r[0].sum() > 0 for r in out[1])
+
+
 def test_autotune_returns_a_measured_candidate():
     s = _system((2, 1, 1))
     best, allr = api.autotune(H.product(), s, 16, delays=(4, 8), n_steps=1)
