@@ -1,4 +1,5 @@
-// sweep_queue.cu -- the fused sweep of one batch in the work-queue form:
+// sweep_queue.cu -- the fused sweep in the work-queue form, over a list of
+// tasks (one batch, or the batches of a group or of the request loop):
 // every resident CTA slot takes units of a few moves of a walker, walkers
 // passing between CTAs (and SMs) between their units.
 #include "sweep.cuh"
@@ -7,24 +8,26 @@ namespace qmc
 {
 // ------------------------------------------------- queue schedule -----
 // With more walkers than SMs the static launch leaves some SMs with one
-// walker more than others (512 walkers on 148 SMs: 68 SMs with four, 80
-// with three), and the SMs with four set the step while the others idle at
-// its end.  The queue form runs every resident CTA slot and cuts each
-// walker's step into units of at most `unit` consecutive moves of one spin.
-// The spare slots (592 - 512 at that size) are CTAs waiting for a walker.
-// When a unit ends on an SM where no CTA waits, its SM runs one walker more
-// than the others: the CTA hands the walker to the CTA that has waited
-// longest (on a quieter SM) and becomes that SM's waiting CTA; where a CTA
-// waits already, the walker goes on in place.  So walkers move from busier
-// to quieter SMs only, the roles rotate, every walker spends about the same
-// share of its step on busier SMs, and no walker waits for a CTA.
+// walker more than others (512 walkers on 148 SMs at four per SM: 68 SMs
+// with four, 80 with three), and the SMs with four set the step while the
+// others idle at its end.  The queue form runs every resident CTA slot and
+// cuts each walker's step into units of at most `unit` consecutive moves of
+// one spin.  Where slots outnumber walkers, the spare slots are CTAs waiting
+// for a walker.  When a unit ends on an SM where no CTA waits, its SM runs
+// one walker more than the others: the CTA hands the walker to the CTA
+// that has waited longest (on a quieter SM) and becomes that SM's waiting
+// CTA; where a CTA waits already, the walker goes on in place.  So walkers
+// move from busier to quieter SMs only, the roles rotate, every walker
+// spends about the same share of its step on busier SMs, and no walker
+// waits for a CTA.  Where walkers outnumber slots, every unit end hands its
+// walker on and the walkers take turns on the slots.
 //
 // Hand-overs go through a ring: a CTA without a walker takes a ticket; the
-// first W tickets are the walkers' first units, and ticket t >= W waits
-// (bounded) for ring slot t, which hand-over t - W fills.  A waiting CTA
-// leaves when every unit of the launch has ended (or the launch stops), so
-// every wait ends; the bound only catches a launch in which no unit has
-// ended for kQueueWaitNs.
+// first n_walkers tickets are the walkers' first units, and ticket
+// t >= n_walkers waits (bounded) for ring slot t, which hand-over
+// t - n_walkers fills.  A waiting CTA leaves when every unit of the launch
+// has ended (or the launch stops), so every wait ends; the bound only
+// catches a launch in which no unit has ended for kQueueWaitNs.
 //
 // Between units the walker's state is all in global memory: a unit that
 // ends a spin flushes its delayed rows (completeUpdates of that spin, as the
@@ -33,11 +36,13 @@ namespace qmc
 // that spin's Binv back.  The moves' arithmetic and order are those of the
 // static form, so the two give the same results bit for bit.
 //
-// sched (device ints, zero before the launch; QUEUE_HDR + QUEUE_SMS + W +
-// CTAs + units): [0] hand-overs, [1] tickets taken, [2] the stop flag (a
-// timed-out wait or an aborted tensor-core flush), [3] units ended; then the
-// CTAs waiting on each SM, the units done by each walker, and the ring
-// (1 + the walker handed over with each ticket).
+// Walkers are numbered over all tasks (a task's first_block is its first).
+// sched (device ints, zero before the launch; sweep_queue_words of them):
+// [0] hand-overs, [1] tickets taken, [2] the stop flag (a timed-out wait or
+// an aborted tensor-core flush), [3] units ended; then the CTAs waiting on
+// each SM, the units done by each walker, and the ring (1 + the walker
+// handed over with each ticket).
+//
 // the waits poll with relaxed loads and take one acquire fence when they
 // end: an acquire at GPU scope also drops the SM's L1 lines, which the
 // walkers running beside a waiting CTA still use
