@@ -158,12 +158,12 @@ def build_workload(lib, args, capi, api, device_rng_seeds):
     return spec, system, walkers
 
 
-# DRAM bytes per electron move of sweep_kernel<float> measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 24.772 + 5.215 GB over one
+# DRAM bytes per electron move of sweep_queue_kernel<float> measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum = 24.809 + 5.231 GB over one
 # launch of 64 walkers x 1536 moves, NiO 4x4x2, grid 74x74x37, k=32, mixed,
-# tensor-core flush); the bench's traffic figure scales it by the moves of
-# one launch
-MEASURED_TRAFFIC_PER_MOVE = (24.772e9 + 5.215e9) / (64 * 1536)
+# tensor-core flush; the static sweep_kernel measured 24.772 + 5.215 GB);
+# the bench's traffic figure scales it by the moves of one launch
+MEASURED_TRAFFIC_PER_MOVE = (24.809e9 + 5.231e9) / (64 * 1536)
 
 
 def schedule_of(lib, walkers, args):
@@ -767,7 +767,8 @@ def main():
                 'frac': achieved / pk['hbm_gbs'],
                 'traffic': (MEASURED_TRAFFIC_PER_MOVE * W * N
                             if (args.precision == 'mixed' and args.delay == 32) else None),
-                'traffic_source': 'ncu dram bytes per move (64 walkers, grid 74x74x37) x moves per launch',
+                'traffic_source': 'ncu dram bytes per move of sweep_queue_kernel (64 walkers, grid 74x74x37) '
+                                  'x moves per launch',
                 'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm,
                 'kernel': '%s<%s>' % (sched['kernel'], 'float' if s == 4 else 'double'), 'launch_ms': avg_launch_ms}
     # the Woodbury GEMMs on the tensor cores (tcgen05 kind::tf32, 3xTF32):
