@@ -67,6 +67,8 @@ def parse():
                     help='the sweep CTAs\' schedule (qmc_walkers_set_schedule)')
     ap.add_argument('--unit', type=int, default=0, help='moves per unit of the work-queue schedule (0: default)')
     ap.add_argument('--threads', type=int, default=0, help='threads per walker (0: the library default)')
+    ap.add_argument('--max-moves', type=int, default=1,
+                    help='moves the sweep evaluates together (qmc_walkers_set_move_batching)')
     ap.add_argument('--flush', default='tc', choices=['tc', 'simt'],
                     help='Woodbury flush on the tensor cores (tcgen05 3xTF32) or the CUDA cores (FP32 FMA)')
     ap.add_argument('--plain-steps', type=int, default=4,
@@ -661,6 +663,8 @@ def main():
         lib.call('walkers_set_tensor_cores', walkers.h, 1 if args.flush == 'tc' else 0)
     if args.threads:
         lib.call('walkers_set_threads', walkers.h, args.threads)
+    if args.max_moves != 1:
+        lib.call('walkers_set_move_batching', walkers.h, args.max_moves)
     mode = {'auto': capi.SCHED_AUTO, 'static': capi.SCHED_STATIC, 'queue': capi.SCHED_QUEUE}[args.schedule]
     lib.call('walkers_set_schedule', walkers.h, mode, args.unit, 0)
     sched = schedule_of(lib, walkers, args)
