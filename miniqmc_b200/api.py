@@ -314,6 +314,11 @@ class Walkers:
         self.lib.call('wf_ratio', self.h, iat, _pd(r))
         return r
 
+    def set_schedule(self, mode=capi.SCHED_AUTO, unit_moves=0, ctas=0):
+        """qmc_walkers_set_schedule: the fused sweep's CTAs in the work-queue
+        form (AUTO, QUEUE) or one per walker (STATIC)."""
+        self.lib.call('walkers_set_schedule', self.h, mode, unit_moves, ctas)
+
     def evaluate_ratios(self, walker, iat, pos):
         """WaveFunction::evaluateRatios: one walker's ratios of electron iat
         at absolute positions pos[n][3]."""
@@ -489,6 +494,9 @@ class Group:
 
     def use_graph(self, enable=True):
         self.lib.call('group_use_graph', self.h, 1 if enable else 0)
+
+    def set_schedule(self, mode=capi.SCHED_AUTO, unit_moves=0, ctas=0):
+        self.lib.call('group_set_schedule', self.h, mode, unit_moves, ctas)
 
     def sweep(self, n_steps=1, n_substeps=1, accept=0.5, recompute_every=0):
         self.lib.call('group_sweep', self.h, n_steps, n_substeps, accept, recompute_every)

@@ -86,7 +86,7 @@ def test_group_queue_equals_static(graph):
     for mode, unit, ctas in ((capi.SCHED_STATIC, 0, 0), (capi.SCHED_QUEUE, 5, 3)):
         ws = [_batch(s, W, k, seed) for s, W, k, seed in zip(systems, (4, 3, 2), (4, 8, 8), (5, 17, 29))]
         g = api.Group(H.product(), ws)
-        H.product().call('group_set_schedule', g.h, mode, unit, ctas)
+        g.set_schedule(mode, unit, ctas)
         g.use_graph(graph)
         g.sweep(3, 1, 0.5, recompute_every=2)
         g.sync()

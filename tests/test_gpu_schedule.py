@@ -29,7 +29,7 @@ def _batch(spec, precision, W, delay, seeds, mode, unit=0, ctas=0, moves=1, tc=N
     w.init_random(seeds)
     if threads:
         lib.call('walkers_set_threads', w.h, threads)
-    lib.call('walkers_set_schedule', w.h, mode, unit, ctas)
+    w.set_schedule(mode, unit, ctas)
     if moves > 1:
         lib.call('walkers_set_move_batching', w.h, moves)
     if tc is not None:
