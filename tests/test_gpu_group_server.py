@@ -98,6 +98,19 @@ def test_group_queue_equals_static(graph):
     assert any(r[0].sum() > 0 for r in out[1])
 
 
+def test_group_schedule_rejects_bad_settings():
+    ws = [_batch(_system((1, 1, 1)), 2, 4, 3)]
+    g = api.Group(H.product(), ws)
+    for bad in ((3, 0, 0), (-1, 0, 0), (capi.SCHED_QUEUE, -1, 0), (capi.SCHED_QUEUE, 0, -1)):
+        with pytest.raises(api.QMCError) as e:
+            g.set_schedule(*bad)
+        assert e.value.status == 1  # QMC_ERR_ARG
+    g.set_schedule(capi.SCHED_STATIC)
+    g.sweep(1, 1, 0.5)
+    g.sync()
+    g.close()
+
+
 def test_autotune_returns_a_measured_candidate():
     s = _system((2, 1, 1))
     best, allr = api.autotune(H.product(), s, 16, delays=(4, 8), n_steps=1)

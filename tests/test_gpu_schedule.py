@@ -87,6 +87,11 @@ def test_queue_three_body_jastrow():
     _compare(SMALL, capi.PREC_FP64, 4, 4, unit=5, ctas=3, components=capi.WF_ALL | capi.WF_J3)
 
 
+def test_queue_jastrow_only():
+    # no determinant: no Binv to carry between units, no flushes
+    _compare(SMALL, capi.PREC_MIXED, 5, 4, unit=7, ctas=2, components=capi.WF_J1 | capi.WF_J2)
+
+
 def test_queue_epochs():
     _compare(SMALL, capi.PREC_MIXED, 4, 8, unit=7, ctas=2, moves=4)
 
