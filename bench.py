@@ -161,11 +161,12 @@ def build_workload(lib, args, capi, api, device_rng_seeds):
 
 
 # DRAM bytes per electron move of sweep_queue_kernel<float> measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 24.809 + 5.231 GB over one
-# launch of 64 walkers x 1536 moves, NiO 4x4x2, grid 74x74x37, k=32, mixed,
-# tensor-core flush; the static sweep_kernel measured 24.772 + 5.215 GB);
+# at the default workload (dram__bytes_read.sum + dram__bytes_write.sum =
+# 360.58 + 77.51 GB over one launch of 512 walkers x 1536 moves, NiO 4x4x2,
+# grid 148x148x74, k=32, mixed, tensor-core flush; 64 walkers on a 74x74x37
+# grid measured 24.81 + 5.23 GB, the L2 then holding more of each walker);
 # the bench's traffic figure scales it by the moves of one launch
-MEASURED_TRAFFIC_PER_MOVE = (24.809e9 + 5.231e9) / (64 * 1536)
+MEASURED_TRAFFIC_PER_MOVE = (360.58e9 + 77.51e9) / (512 * 1536)
 
 
 def schedule_of(lib, walkers, args):
@@ -771,7 +772,7 @@ def main():
                 'frac': achieved / pk['hbm_gbs'],
                 'traffic': (MEASURED_TRAFFIC_PER_MOVE * W * N
                             if (args.precision == 'mixed' and args.delay == 32) else None),
-                'traffic_source': 'ncu dram bytes per move of sweep_queue_kernel (64 walkers, grid 74x74x37) '
+                'traffic_source': 'ncu dram bytes per move of sweep_queue_kernel (512 walkers, grid 148x148x74) '
                                   'x moves per launch',
                 'peak_kind': pk_kind, 'algorithmic_bytes_per_move': bpm,
                 'kernel': '%s<%s>' % (sched['kernel'], 'float' if s == 4 else 'double'), 'launch_ms': avg_launch_ms}
